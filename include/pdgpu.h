@@ -1,0 +1,232 @@
+/*
+ * pdgpu.h -- C ABI of libpdgpu.so, a B200-native (sm_100a) drop-in for the
+ * single-process GPU particle path of OpenFPM pdata's vector_dist.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (PD_OK or a negative PD_E* code, never throws across the ABI) and, where it
+ * launches GPU work, a caller-provided CUDA stream passed as `void*`
+ * (NULL = the legacy default stream).  Host buffers are caller-owned; device
+ * storage is owned by the handles.  Each declaration names the reference
+ * interface it replaces (file:line inside the openfpm_pdata project).
+ *
+ * Positions cross the ABI as AoS xyz triples (Point<3,St>); properties as
+ * component-major arrays (component c of particle i at [c*n + i]).
+ */
+#ifndef PDGPU_H
+#define PDGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PD_OK 0
+#define PD_EINVAL (-1)    /* bad argument (the reference: ACTION_ON_ERROR under SE_CLASS1) */
+#define PD_ENOMEM (-2)    /* device allocation failed */
+#define PD_ECUDA (-3)     /* a CUDA call failed; pd_last_error() has the text */
+#define PD_ESTALE (-4)    /* handle built for an older decomposition / particle set */
+#define PD_ETIMEOUT (-5)  /* a bounded device wait gave up */
+#define PD_EOVERFLOW (-6) /* a device-side capacity was exceeded; the result is void */
+#define PD_ESTATE (-7)    /* call out of order (e.g. restore_order without a reorder) */
+
+/* ---- value types -------------------------------------------------------- */
+#define PD_F32 1
+#define PD_F64 2
+#define PD_I32 3
+#define PD_U32 4
+#define PD_I64 5
+
+/* boundary conditions: same values as the reference (NON_PERIODIC, PERIODIC) */
+#define PD_NON_PERIODIC 0
+#define PD_PERIODIC 1
+
+/* ghost_get / map options, same values as the reference
+ * (Vector/cuda/vector_dist_comm_util_funcs.cuh:13-15, util/common_pdata.hpp:12-13) */
+#define PD_NO_POSITION 1
+#define PD_WITH_POSITION 2
+#define PD_NO_CHANGE_ELEMENTS 4
+#define PD_SKIP_LABELLING 512
+#define PD_KEEP_PROPERTIES 512
+#define PD_RUN_ON_DEVICE 1024
+
+/* cell-list options (CL_* of openfpm_data; values are this library's own) */
+#define PD_CL_NON_SYMMETRIC 2
+#define PD_CL_GPU_REORDER_POSITION 64
+#define PD_CL_GPU_REORDER_PROPERTY 128
+#define PD_CL_GPU_REORDER (PD_CL_GPU_REORDER_POSITION | PD_CL_GPU_REORDER_PROPERTY)
+
+/* reductions (reduce_local<prp,_add_/_max_>) */
+#define PD_RED_ADD 1
+#define PD_RED_MAX 2
+
+typedef struct pd_vd_s* pd_vd; /* vector_dist_gpu<3,St,aggregate<...>>          */
+typedef struct pd_cl_s* pd_cl; /* CellList_gpu<3,St,CudaMemory,shift_only<3,St>> */
+typedef struct pd_vl_s* pd_vl; /* VerletList<3,St,VL_NON_SYMMETRIC,...>         */
+typedef struct pd_md_s* pd_md; /* velocity-Verlet LJ driver bound to a vector   */
+
+/* Kernel view of a vector (vector_dist_ker, Vector/vector_dist_kernel.hpp:57-305):
+ * non-owning device pointers, invalid after any call that can reallocate
+ * (map, ghost_get, resize); `epoch` increments on every such call. */
+typedef struct {
+    void* pos;          /* float4 / double4 records (x, y, z, unused)       */
+    void* prop[16];     /* component-major property arrays, stride `stride` */
+    int prop_type[16];
+    int prop_ncomp[16];
+    int n_prop;
+    int dtype;
+    long stride;        /* allocated capacity in particles                  */
+    long size_local;    /* ghostMarker: real particles are [0, size_local)  */
+    long size;          /* real + ghost particles                           */
+    long epoch;
+} pd_view_t;
+
+/* Kernel view of a cell list (CellList_gpu::toKernel): the grid and the
+ * counting-sort result. */
+typedef struct {
+    const int* cell_start;  /* ncells + 1 offsets into sorted_ids            */
+    const int* sorted_ids;  /* particle index of each sorted slot            */
+    const int* dom_sort_ids;/* sorted slot of each domain particle, in order  */
+    long ncells;
+    int gs[3];              /* cells per dimension including padding         */
+    int div[3];
+    int pad;
+    int nn_box;             /* NNIteratorBox layers                          */
+    double box_lo[3];
+    double spacing[3];
+    long ghost_marker;
+    long n_part;
+} pd_cl_view_t;
+
+/* launch shape of getDomainIteratorGPU (vector_dist.hpp:1958-1965) */
+typedef struct {
+    unsigned int wthr[3];
+    unsigned int thr[3];
+} pd_launch_t;
+
+/* LJ 12-6 parameters */
+typedef struct {
+    double eps, sigma, r_cut;
+} pd_lj_params_t;
+
+/* velocity-Verlet parameters */
+typedef struct {
+    double dt, mass, skin;
+    int vel_prop;   /* property id holding velocities (3 comps, dtype of the vector) */
+    int force_prop; /* property id receiving forces   (3 comps, dtype of the vector) */
+    int use_cell_list; /* 1: force from the cell list every step (no Verlet list) */
+} pd_md_params_t;
+
+/* ---- library ------------------------------------------------------------ */
+const char* pd_last_error(void);
+/* number of CUDA kernels this library has launched so far (all handles) */
+unsigned long long pd_launch_count(void);
+int pd_device_info(int* sm_count, long* free_bytes, long* total_bytes);
+
+/* ---- vector_dist -------------------------------------------------------- */
+/* vector_dist(size_t np, Box<dim,St> box, const size_t (&bc)[dim], const Ghost<dim,St>& g)
+ * -- Vector/vector_dist.hpp:498-518.  dim must be 3; ghost is per dimension. */
+int pd_create(int dim, int dtype, long n, const double* lo, const double* hi, const int* bc,
+              const double* ghost, int opts, pd_vd* out);
+int pd_destroy(pd_vd h);
+/* aggregate<...> property list: append one property of `ncomp` components */
+int pd_add_prop(pd_vd h, int type, int ncomp, int* prop_id);
+/* size_local / size_local_with_ghost -- vector_dist.hpp:559-572 */
+int pd_size(pd_vd h, long* size_local, long* size_with_ghost);
+/* resize of the local part (drops ghosts) -- vector_dist.hpp:923-984 add/resize */
+int pd_resize(pd_vd h, long n);
+/* hostToDevicePos / deviceToHostPos -- vector_dist.hpp:2984-3030; host AoS xyz in
+ * the vector's dtype, particles [offset, offset+count) */
+int pd_h2d_pos(pd_vd h, const void* host_xyz, long offset, long count, void* stream);
+int pd_d2h_pos(pd_vd h, void* host_xyz, long offset, long count, void* stream);
+/* hostToDeviceProp<prp> / deviceToHostProp<prp>; host component-major [ncomp][count] */
+int pd_h2d_prop(pd_vd h, int prop, const void* host, long offset, long count, void* stream);
+int pd_d2h_prop(pd_vd h, int prop, void* host, long offset, long count, void* stream);
+/* map(RUN_ON_DEVICE) on one process -- vector_dist.hpp:2158-2176 ->
+ * vector_dist_comm.hpp:1405-1437 -> apply_bc_each_part (vector_dist_cuda_funcs.cuh:45-53):
+ * drops the ghost and wraps every periodic coordinate with periodic_l. */
+int pd_map(pd_vd h, int opt, void* stream);
+/* ghost_get<prp...>(opt) on one process -- vector_dist.hpp:2203-2231 ->
+ * vector_dist_comm.hpp:1754-1829, 734-795: periodic images of the real particles,
+ * appended after ghostMarker, particle-major with shift ids ascending, all
+ * properties copied.  opt & PD_SKIP_LABELLING replays the stored image list
+ * (process_ghost_particles_local, vector_dist_cuda_funcs.cuh:133-155); with
+ * PD_NO_POSITION only properties are refreshed.  prop_mask selects the
+ * properties copied on a replay (bit p = property p; ~0 = all). */
+int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream);
+/* the (source, shift id) record of every ghost (o_part_loc) */
+int pd_ghost_records(pd_vd h, int* src, int* shift_id, long cap, long* n_img);
+/* explicit box-list image kernels, the reference's num_shift_ghost_each_part +
+ * scan + shift_ghost_each_part (vector_dist_cuda_funcs.cuh:157-233) on caller
+ * data: boxes [nb][2][3] (lo, hi), sv[nb] shift ids sorted ascending, shifts[..][3].
+ * Device pointers; counts[n] out; images written after `n` in pos/prop arrays. */
+int pd_ghost_count_boxes(pd_vd h, const double* boxes_host, const int* sv_host, int nb, int* counts_host,
+                         void* stream);
+int pd_ghost_get_boxes(pd_vd h, const double* boxes_host, const int* sv_host, int nb,
+                       const double* shifts_host, int n_shifts, void* stream);
+/* toKernel() -- vector_dist.hpp:2961-2966 */
+int pd_view(pd_vd h, pd_view_t* out);
+/* getDomainIteratorGPU(n_thr) / getDomainAndGhostIteratorGPU -- vector_dist.hpp:1958-1979 */
+int pd_domain_iterator(pd_vd h, int n_thr, int with_ghost, pd_launch_t* out);
+/* reduce_local<prp,_add_/_max_> -- vector_dist_cuda_funcs.cuh:247-270 (component `comp`) */
+int pd_reduce(pd_vd h, int prop, int comp, int op, void* stream, double* out);
+/* the original index of every particle in its current storage slot */
+int pd_d2h_gid(pd_vd h, long* host, long offset, long count, void* stream);
+
+/* ---- cell list ---------------------------------------------------------- */
+/* getCellListGPU<CellList_gpu<...>>(r_cut, opt, NNIteratorBox, no_se3, ghostEnlargeFactor)
+ * -- vector_dist.hpp:1222-1260 (geometry only; nothing is binned yet) */
+int pd_celllist_create(pd_vd h, double r_cut, int opt, int nn_box, double enlarge_factor, pd_cl* out);
+int pd_celllist_destroy(pd_cl cl);
+/* updateCellListGPU<prp...>(cl) -- vector_dist.hpp:1334-1401: cell hash, warp-aggregated
+ * counting sort (stable), and with PD_CL_GPU_REORDER a coalesced reorder of the
+ * positions / the properties in prop_mask into cell order. */
+int pd_celllist_update(pd_vd h, pd_cl cl, unsigned long prop_mask, void* stream);
+/* restoreOrder<prp...>(cl) -- vector_dist.hpp:3042-3049 */
+int pd_restore_order(pd_vd h, pd_cl cl, unsigned long prop_mask, void* stream);
+int pd_celllist_view(pd_cl cl, pd_cl_view_t* out);
+/* download: cell_start[ncells+1], sorted_ids[n] (NULL to skip either) */
+int pd_celllist_get(pd_cl cl, int* cell_start, int* sorted_ids, void* stream);
+/* the reference's test functor calculate_force / calculate_force_sort
+ * (Vector/cuda/vector_dist_gpu_unit_tests.cu:46-119) as a device kernel:
+ * out_prop(p) = sum over getNNIteratorBox q != p of in_prop(q)*(xq-xp)/|xq-xp| */
+int pd_test_force(pd_vd h, pd_cl cl, int in_prop, int out_prop, int sorted, void* stream);
+
+/* ---- Verlet list -------------------------------------------------------- */
+/* getVerlet(r_cut) -- vector_dist.hpp:1514-1547: full list of every domain particle
+ * over domain + ghost within r_cut (self included), built from a cell list of
+ * side r_cut on the domain enlarged by the ghost magnified 1.013. */
+int pd_verlet_create(pd_vd h, double r_cut, pd_vl* out);
+int pd_verlet_destroy(pd_vl vl);
+/* updateVerlet(vl, r_cut) -- vector_dist.hpp:1556-1620 */
+int pd_verlet_update(pd_vd h, pd_vl vl, void* stream);
+/* download as CSR: counts[n] (and idx[sum counts] if non-NULL) */
+int pd_verlet_get(pd_vl vl, int* counts, int* idx, long idx_cap, void* stream);
+
+/* ---- pair kernels ------------------------------------------------------- */
+/* LJ forces of the domain particles from a Verlet list (vl) or a cell list (cl);
+ * writes force_prop (3 comps); returns sum PE and sum virial in energy[2] (FP64). */
+int pd_lj_forces(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t* lj, int force_prop, void* stream,
+                 double* energy);
+
+/* ---- velocity-Verlet LJ driver ------------------------------------------ */
+/* Binds a vector holding real particles (no ghost) to an integrator that keeps
+ * the particles in cell order, periodic images and a skin Verlet list on the
+ * device; rebuilds when the largest displacement since the last build exceeds
+ * skin/2 (skin <= 0: every step). */
+int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* md, pd_md* out);
+int pd_md_destroy(pd_md md);
+/* run `steps` steps; E (if non-NULL) receives [steps][4] = KE, PE, virial, rebuilt */
+int pd_md_run(pd_md md, int steps, void* stream, double* E);
+/* statistics: builds so far, steps so far, device-side error word */
+int pd_md_stats(pd_md md, long* builds, long* steps, int* err);
+/* per-phase device time (CUDA events on the run's stream, one synchronisation per
+ * step while enabled): ms/counts[4] = integrate, rebuild, image refresh, force */
+int pd_md_set_timing(pd_md md, int on);
+/* Verlet rows of the last build: domain particles, mean and longest row */
+int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn);
+int pd_md_timers(pd_md md, double* ms, long* counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDGPU_H */

@@ -1,0 +1,173 @@
+// pd_internal.cuh -- shared internals of libpdgpu.so (host structures, device helpers).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pdgpu.h"
+
+namespace pd {
+
+void set_error(const char* fmt, ...);
+
+#define PD_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) {                                                                        \
+            pd::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));           \
+            return e_ == cudaErrorMemoryAllocation ? PD_ENOMEM : PD_ECUDA;                              \
+        }                                                                                               \
+    } while (0)
+
+#define PD_LAUNCH_CHECK() PD_CUDA(cudaGetLastError())
+
+#define PD_TRY(expr)             \
+    do {                         \
+        int r_ = (expr);         \
+        if (r_ != PD_OK) return r_; \
+    } while (0)
+
+// Device-side error bits (Ctrl::err)
+enum : unsigned int {
+    ERR_IMG_OVERFLOW = 1u,  // more periodic images than the image capacity
+    ERR_NN_OVERFLOW = 2u,   // a Verlet row longer than the list capacity
+    ERR_CELL_RANGE = 4u,    // a particle outside the cell grid (clamped)
+    ERR_CAP_OVERFLOW = 8u,  // real + images beyond the particle capacity
+};
+
+// Control block resident in device memory: sizes that change on the device and
+// reductions read back by the host.
+struct Ctrl {
+    unsigned int n_img;          // periodic images currently stored after the real particles
+    unsigned int err;            // ERR_* bits
+    unsigned int nn_max;         // longest Verlet row seen by the last build
+    unsigned int rebuild;        // rebuild flag of the integrator
+    unsigned long long maxdisp2; // bits of the largest squared displacement (non-negative double)
+    unsigned long long steps;
+    unsigned long long builds;
+};
+
+// Growable device buffer
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b);
+    void release();
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct Prop {
+    int type = 0;
+    int ncomp = 0;
+    int esize = 0;
+    char* d = nullptr;  // component-major [ncomp][cap]
+};
+
+inline int type_size(int t) {
+    switch (t) {
+        case PD_F32: case PD_I32: case PD_U32: return 4;
+        case PD_F64: case PD_I64: return 8;
+        default: return 0;
+    }
+}
+
+// exclusive scan of n uint32 values (in may equal out); writes the total to *total_dev
+int scan_u32(const unsigned int* in, unsigned int* out, long n, unsigned int* total_dev, Buf& scratch,
+             cudaStream_t st);
+
+inline unsigned int grid_for(long n, int block, long cap_blocks = 148L * 64) {
+    long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap_blocks) g = cap_blocks;
+    return (unsigned int)g;
+}
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Every kernel launch of the library goes through launch(): it counts launches
+// (pd_launch_count) so a caller can verify how many native kernels ran.
+extern unsigned long long g_launches;
+template <typename... KArgs, typename... Args>
+inline void launch(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t st, Args... args) {
+    k<<<g, b, smem, st>>>(args...);
+    __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED);
+}
+
+}  // namespace pd
+
+// ---------------------------------------------------------------------------
+// handles
+struct pd_vd_s {
+    int dtype = PD_F64;
+    int pos_bytes = 32;  // per record
+    double lo[3], hi[3], g[3];
+    int bc[3];
+    long n_real = 0;   // ghostMarker
+    long n_total = 0;  // real + ghosts
+    long cap = 0;      // capacity in particles
+    void* pos = nullptr;
+    int* gid = nullptr;  // original index of the particle in each slot
+    std::vector<pd::Prop> props;
+    // periodic images (o_part_loc): source slot and shift id of each ghost
+    pd::Buf img_src, img_shift, img_cnt, img_start;
+    pd::Buf boxes, box_sv, shifts;  // device copies of the local ghost boxes
+    int nbox = 0;
+    long n_img = 0;
+    bool img_valid = false;
+    pd::Ctrl* ctrl = nullptr;    // device
+    pd::Ctrl* ctrl_h = nullptr;  // pinned host mirror
+    pd::Buf scan_scratch, tmp, tmp2, red;
+    long epoch = 0;
+};
+
+struct pd_cl_s {
+    pd_vd owner = nullptr;
+    double r_cut = 0;
+    int opt = 0;
+    int nn_box = 1;
+    double enlarge = 1.013f;
+    int pad = 1;
+    int div[3], gs[3];
+    double box_lo[3], spacing[3];
+    long ncells = 0;
+    pd::Buf cell_start, cell_cnt, sorted, sorted_tmp, cell_of, slot, dom_sort, flags;
+    long n_part = 0;
+    long ghost_marker = 0;
+    bool reordered = false;  // the vector holds cell-ordered data until restore_order
+    unsigned long reordered_mask = 0;
+    long epoch = -1;
+};
+
+struct pd_vl_s {
+    pd_vd owner = nullptr;
+    double r_cut = 0;
+    pd_cl cl = nullptr;  // internal cell list (side r_cut)
+    pd::Buf nbr, nn;     // nbr[k*stride + i], nn[i]
+    long stride = 0;
+    int max_nn = 0;
+    long n_dom = 0;
+    long epoch = -1;
+};
+
+// ---------------------------------------------------------------------------
+// internal host API shared between translation units
+namespace pd {
+int ensure_capacity(pd_vd h, long need, cudaStream_t st);
+int set_ctrl_n_img(pd_vd h, long n_img, cudaStream_t st);
+int read_ctrl(pd_vd h, cudaStream_t st);
+int cl_geometry(pd_cl cl, pd_vd h, double r_cut, double enlarge, int nn_box);
+int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st);
+int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
+               cudaStream_t st);
+int ghost_boxes_upload(pd_vd h, cudaStream_t st);
+int ghost_generate(pd_vd h, long img_cap, bool sync_count, cudaStream_t st);
+int ghost_replay(pd_vd h, unsigned long prop_mask, bool with_pos, const unsigned int* n_img_dev, long n_img_bound,
+                 cudaStream_t st);
+int verlet_build(pd_vd h, pd_vl vl, long n_dom, const unsigned int* n_img_dev, cudaStream_t st, bool check);
+int wrap_positions(pd_vd h, long n, cudaStream_t st);
+}  // namespace pd

@@ -1,0 +1,575 @@
+// pd_md.cu -- Lennard-Jones pair kernels and the velocity-Verlet driver.
+//
+// The reference has no LJ physics (its pair functors are test sums,
+// vector_dist_gpu_unit_tests.cu:46-119, and vector_dist_performance_common.hpp:18-85);
+// the kernels follow that functor pattern -- one thread per domain particle
+// walking its neighbours -- with the LJ 12-6 pair force of a plain cutoff:
+//   F_i = sum_j 24 eps (2 (s/r)^12 - (s/r)^6) / r^2 * (x_i - x_j),   r < r_cut
+//   U   = 1/2 sum_i sum_j 4 eps ((s/r)^12 - (s/r)^6)
+// Velocity Verlet (Swope et al. 1982): v += dt/2 f/m; x += dt v; [rebuild or
+// refresh images]; f = F(x); v += dt/2 f/m.  Energies are reduced in FP64 with a
+// fixed block order (deterministic).
+#include "pd_device.cuh"
+#include "pd_internal.cuh"
+
+namespace pd {
+
+static constexpr int FBLOCK = 256;
+
+template <class T> struct LJP {
+    T eps24, eps4, sig2, rc2;
+};
+
+template <class T>
+__device__ __forceinline__ void lj_acc(const LJP<T>& P, T r2, T dx, T dy, T dz, T& fx, T& fy, T& fz, T& e, T& w) {
+    T ir2 = T(1) / r2;
+    T s2 = P.sig2 * ir2;
+    T s6 = s2 * s2 * s2;
+    T ff = P.eps24 * ir2 * s6 * (T(2) * s6 - T(1));
+    fx += ff * dx;
+    fy += ff * dy;
+    fz += ff * dz;
+    e += P.eps4 * s6 * (s6 - T(1));
+    w += ff * r2;
+}
+
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_lj_verlet(const typename V4<T>::type* __restrict__ pos, long n,
+                                                      const int* __restrict__ nbr, const int* __restrict__ nn,
+                                                      long stride, LJP<T> P, T* __restrict__ f, long fcap,
+                                                      double* __restrict__ part) {
+    double pe = 0, vir = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        typename V4<T>::type xi = ld4(pos, i);
+        int m = nn[i];
+        T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
+        const int* row = nbr + i;
+#pragma unroll 4
+        for (int k = 0; k < m; ++k) {
+            int q = __ldg(row + (long)k * stride);
+            if (q == (int)i) continue;
+            typename V4<T>::type xq = ld4(pos, q);
+            T dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
+            T r2 = dist2(dx, dy, dz);
+            if (r2 < P.rc2) lj_acc(P, r2, dx, dy, dz, fx, fy, fz, e, w);
+        }
+        f[i] = fx;
+        f[fcap + i] = fy;
+        f[2 * fcap + i] = fz;
+        pe += 0.5 * (double)e;
+        vir += 0.5 * (double)w;
+    }
+    pe = block_sum<double, FBLOCK>(pe);
+    vir = block_sum<double, FBLOCK>(vir);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = pe;
+        part[2 * blockIdx.x + 1] = vir;
+    }
+}
+
+// LJ through the cell list (27-cell walk over the cell-ordered positions pcs,
+// whose 4th word holds the original index)
+template <class T> struct IdxDec;
+template <> struct IdxDec<double> {
+    __device__ static int dec(double w) { return (int)__double_as_longlong(w); }
+};
+template <> struct IdxDec<float> {
+    __device__ static int dec(float w) { return __float_as_int(w); }
+};
+
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_lj_cell(const typename V4<T>::type* __restrict__ pos, long n,
+                                                    const typename V4<T>::type* __restrict__ pcs,
+                                                    const unsigned int* __restrict__ cs, Grid<T> G, LJP<T> P,
+                                                    T* __restrict__ f, long fcap, double* __restrict__ part) {
+    double pe = 0, vir = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        typename V4<T>::type xi = ld4(pos, i);
+        unsigned int bad = 0;
+        int c0 = G.coord(0, xi.x, bad), c1 = G.coord(1, xi.y, bad), c2 = G.coord(2, xi.z, bad);
+        T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy) {
+                int y = c1 + dy, z = c2 + dz;
+                if (y < 0 || z < 0 || y >= G.gs[1] || z >= G.gs[2]) continue;
+                int xa = max(c0 - 1, 0), xb = min(c0 + 1, G.gs[0] - 1);
+                long rb = (long)G.gs[0] * (y + (long)G.gs[1] * z);
+                unsigned int a = cs[rb + xa], b = cs[rb + xb + 1];
+                for (unsigned int k = a; k < b; ++k) {
+                    typename V4<T>::type xq = ld4(pcs, k);
+                    if (IdxDec<T>::dec(xq.w) == (int)i) continue;
+                    T dx = xi.x - xq.x, dy2 = xi.y - xq.y, dz2 = xi.z - xq.z;
+                    T r2 = dist2(dx, dy2, dz2);
+                    if (r2 < P.rc2) lj_acc(P, r2, dx, dy2, dz2, fx, fy, fz, e, w);
+                }
+            }
+        f[i] = fx;
+        f[fcap + i] = fy;
+        f[2 * fcap + i] = fz;
+        pe += 0.5 * (double)e;
+        vir += 0.5 * (double)w;
+    }
+    pe = block_sum<double, FBLOCK>(pe);
+    vir = block_sum<double, FBLOCK>(vir);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = pe;
+        part[2 * blockIdx.x + 1] = vir;
+    }
+}
+
+template <class T>
+__global__ void k_gather_cs2(const typename V4<T>::type* __restrict__ pos, const int* __restrict__ sorted, long n,
+                             typename V4<T>::type* __restrict__ out) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        int i = sorted[k];
+        typename V4<T>::type r = ld4(pos, i);
+        if (sizeof(T) == 8) r.w = __longlong_as_double((long long)i);
+        else r.w = __int_as_float(i);
+        st4(out, k, r);
+    }
+}
+
+// v += h f ; x += dt v ; largest |x - xb|^2
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_kick_drift(typename V4<T>::type* __restrict__ pos,
+                                                       const typename V4<T>::type* __restrict__ xb, T* __restrict__ v,
+                                                       const T* __restrict__ f, long cap, long n, T half, T dt,
+                                                       unsigned long long* __restrict__ maxd2) {
+    double mx = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        typename V4<T>::type x = ld4(pos, i);
+        T vx = v[i] + half * f[i];
+        T vy = v[cap + i] + half * f[cap + i];
+        T vz = v[2 * cap + i] + half * f[2 * cap + i];
+        x.x += dt * vx;
+        x.y += dt * vy;
+        x.z += dt * vz;
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        st4(pos, i, x);
+        typename V4<T>::type b = ld4(xb, i);
+        T dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
+        mx = fmax(mx, (double)dist2(dx, dy, dz));
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
+}
+
+// v += h f ; kinetic energy partial sums
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_kick(T* __restrict__ v, const T* __restrict__ f, long cap, long n, T half,
+                                                 double mass, double* __restrict__ part) {
+    double ke = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        T vx = v[i] + half * f[i];
+        T vy = v[cap + i] + half * f[cap + i];
+        T vz = v[2 * cap + i] + half * f[2 * cap + i];
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        ke += 0.5 * mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+    }
+    ke = block_sum<double, FBLOCK>(ke);
+    if (threadIdx.x == 0) part[blockIdx.x] = ke;
+}
+
+// KE only (initial state)
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_ke(const T* __restrict__ v, long cap, long n, double mass,
+                                               double* __restrict__ part) {
+    double ke = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        double vx = v[i], vy = v[cap + i], vz = v[2 * cap + i];
+        ke += 0.5 * mass * (vx * vx + vy * vy + vz * vz);
+    }
+    ke = block_sum<double, FBLOCK>(ke);
+    if (threadIdx.x == 0) part[blockIdx.x] = ke;
+}
+
+// E[s] = (KE, PE, virial, rebuilt) from the fixed-order partials
+__global__ void k_energy(const double* __restrict__ fpart, const double* __restrict__ kpart, int nb,
+                         const unsigned int* __restrict__ rebuilt, double* __restrict__ E) {
+    __shared__ double sh[3][256];
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < nb; i += 256) {
+        a += kpart[i];
+        b += fpart[2 * i];
+        c += fpart[2 * i + 1];
+    }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = b;
+    sh[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        E[0] = sh[0][0];
+        E[1] = sh[1][0];
+        E[2] = sh[2][0];
+        E[3] = rebuilt ? (double)*rebuilt : 0.0;
+    }
+}
+
+}  // namespace pd
+
+struct pd_md_s {
+    pd_vd h = nullptr;
+    pd_lj_params_t lj;
+    pd_md_params_t mp;
+    pd_vl vl = nullptr;   // Verlet list (r_cut + skin)
+    pd_cl cl = nullptr;   // cell list of side r_cut (cell-list mode)
+    pd::Buf xb, fpart, kpart, E;
+    int nblk = 0;
+    bool ready = false;
+    long builds = 0, steps = 0;
+    // optional per-phase device timing (CUDA events on the run's stream)
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    double ms[4] = {0, 0, 0, 0};   // integrate, rebuild, images, force
+    long cnt[4] = {0, 0, 0, 0};
+};
+
+namespace pd {
+
+template <class T> static LJP<T> ljp(const pd_lj_params_t& lj) {
+    LJP<T> P;
+    P.eps24 = (T)(24.0 * lj.eps);
+    P.eps4 = (T)(4.0 * lj.eps);
+    P.sig2 = (T)(lj.sigma * lj.sigma);
+    T rc = (T)lj.r_cut;
+    P.rc2 = rc * rc;
+    return P;
+}
+
+template <class T> static Grid<T> grid_of(pd_cl cl) {
+    Grid<T> G;
+    for (int d = 0; d < 3; ++d) {
+        G.lo[d] = (T)cl->box_lo[d];
+        G.sp[d] = (T)cl->spacing[d];
+        G.gs[d] = cl->gs[d];
+    }
+    G.pad = cl->pad;
+    return G;
+}
+
+// forces of [0, n_real) into force_prop; partials (pe, vir) per block into part
+static int lj_launch(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t& lj, int force_prop, double* part, int nblk,
+                     cudaStream_t st) {
+    Prop& F = h->props[force_prop];
+    long n = h->n_real;
+    if (vl) {
+        if (h->dtype == PD_F64)
+            pd::launch(k_lj_verlet<double>, nblk, FBLOCK, 0, st, (const double4*)h->pos, n, vl->nbr.as<int>(),
+                                                         vl->nn.as<int>(), vl->stride, ljp<double>(lj), (double*)F.d,
+                                                         h->cap, part);
+        else
+            pd::launch(k_lj_verlet<float>, nblk, FBLOCK, 0, st, (const float4*)h->pos, n, vl->nbr.as<int>(), vl->nn.as<int>(),
+                                                        vl->stride, ljp<float>(lj), (float*)F.d, h->cap, part);
+    } else {
+        // cell-ordered copy of all positions for the walk
+        long nt = h->n_total;
+        PD_TRY(h->tmp.ensure((size_t)(nt > 0 ? nt : 1) * h->pos_bytes));
+        unsigned g = grid_for(nt, 256);
+        if (h->dtype == PD_F64) {
+            pd::launch(k_gather_cs2<double>, g, 256, 0, st, (const double4*)h->pos, cl->sorted.as<int>(), nt,
+                                                    h->tmp.as<double4>());
+            pd::launch(k_lj_cell<double>, nblk, FBLOCK, 0, st, (const double4*)h->pos, n, h->tmp.as<double4>(),
+                                                       cl->cell_start.as<unsigned int>(), grid_of<double>(cl),
+                                                       ljp<double>(lj), (double*)F.d, h->cap, part);
+        } else {
+            pd::launch(k_gather_cs2<float>, g, 256, 0, st, (const float4*)h->pos, cl->sorted.as<int>(), nt,
+                                                   h->tmp.as<float4>());
+            pd::launch(k_lj_cell<float>, nblk, FBLOCK, 0, st, (const float4*)h->pos, n, h->tmp.as<float4>(),
+                                                      cl->cell_start.as<unsigned int>(), grid_of<float>(cl),
+                                                      ljp<float>(lj), (float*)F.d, h->cap, part);
+        }
+    }
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+static int force_blocks(long n) {
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long want = (n + FBLOCK - 1) / FBLOCK;
+    long cap = (long)sms * 8;
+    if (want > cap) want = cap;
+    if (want < 1) want = 1;
+    return (int)want;
+}
+
+// wrap, sort the real particles into cell order, periodic images, neighbour structure
+static int md_rebuild(pd_md md, cudaStream_t st) {
+    pd_vd h = md->h;
+    h->n_total = h->n_real;
+    h->img_valid = false;
+    PD_TRY(wrap_positions(h, h->n_real, st));
+    pd_cl sort_cl = md->mp.use_cell_list ? md->cl : md->vl->cl;
+    PD_TRY(cl_build(h, sort_cl, h->n_real, nullptr, st));
+    unsigned long mask = 1ul << md->mp.vel_prop;
+    PD_TRY(cl_reorder(h, sort_cl, h->n_real, mask, true, true, st));
+    if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
+    PD_TRY(ghost_generate(h, 0, true, st));
+    if (md->mp.use_cell_list) {
+        PD_TRY(cl_build(h, md->cl, h->n_total, nullptr, st));
+    } else {
+        PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
+        PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    h->epoch++;
+    md->builds++;
+    return PD_OK;
+}
+
+static int md_forces(pd_md md, cudaStream_t st) {
+    return lj_launch(md->h, md->mp.use_cell_list ? nullptr : md->vl, md->mp.use_cell_list ? md->cl : nullptr, md->lj,
+                     md->mp.force_prop, md->fpart.as<double>(), md->nblk, st);
+}
+
+}  // namespace pd
+
+using namespace pd;
+
+extern "C" {
+
+int pd_lj_forces(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t* lj, int force_prop, void* stream,
+                 double* energy) {
+    if (!h || !lj || (!vl && !cl) || force_prop < 0 || force_prop >= (int)h->props.size()) return PD_EINVAL;
+    Prop& F = h->props[force_prop];
+    if (F.type != h->dtype || F.ncomp < 3) {
+        set_error("pd_lj_forces: force property must have 3 components of the vector's dtype");
+        return PD_EINVAL;
+    }
+    if (vl && vl->n_dom != h->n_real) {
+        set_error("pd_lj_forces: Verlet list is stale (update it after map/ghost_get)");
+        return PD_ESTALE;
+    }
+    if (!vl && cl->n_part != h->n_total) {
+        set_error("pd_lj_forces: cell list is stale");
+        return PD_ESTALE;
+    }
+    cudaStream_t st = S(stream);
+    int nblk = force_blocks(h->n_real);
+    PD_TRY(h->red.ensure(sizeof(double) * 2 * nblk));
+    if (h->n_real > 0) PD_TRY(lj_launch(h, vl, cl, *lj, force_prop, h->red.as<double>(), nblk, st));
+    if (energy) {
+        std::vector<double> part(2 * nblk, 0.0);
+        if (h->n_real > 0)
+            PD_CUDA(cudaMemcpyAsync(part.data(), h->red.p, sizeof(double) * 2 * nblk, cudaMemcpyDeviceToHost, st));
+        PD_CUDA(cudaStreamSynchronize(st));
+        energy[0] = energy[1] = 0;
+        for (int b = 0; b < nblk; ++b) {
+            energy[0] += part[2 * b];
+            energy[1] += part[2 * b + 1];
+        }
+    }
+    return PD_OK;
+}
+
+int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* mp, pd_md* out) {
+    if (!h || !lj || !mp || !out) return PD_EINVAL;
+    int np = (int)h->props.size();
+    if (mp->vel_prop < 0 || mp->vel_prop >= np || mp->force_prop < 0 || mp->force_prop >= np ||
+        mp->vel_prop == mp->force_prop) {
+        set_error("pd_md_create: bad property ids");
+        return PD_EINVAL;
+    }
+    if (h->props[mp->vel_prop].type != h->dtype || h->props[mp->vel_prop].ncomp != 3 ||
+        h->props[mp->force_prop].type != h->dtype || h->props[mp->force_prop].ncomp != 3) {
+        set_error("pd_md_create: velocity and force must be 3-component properties of the vector's dtype");
+        return PD_EINVAL;
+    }
+    if (!(mp->dt > 0) || !(mp->mass > 0) || !(lj->r_cut > 0) || !(lj->sigma > 0)) return PD_EINVAL;
+    double rlist = lj->r_cut + (mp->skin > 0 ? mp->skin : 0);
+    for (int d = 0; d < 3; ++d)
+        if (h->bc[d] == PD_PERIODIC && h->g[d] < rlist) {
+            set_error("pd_md_create: ghost %.6g in dimension %d is smaller than r_cut + skin %.6g", h->g[d], d, rlist);
+            return PD_EINVAL;
+        }
+    pd_md md = new pd_md_s();
+    md->h = h;
+    md->lj = *lj;
+    md->mp = *mp;
+    int r;
+    if (mp->use_cell_list) {
+        r = pd_celllist_create(h, lj->r_cut, PD_CL_NON_SYMMETRIC, 1, (double)1.013f, &md->cl);
+    } else {
+        r = pd_verlet_create(h, rlist, &md->vl);
+    }
+    if (r != PD_OK) {
+        delete md;
+        return r;
+    }
+    md->nblk = force_blocks(h->n_real);
+    if ((r = md->fpart.ensure(sizeof(double) * 2 * md->nblk)) != PD_OK ||
+        (r = md->kpart.ensure(sizeof(double) * md->nblk)) != PD_OK ||
+        (r = md->xb.ensure((size_t)(h->n_real > 0 ? h->n_real : 1) * h->pos_bytes)) != PD_OK) {
+        pd_md_destroy(md);
+        return r;
+    }
+    *out = md;
+    return PD_OK;
+}
+
+int pd_md_destroy(pd_md md) {
+    if (!md) return PD_EINVAL;
+    if (md->vl) pd_verlet_destroy(md->vl);
+    if (md->cl) pd_celllist_destroy(md->cl);
+    md->xb.release();
+    md->fpart.release();
+    md->kpart.release();
+    md->E.release();
+    for (int i = 0; i < 8; ++i)
+        if (md->ev[i]) cudaEventDestroy(md->ev[i]);
+    delete md;
+    return PD_OK;
+}
+
+int pd_md_run(pd_md md, int steps, void* stream, double* E) {
+    if (!md || steps < 0) return PD_EINVAL;
+    pd_vd h = md->h;
+    cudaStream_t st = S(stream);
+    long n = h->n_real;
+    PD_TRY(md->E.ensure(sizeof(double) * 4 * (steps + 1)));
+    Prop& V = h->props[md->mp.vel_prop];
+    Prop& F = h->props[md->mp.force_prop];
+    if (!md->ready) {
+        PD_TRY(md_rebuild(md, st));
+        PD_TRY(md_forces(md, st));
+        md->ready = true;
+    }
+    double half = 0.5 * md->mp.dt / md->mp.mass;
+    double lim = 0.5 * md->mp.skin;
+    double lim2 = lim * lim;
+    for (int s = 0; s < steps; ++s) {
+        unsigned int rebuilt = 0;
+        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[0], st));
+        PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
+        if (h->dtype == PD_F64)
+            pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,
+                                                              (const double*)F.d, h->cap, n, half, md->mp.dt,
+                                                              &h->ctrl->maxdisp2);
+        else
+            pd::launch(k_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos, md->xb.as<float4>(), (float*)V.d,
+                                                             (const float*)F.d, h->cap, n, (float)half,
+                                                             (float)md->mp.dt, &h->ctrl->maxdisp2);
+        PD_LAUNCH_CHECK();
+        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[1], st));
+        bool rb = md->mp.skin <= 0 || md->mp.use_cell_list;
+        if (!rb) {
+            PD_CUDA(cudaMemcpyAsync(&h->ctrl_h->maxdisp2, &h->ctrl->maxdisp2, sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st));
+            PD_CUDA(cudaStreamSynchronize(st));
+            double d2;
+            memcpy(&d2, &h->ctrl_h->maxdisp2, sizeof(double));
+            rb = d2 > lim2;
+        }
+        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[2], st));
+        if (rb) {
+            PD_TRY(md_rebuild(md, st));
+            rebuilt = 1;
+        } else {
+            PD_TRY(ghost_replay(h, 0ul, true, nullptr, h->n_img, st));
+        }
+        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[3], st));
+        PD_TRY(md_forces(md, st));
+        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[4], st));
+        if (h->dtype == PD_F64)
+            pd::launch(k_kick<double>, md->nblk, FBLOCK, 0, st, (double*)V.d, (const double*)F.d, h->cap, n, half,
+                                                        md->mp.mass, md->kpart.as<double>());
+        else
+            pd::launch(k_kick<float>, md->nblk, FBLOCK, 0, st, (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
+                                                       md->mp.mass, md->kpart.as<double>());
+        PD_LAUNCH_CHECK();
+        h->ctrl_h->rebuild = rebuilt;
+        PD_CUDA(cudaMemcpyAsync(&h->ctrl->rebuild, &h->ctrl_h->rebuild, sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+        pd::launch(k_energy, 1, 256, 0, st, md->fpart.as<double>(), md->kpart.as<double>(), md->nblk, &h->ctrl->rebuild,
+                                     md->E.as<double>() + 4 * s);
+        PD_LAUNCH_CHECK();
+        md->steps++;
+        if (md->timing) {
+            PD_CUDA(cudaEventRecord(md->ev[5], st));
+            PD_CUDA(cudaEventSynchronize(md->ev[5]));
+            float a = 0, b = 0, c = 0, d = 0;
+            cudaEventElapsedTime(&a, md->ev[0], md->ev[1]);
+            cudaEventElapsedTime(&b, md->ev[2], md->ev[3]);
+            cudaEventElapsedTime(&c, md->ev[3], md->ev[4]);
+            cudaEventElapsedTime(&d, md->ev[4], md->ev[5]);
+            md->ms[0] += a + d;
+            md->cnt[0] += 1;
+            md->ms[rebuilt ? 1 : 2] += b;
+            md->cnt[rebuilt ? 1 : 2] += 1;
+            md->ms[3] += c;
+            md->cnt[3] += 1;
+        }
+    }
+    if (E && steps > 0) {
+        PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));
+    }
+    PD_CUDA(cudaStreamSynchronize(st));
+    PD_TRY(read_ctrl(h, st));
+    if (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW)) {
+        set_error("pd_md_run: device capacity overflow (err=0x%x)", h->ctrl_h->err);
+        return PD_EOVERFLOW;
+    }
+    return PD_OK;
+}
+
+int pd_md_set_timing(pd_md md, int on) {
+    if (!md) return PD_EINVAL;
+    if (on && !md->ev[0])
+        for (int i = 0; i < 8; ++i) PD_CUDA(cudaEventCreate(&md->ev[i]));
+    md->timing = on != 0;
+    for (int i = 0; i < 4; ++i) {
+        md->ms[i] = 0;
+        md->cnt[i] = 0;
+    }
+    return PD_OK;
+}
+
+int pd_md_timers(pd_md md, double* ms, long* counts) {
+    if (!md || !ms || !counts) return PD_EINVAL;
+    for (int i = 0; i < 4; ++i) {
+        ms[i] = md->ms[i];
+        counts[i] = md->cnt[i];
+    }
+    return PD_OK;
+}
+
+int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn) {
+    if (!md || !n_dom || !mean_nn || !max_nn) return PD_EINVAL;
+    *n_dom = 0;
+    *mean_nn = 0;
+    *max_nn = 0;
+    if (!md->vl || md->vl->n_dom == 0) return PD_OK;
+    std::vector<int> c(md->vl->n_dom);
+    PD_CUDA(cudaMemcpy(c.data(), md->vl->nn.p, sizeof(int) * c.size(), cudaMemcpyDeviceToHost));
+    double s = 0;
+    int m = 0;
+    for (int x : c) {
+        s += x;
+        m = std::max(m, x);
+    }
+    *n_dom = (long)c.size();
+    *mean_nn = s / (double)c.size();
+    *max_nn = m;
+    return PD_OK;
+}
+
+int pd_md_stats(pd_md md, long* builds, long* steps, int* err) {
+    if (!md) return PD_EINVAL;
+    if (builds) *builds = md->builds;
+    if (steps) *steps = md->steps;
+    if (err) {
+        PD_TRY(read_ctrl(md->h, 0));
+        *err = (int)md->h->ctrl_h->err;
+    }
+    return PD_OK;
+}
+
+}  // extern "C"

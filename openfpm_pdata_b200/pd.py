@@ -1,0 +1,405 @@
+"""ctypes binding of libpdgpu.so, mirroring the reference's vector_dist GPU API.
+
+Names follow the reference (Vector/vector_dist.hpp): ``map``,
+``ghost_get``, ``getCellListGPU``, ``updateCellListGPU``, ``restoreOrder``,
+``getVerlet``, ``updateVerlet``, ``getDomainIteratorGPU``, ``toKernel``,
+``hostToDevicePos`` / ``deviceToHostPos`` and the property variants.  Errors
+raise ``PdError`` carrying the library's message, like the reference's
+ACTION_ON_ERROR.  There is no CPU fallback: importing this module on a host
+without the built library raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpdgpu.so")
+
+PD_F32, PD_F64, PD_I32, PD_U32, PD_I64 = 1, 2, 3, 4, 5
+NON_PERIODIC, PERIODIC = 0, 1
+NO_POSITION, WITH_POSITION, NO_CHANGE_ELEMENTS = 1, 2, 4
+SKIP_LABELLING = KEEP_PROPERTIES = 512
+RUN_ON_DEVICE = 1024
+CL_NON_SYMMETRIC = 2
+CL_GPU_REORDER_POSITION, CL_GPU_REORDER_PROPERTY = 64, 128
+CL_GPU_REORDER = CL_GPU_REORDER_POSITION | CL_GPU_REORDER_PROPERTY
+RED_ADD, RED_MAX = 1, 2
+
+_NP = {PD_F32: np.float32, PD_F64: np.float64, PD_I32: np.int32, PD_U32: np.uint32, PD_I64: np.int64}
+_CODES = {-1: "PD_EINVAL", -2: "PD_ENOMEM", -3: "PD_ECUDA", -4: "PD_ESTALE", -5: "PD_ETIMEOUT",
+          -6: "PD_EOVERFLOW", -7: "PD_ESTATE"}
+
+
+class PdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class View(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_void_p), ("prop", ctypes.c_void_p * 16), ("prop_type", ctypes.c_int * 16),
+                ("prop_ncomp", ctypes.c_int * 16), ("n_prop", ctypes.c_int), ("dtype", ctypes.c_int),
+                ("stride", ctypes.c_long), ("size_local", ctypes.c_long), ("size", ctypes.c_long),
+                ("epoch", ctypes.c_long)]
+
+
+class CLView(ctypes.Structure):
+    _fields_ = [("cell_start", ctypes.c_void_p), ("sorted_ids", ctypes.c_void_p), ("dom_sort_ids", ctypes.c_void_p),
+                ("ncells", ctypes.c_long), ("gs", ctypes.c_int * 3), ("div", ctypes.c_int * 3),
+                ("pad", ctypes.c_int), ("nn_box", ctypes.c_int), ("box_lo", ctypes.c_double * 3),
+                ("spacing", ctypes.c_double * 3), ("ghost_marker", ctypes.c_long), ("n_part", ctypes.c_long)]
+
+
+class Launch(ctypes.Structure):
+    _fields_ = [("wthr", ctypes.c_uint * 3), ("thr", ctypes.c_uint * 3)]
+
+
+class LJParams(ctypes.Structure):
+    _fields_ = [("eps", ctypes.c_double), ("sigma", ctypes.c_double), ("r_cut", ctypes.c_double)]
+
+
+class MDParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("mass", ctypes.c_double), ("skin", ctypes.c_double),
+                ("vel_prop", ctypes.c_int), ("force_prop", ctypes.c_int), ("use_cell_list", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libpdgpu.so; raises if it was not built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                              "(make -C openfpm_pdata_b200/csrc)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, lp, ip, dp = ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+        P = ctypes.POINTER
+        sig = {
+            "pd_last_error": ([], ctypes.c_char_p),
+            "pd_device_info": ([P(ctypes.c_int), P(ctypes.c_long), P(ctypes.c_long)], ip),
+            "pd_create": ([ip, ip, lp, dp, dp, P(ctypes.c_int), dp, ip, P(vp)], ip),
+            "pd_destroy": ([vp], ip),
+            "pd_add_prop": ([vp, ip, ip, P(ctypes.c_int)], ip),
+            "pd_size": ([vp, P(ctypes.c_long), P(ctypes.c_long)], ip),
+            "pd_resize": ([vp, lp], ip),
+            "pd_h2d_pos": ([vp, vp, lp, lp, vp], ip),
+            "pd_d2h_pos": ([vp, vp, lp, lp, vp], ip),
+            "pd_h2d_prop": ([vp, ip, vp, lp, lp, vp], ip),
+            "pd_d2h_prop": ([vp, ip, vp, lp, lp, vp], ip),
+            "pd_map": ([vp, ip, vp], ip),
+            "pd_ghost_get": ([vp, ctypes.c_ulong, ip, vp], ip),
+            "pd_ghost_records": ([vp, vp, vp, lp, P(ctypes.c_long)], ip),
+            "pd_ghost_count_boxes": ([vp, vp, vp, ip, vp, vp], ip),
+            "pd_ghost_get_boxes": ([vp, vp, vp, ip, vp, ip, vp], ip),
+            "pd_view": ([vp, P(View)], ip),
+            "pd_domain_iterator": ([vp, ip, ip, P(Launch)], ip),
+            "pd_reduce": ([vp, ip, ip, ip, vp, dp], ip),
+            "pd_d2h_gid": ([vp, vp, lp, lp, vp], ip),
+            "pd_celllist_create": ([vp, ctypes.c_double, ip, ip, ctypes.c_double, P(vp)], ip),
+            "pd_celllist_destroy": ([vp], ip),
+            "pd_celllist_update": ([vp, vp, ctypes.c_ulong, vp], ip),
+            "pd_restore_order": ([vp, vp, ctypes.c_ulong, vp], ip),
+            "pd_celllist_view": ([vp, P(CLView)], ip),
+            "pd_celllist_get": ([vp, vp, vp, vp], ip),
+            "pd_test_force": ([vp, vp, ip, ip, ip, vp], ip),
+            "pd_verlet_create": ([vp, ctypes.c_double, P(vp)], ip),
+            "pd_verlet_destroy": ([vp], ip),
+            "pd_verlet_update": ([vp, vp, vp], ip),
+            "pd_verlet_get": ([vp, vp, vp, lp, vp], ip),
+            "pd_lj_forces": ([vp, vp, vp, P(LJParams), ip, vp, dp], ip),
+            "pd_md_create": ([vp, P(LJParams), P(MDParams), P(vp)], ip),
+            "pd_md_destroy": ([vp], ip),
+            "pd_md_run": ([vp, ip, vp, vp], ip),
+            "pd_md_stats": ([vp, P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_int)], ip),
+            "pd_md_set_timing": ([vp, ip], ip),
+            "pd_md_timers": ([vp, P(ctypes.c_double), P(ctypes.c_long)], ip),
+            "pd_launch_count": ([], ctypes.c_ulonglong),
+            "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise PdError(rc, lib().pd_last_error().decode(errors="replace"))
+    return rc
+
+
+def _d3(x):
+    a = (ctypes.c_double * 3)(*[float(v) for v in np.broadcast_to(np.asarray(x, dtype=np.float64), (3,))])
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def launch_count():
+    """Kernels launched by libpdgpu.so so far."""
+    return int(lib().pd_launch_count())
+
+
+def device_info():
+    sm, fr, tot = ctypes.c_int(0), ctypes.c_long(0), ctypes.c_long(0)
+    check(lib().pd_device_info(ctypes.byref(sm), ctypes.byref(fr), ctypes.byref(tot)))
+    return sm.value, fr.value, tot.value
+
+
+class CellList:
+    """CellList_gpu handle (getCellListGPU / updateCellListGPU / restoreOrder)."""
+
+    def __init__(self, vd, r_cut, opt=CL_NON_SYMMETRIC, nn_box=1, enlarge=None):
+        self.vd = vd
+        h = ctypes.c_void_p()
+        enl = float(np.float32(1.013)) if enlarge is None else float(enlarge)
+        check(lib().pd_celllist_create(vd.h, float(r_cut), int(opt), int(nn_box), enl, ctypes.byref(h)))
+        self.h = h
+
+    def view(self):
+        v = CLView()
+        check(lib().pd_celllist_view(self.h, ctypes.byref(v)))
+        return v
+
+    def get(self):
+        """(cell_start[ncells+1], sorted_ids[n]) on the host."""
+        v = self.view()
+        cs = np.zeros(v.ncells + 1, np.int32)
+        so = np.zeros(max(v.n_part, 1), np.int32)
+        check(lib().pd_celllist_get(self.h, _ptr(cs), _ptr(so), None))
+        return cs, so[: v.n_part]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pd_celllist_destroy(self.h)
+            self.h = None
+
+
+class VerletList:
+    """VerletList handle (getVerlet / updateVerlet)."""
+
+    def __init__(self, vd, r_cut):
+        self.vd = vd
+        h = ctypes.c_void_p()
+        check(lib().pd_verlet_create(vd.h, float(r_cut), ctypes.byref(h)))
+        self.h = h
+
+    def get(self):
+        """CSR (offsets[n+1], idx) of the list on the host."""
+        n = self.vd.size_local()
+        counts = np.zeros(max(n, 1), np.int32)
+        check(lib().pd_verlet_get(self.h, _ptr(counts), None, 0, None))
+        counts = counts[:n]
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum(counts)
+        idx = np.zeros(max(int(off[-1]), 1), np.int32)
+        check(lib().pd_verlet_get(self.h, _ptr(counts), _ptr(idx), int(idx.shape[0]), None))
+        return off, idx[: off[-1]]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pd_verlet_destroy(self.h)
+            self.h = None
+
+
+class VectorDist:
+    """vector_dist_gpu<3, St, aggregate<...>> on one GPU.
+
+    ``props`` is a list of (type, ncomp) with type in PD_F32/PD_F64/PD_I32/PD_U32/PD_I64.
+    """
+
+    def __init__(self, n, lo, hi, bc, ghost, dtype=np.float64, props=()):
+        self.dtype = np.dtype(dtype)
+        code = PD_F64 if self.dtype == np.float64 else PD_F32
+        bcs = (ctypes.c_int * 3)(*[int(b) for b in np.broadcast_to(np.asarray(bc), (3,))])
+        h = ctypes.c_void_p()
+        check(lib().pd_create(3, code, int(n), _d3(lo), _d3(hi), bcs, _d3(ghost), 0, ctypes.byref(h)))
+        self.h = h
+        self.props = []
+        for t, nc in props:
+            self.add_prop(t, nc)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pd_destroy(self.h)
+            self.h = None
+
+    def add_prop(self, t, ncomp):
+        pid = ctypes.c_int(-1)
+        check(lib().pd_add_prop(self.h, int(t), int(ncomp), ctypes.byref(pid)))
+        self.props.append((t, ncomp))
+        return pid.value
+
+    def size_local(self):
+        a, b = ctypes.c_long(0), ctypes.c_long(0)
+        check(lib().pd_size(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value
+
+    def size_local_with_ghost(self):
+        a, b = ctypes.c_long(0), ctypes.c_long(0)
+        check(lib().pd_size(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return b.value
+
+    def resize(self, n):
+        check(lib().pd_resize(self.h, int(n)))
+
+    # -- host <-> device
+    def hostToDevicePos(self, x, offset=0):
+        x = np.ascontiguousarray(x, dtype=self.dtype).reshape(-1, 3)
+        check(lib().pd_h2d_pos(self.h, _ptr(x), int(offset), int(x.shape[0]), None))
+
+    def deviceToHostPos(self, offset=0, count=None, with_ghost=True):
+        n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
+        out = np.zeros((n, 3), self.dtype)
+        if n:
+            check(lib().pd_d2h_pos(self.h, _ptr(out), int(offset), int(n), None))
+        return out
+
+    def hostToDeviceProp(self, p, a, offset=0):
+        t, nc = self.props[p]
+        a = np.asarray(a, dtype=_NP[t]).reshape(-1, nc)
+        cm = np.ascontiguousarray(a.T)
+        check(lib().pd_h2d_prop(self.h, int(p), _ptr(cm), int(offset), int(a.shape[0]), None))
+
+    def deviceToHostProp(self, p, offset=0, count=None, with_ghost=True):
+        t, nc = self.props[p]
+        n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
+        cm = np.zeros((nc, n), _NP[t])
+        if n:
+            check(lib().pd_d2h_prop(self.h, int(p), _ptr(cm), int(offset), int(n), None))
+        return cm.T.copy() if nc > 1 else cm[0].copy()
+
+    def gid(self, with_ghost=True):
+        n = self.size_local_with_ghost() if with_ghost else self.size_local()
+        out = np.zeros(max(n, 1), np.int64)
+        check(lib().pd_d2h_gid(self.h, _ptr(out), 0, int(n), None))
+        return out[:n]
+
+    # -- reference API
+    def map(self, opt=RUN_ON_DEVICE):
+        check(lib().pd_map(self.h, int(opt), None))
+
+    def ghost_get(self, props=None, opt=RUN_ON_DEVICE):
+        mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
+        check(lib().pd_ghost_get(self.h, ctypes.c_ulong(mask), int(opt), None))
+
+    def ghost_records(self):
+        n = ctypes.c_long(0)
+        check(lib().pd_ghost_records(self.h, None, None, 0, ctypes.byref(n)))
+        m = n.value
+        src = np.zeros(max(m, 1), np.int32)
+        shf = np.zeros(max(m, 1), np.int32)
+        check(lib().pd_ghost_records(self.h, _ptr(src), _ptr(shf), m, ctypes.byref(n)))
+        return src[:m], shf[:m]
+
+    def ghost_count_boxes(self, blo, bhi, sv):
+        nb = len(sv)
+        boxes = np.ascontiguousarray(np.concatenate([np.asarray(blo, np.float64).reshape(nb, 3),
+                                                     np.asarray(bhi, np.float64).reshape(nb, 3)], axis=1))
+        svv = np.ascontiguousarray(sv, np.int32)
+        out = np.zeros(max(self.size_local(), 1), np.int32)
+        check(lib().pd_ghost_count_boxes(self.h, _ptr(boxes), _ptr(svv), nb, _ptr(out), None))
+        return out[: self.size_local()]
+
+    def ghost_get_boxes(self, blo, bhi, sv, shifts):
+        nb = len(sv)
+        boxes = np.ascontiguousarray(np.concatenate([np.asarray(blo, np.float64).reshape(nb, 3),
+                                                     np.asarray(bhi, np.float64).reshape(nb, 3)], axis=1))
+        svv = np.ascontiguousarray(sv, np.int32)
+        sh = np.ascontiguousarray(shifts, np.float64).reshape(-1, 3)
+        check(lib().pd_ghost_get_boxes(self.h, _ptr(boxes), _ptr(svv), nb, _ptr(sh), sh.shape[0], None))
+
+    def toKernel(self):
+        v = View()
+        check(lib().pd_view(self.h, ctypes.byref(v)))
+        return v
+
+    def getDomainIteratorGPU(self, n_thr=1024, with_ghost=False):
+        it = Launch()
+        check(lib().pd_domain_iterator(self.h, int(n_thr), int(with_ghost), ctypes.byref(it)))
+        return it
+
+    def reduce_local(self, p, comp=0, op=RED_ADD):
+        out = ctypes.c_double(0)
+        check(lib().pd_reduce(self.h, int(p), int(comp), int(op), None, ctypes.byref(out)))
+        return out.value
+
+    def getCellListGPU(self, r_cut, opt=CL_NON_SYMMETRIC, NNIteratorBox=1, ghostEnlargeFactor=None):
+        return CellList(self, r_cut, opt, NNIteratorBox, ghostEnlargeFactor)
+
+    def updateCellListGPU(self, cl, props=None):
+        mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
+        check(lib().pd_celllist_update(self.h, cl.h, ctypes.c_ulong(mask), None))
+
+    def restoreOrder(self, cl, props=None):
+        mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
+        check(lib().pd_restore_order(self.h, cl.h, ctypes.c_ulong(mask), None))
+
+    def getVerlet(self, r_cut):
+        vl = VerletList(self, r_cut)
+        check(lib().pd_verlet_update(self.h, vl.h, None))
+        return vl
+
+    def updateVerlet(self, vl):
+        check(lib().pd_verlet_update(self.h, vl.h, None))
+
+    def test_force(self, cl, in_prop, out_prop, sorted=False):
+        check(lib().pd_test_force(self.h, cl.h, int(in_prop), int(out_prop), int(bool(sorted)), None))
+
+    def lj_forces(self, force_prop, vl=None, cl=None, eps=1.0, sigma=1.0, r_cut=2.5):
+        p = LJParams(eps, sigma, r_cut)
+        e = (ctypes.c_double * 2)()
+        check(lib().pd_lj_forces(self.h, vl.h if vl else None, cl.h if cl else None, ctypes.byref(p),
+                                 int(force_prop), None, e))
+        return e[0], e[1]
+
+
+class MD:
+    """Velocity-Verlet LJ driver over a VectorDist holding only real particles."""
+
+    def __init__(self, vd, vel_prop, force_prop, dt=0.005, mass=1.0, skin=0.3, eps=1.0, sigma=1.0, r_cut=2.5,
+                 use_cell_list=False):
+        self.vd = vd
+        self.lj = LJParams(eps, sigma, r_cut)
+        self.mp = MDParams(dt, mass, skin, vel_prop, force_prop, int(bool(use_cell_list)))
+        h = ctypes.c_void_p()
+        check(lib().pd_md_create(vd.h, ctypes.byref(self.lj), ctypes.byref(self.mp), ctypes.byref(h)))
+        self.h = h
+
+    def run(self, steps, energies=True):
+        E = np.zeros((max(steps, 1), 4)) if energies else None
+        check(lib().pd_md_run(self.h, int(steps), None, _ptr(E) if energies else None))
+        return E[:steps] if energies else None
+
+    def set_timing(self, on=True):
+        check(lib().pd_md_set_timing(self.h, int(bool(on))))
+
+    def timers(self):
+        """{phase: (total ms, count)} for integrate, rebuild, images, force."""
+        ms = (ctypes.c_double * 4)()
+        cnt = (ctypes.c_long * 4)()
+        check(lib().pd_md_timers(self.h, ms, cnt))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(("integrate", "rebuild", "images", "force"))}
+
+    def list_stats(self):
+        """(domain particles, mean Verlet row length, longest row) of the last build."""
+        n, m, x = ctypes.c_long(0), ctypes.c_double(0), ctypes.c_int(0)
+        check(lib().pd_md_list_stats(self.h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(x)))
+        return n.value, m.value, x.value
+
+    def stats(self):
+        b, s, e = ctypes.c_long(0), ctypes.c_long(0), ctypes.c_int(0)
+        check(lib().pd_md_stats(self.h, ctypes.byref(b), ctypes.byref(s), ctypes.byref(e)))
+        return b.value, s.value, e.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pd_md_destroy(self.h)
+            self.h = None

@@ -557,9 +557,17 @@ template <class T> static void md_refresh_images(MDState<T>& S) {
             S.pos[3 * (n + k) + d] = S.pos[3 * (long)S.src[k] + d] - S.shifts[3 * S.shf[k] + d];
 }
 
+static double wtime() {
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
+
 template <class T>
 static int md_lj_impl(T* x, T* v, long n, const T* lo, const T* hi, const int* bc, const T* ghost, T rc, T skin,
-                      T eps, T sigma, T dt, T mass, int steps, double* E) {
+                      T eps, T sigma, T dt, T mass, int steps, double* E, double* t_loop) {
     MDState<T> S;
     S.n = n;
     S.lo = lo;
@@ -595,6 +603,7 @@ static int md_lj_impl(T* x, T* v, long n, const T* lo, const T* hi, const int* b
     record(0, 1);
     T half = T(0.5) * dt / mass;
     T lim2 = (T(0.5) * skin) * (T(0.5) * skin);
+    double t0 = wtime();
     for (int s = 1; s <= steps; ++s) {
         T mx = 0;
 #pragma omp parallel for schedule(static) reduction(max : mx)
@@ -622,6 +631,7 @@ static int md_lj_impl(T* x, T* v, long n, const T* lo, const T* hi, const int* b
             for (int d = 0; d < 3; ++d) v[3 * i + d] += half * f[3 * i + d];
         record(s, rebuilt);
     }
+    if (t_loop) *t_loop = wtime() - t0;
     std::copy(S.pos.begin(), S.pos.begin() + 3 * n, x);
     return 0;
 }
@@ -825,8 +835,9 @@ void or_sph_rates_d(const double* pos, const double* vel, const double* rho, con
 
 // -- MD driver
 int or_md_lj_d(double* x, double* v, long n, const double* lo, const double* hi, const int* bc, const double* ghost,
-               double rc, double skin, double eps, double sigma, double dt, double mass, int steps, double* E) {
-    return md_lj_impl(x, v, n, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps, E);
+               double rc, double skin, double eps, double sigma, double dt, double mass, int steps, double* E,
+               double* t_loop) {
+    return md_lj_impl(x, v, n, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps, E, t_loop);
 }
 
 int or_num_threads() {

@@ -60,7 +60,8 @@ def lib():
         L.or_lj_verlet_d.argtypes = [_dp, _L, _lp, _lp, _ip, _D, _D, _D, _dp, _dp, _dp]
         L.or_lj_cell_d.argtypes = [_dp, _L, _L, _dp, _dp, _ip, _I, _D, _D, _D, _dp, _dp, _dp]
         L.or_sph_rates_d.argtypes = [_dp, _dp, _dp, _ip, _L, _lp, _lp, _ip, _D, _D, _D, _D, _D, _D, _dp, _dp]
-        L.or_md_lj_d.argtypes = [_dp, _dp, _L, _dp, _dp, _ip, _dp, _D, _D, _D, _D, _D, _D, _I, _dp]
+        L.or_md_lj_d.argtypes = [_dp, _dp, _L, _dp, _dp, _ip, _dp, _D, _D, _D, _D, _D, _D, _I, _dp,
+                                 ctypes.POINTER(ctypes.c_double)]
         L.or_md_lj_d.restype = _I
         L.or_num_threads.restype = _I
         L.or_set_threads.argtypes = [_I]
@@ -254,13 +255,15 @@ def sph_rates(pos, vel, rho, typ, off, idx, h, m, c0, rho0, alpha, gz):
     return acc, drho
 
 
-def md_lj(x, v, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps):
-    """Velocity-Verlet LJ MD with a skin Verlet list; returns (x, v, E[steps+1, 4])."""
+def md_lj(x, v, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps, timing=False):
+    """Velocity-Verlet LJ MD with a skin Verlet list; returns (x, v, E[steps+1, 4])
+    (and the wall time of the step loop, excluding the initial build, if timing)."""
     x = _a(x, np.float64).copy()
     v = _a(v, np.float64).copy()
     E = np.zeros((steps + 1, 4))
     g = np.broadcast_to(np.asarray(ghost, np.float64), (3,))
+    t = ctypes.c_double(0.0)
     rc_ = lib().or_md_lj_d(x, v, x.shape[0], _a(lo, np.float64), _a(hi, np.float64), _a(bc, np.int32),
-                           _a(g, np.float64), rc, skin, eps, sigma, dt, mass, steps, E)
+                           _a(g, np.float64), rc, skin, eps, sigma, dt, mass, steps, E, ctypes.byref(t))
     assert rc_ == 0
-    return x, v, E
+    return (x, v, E, t.value) if timing else (x, v, E)
