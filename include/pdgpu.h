@@ -191,6 +191,22 @@ int pd_celllist_get(pd_cl cl, int* cell_start, int* sorted_ids, void* stream);
  * out_prop(p) = sum over getNNIteratorBox q != p of in_prop(q)*(xq-xp)/|xq-xp| */
 int pd_test_force(pd_vd h, pd_cl cl, int in_prop, int out_prop, int sorted, void* stream);
 
+/* No counterpart in the reference.  The counting sort of pd_celllist_update for
+ * callers that cannot allocate device memory: code that runs while a CUDA graph
+ * is being captured, hosts whose device memory belongs to their own pool, and
+ * callers that must not let cudaMalloc/cudaFree synchronise the device.  It
+ * calls no allocator; its only scratch is a fixed static device array (about
+ * 8.4 MB, held on every GPU that loads the library until exit).  Inputs and
+ * outputs are caller-owned device buffers: pos_xyz [n][3] in dtype, cell_start
+ * [gs0*gs1*gs2 + 1], sorted_ids [n]; the results equal pd_celllist_update's
+ * for the same positions and grid (box_lo, spacing, gs including `pad`
+ * padding layers).  Limits: n <= 524288 particles and gs0*gs1*gs2 <= 524288
+ * cells, else PD_EINVAL.  The first call on each device looks up the scratch
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the scratch: calls that overlap on the GPU race. */
+int pd_celllist_build_static(int dtype, const void* pos_xyz, long n, const double* box_lo, const double* spacing,
+                             const int* gs, int pad, int* cell_start, int* sorted_ids, void* stream);
+
 /* ---- Verlet list -------------------------------------------------------- */
 /* getVerlet(r_cut) -- vector_dist.hpp:1514-1547: full list of every domain particle
  * over domain + ghost within r_cut (self included), built from a cell list of

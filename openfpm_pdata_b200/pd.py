@@ -118,6 +118,7 @@ def lib():
             "pd_md_timers": ([vp, P(ctypes.c_double), P(ctypes.c_long)], ip),
             "pd_launch_count": ([], ctypes.c_ulonglong),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
+            "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
