@@ -113,6 +113,9 @@ def make_workload():
     return x, v, L
 
 
+TUNE = {"tiles": 1, "tx": 0, "tpp": 0}
+
+
 def build_system(pd, x, v, L):
     lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
     vd = pd.VectorDist(x.shape[0], lo, hi, bc, R_CUT + SKIN, dtype=np.float64,
@@ -120,6 +123,7 @@ def build_system(pd, x, v, L):
     vd.hostToDevicePos(x)
     vd.hostToDeviceProp(0, v)
     md = pd.MD(vd, 0, 1, dt=DT, mass=MASS, skin=SKIN, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+    md.set_tiles(bool(TUNE["tiles"]), TUNE["tx"], TUNE["tpp"])
     return vd, md
 
 
@@ -151,7 +155,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tiles", type=int, default=1, help="1: tiled shared-memory rows, 0: global-index rows")
+    ap.add_argument("--tx", type=int, default=0, help="cells per tile along x (0: automatic)")
+    ap.add_argument("--tpp", type=int, default=0, help="threads per particle in the pair kernel (0: 2)")
     a = ap.parse_args()
+    TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp)
     if a.warmup < 3:
         a.warmup = 3
     world, rank, local = dist_setup(a.gpus)
@@ -223,7 +231,8 @@ def main():
     # = N * (32 B position record + 4 B row length + 4 B * mean row + 24 B force)
     f_ms, f_cnt = timers["force"]
     f_avg_s = f_ms / max(f_cnt, 1) / 1000.0
-    alg_bytes = n * (32 + 4 + 4 * mean_nn + 24)
+    # tiled rows: 2-byte entries, the position record is staged once per tile (counted once)
+    alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
     traffic = read_traffic()
@@ -237,7 +246,8 @@ def main():
                    "list_rebuilds_in_timed_region": builds, "mean_verlet_row": round(mean_nn, 2),
                    "max_verlet_row": max_nn},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_lj_verlet<double>", "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "k_vtile_lj<double>" if a.tiles else "k_lj_verlet<double>",
+                     "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0},
         "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in timers.items()},
         "gpu_launches": int(launches),

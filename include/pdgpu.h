@@ -224,6 +224,10 @@ int pd_verlet_get(pd_vl vl, int* counts, int* idx, long idx_cap, void* stream);
 int pd_lj_forces(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t* lj, int force_prop, void* stream,
                  double* energy);
 
+/* the reciprocal used by the pair kernels (Newton-Raphson on the hardware
+ * approximation), evaluated on n host values -- a self-test of its error bound */
+int pd_selftest_recip(int dtype, const void* x_host, void* out_host, long n);
+
 /* ---- velocity-Verlet LJ driver ------------------------------------------ */
 /* Binds a vector holding real particles (no ghost) to an integrator that keeps
  * the particles in cell order, periodic images and a skin Verlet list on the
@@ -238,6 +242,13 @@ int pd_md_stats(pd_md md, long* builds, long* steps, int* err);
 /* per-phase device time (CUDA events on the run's stream, one synchronisation per
  * step while enabled): ms/counts[4] = integrate, rebuild, image refresh, force */
 int pd_md_set_timing(pd_md md, int on);
+/* neighbour structure of the driver: tiled shared-memory rows (on, default) or
+ * global-index rows; tx = cells per tile along x (0 = from the mean occupancy),
+ * threads_per_particle = 1, 2 or 4 lanes sharing one row (0 = 2) */
+int pd_md_set_tiles(pd_md md, int on, int tx, int threads_per_particle);
+/* the driver's Verlet rows as CSR of global particle indices (current storage
+ * order: real particles then images); *tiled tells which structure is active */
+int pd_md_verlet_get(pd_md md, int* counts, int* idx, long idx_cap, int* tiled);
 /* Verlet rows of the last build: domain particles, mean and longest row */
 int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn);
 int pd_md_timers(pd_md md, double* ms, long* counts);

@@ -130,7 +130,7 @@ __global__ void k_cl_stabilise(long ncells, const unsigned int* __restrict__ sta
     }
 }
 
-int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st) {
+int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st, long first) {
     // n_part: exact count, or (with n_part_dev) an upper bound; the device count is *n_part_dev + n_real
     long nc = cl->ncells;
     PD_TRY(cl->cell_cnt.ensure(sizeof(unsigned int) * (nc + 1)));
@@ -145,12 +145,12 @@ int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cud
     if (n_part > 0) {
         unsigned g = grid_for(n_part, 256);
         if (h->dtype == PD_F64)
-            pd::launch(k_cl_hash<double>, g, 256, 0, st, (const double4*)h->pos, n_part, n_part_dev, n_add,
+            pd::launch(k_cl_hash<double>, g, 256, 0, st, (const double4*)h->pos + first, n_part, n_part_dev, n_add,
                                                  make_grid<double>(cl), cl->cell_cnt.as<unsigned int>(),
                                                  cl->cell_of.as<unsigned int>(), cl->slot.as<unsigned int>(),
                                                  &h->ctrl->err);
         else
-            pd::launch(k_cl_hash<float>, g, 256, 0, st, (const float4*)h->pos, n_part, n_part_dev, n_add,
+            pd::launch(k_cl_hash<float>, g, 256, 0, st, (const float4*)h->pos + first, n_part, n_part_dev, n_add,
                                                 make_grid<float>(cl), cl->cell_cnt.as<unsigned int>(),
                                                 cl->cell_of.as<unsigned int>(), cl->slot.as<unsigned int>(),
                                                 &h->ctrl->err);
@@ -238,6 +238,21 @@ static int permute(pd_vd h, const int* ids, long n, unsigned long prop_mask, boo
             PD_CUDA(cudaMemcpyAsync(base, h->tmp2.p, (size_t)n * P.esize, cudaMemcpyDeviceToDevice, st));
         }
     }
+    return PD_OK;
+}
+
+int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, cudaStream_t st) {
+    if (n <= 0) return PD_OK;
+    unsigned g = grid_for(n, 256);
+    switch (esize) {
+        case 1: pd::launch(k_gather<unsigned char>, g, 256, 0, st, (const unsigned char*)src, (unsigned char*)dst, ids, n); break;
+        case 4: pd::launch(k_gather<int>, g, 256, 0, st, (const int*)src, (int*)dst, ids, n); break;
+        case 8: pd::launch(k_gather<long long>, g, 256, 0, st, (const long long*)src, (long long*)dst, ids, n); break;
+        case 16: pd::launch(k_gather4<float>, g, 256, 0, st, (const float4*)src, (float4*)dst, ids, n); break;
+        case 32: pd::launch(k_gather4<double>, g, 256, 0, st, (const double4*)src, (double4*)dst, ids, n); break;
+        default: set_error("gather_bytes: element size %d", esize); return PD_EINVAL;
+    }
+    PD_LAUNCH_CHECK();
     return PD_OK;
 }
 

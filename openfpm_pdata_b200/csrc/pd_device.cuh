@@ -113,4 +113,41 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double 
     atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 
+// ---------------------------------------------------------------------------
+// 1-D bulk copies global -> shared through the TMA engine (cp.async.bulk, no
+// tensor map, no multicast) completing on an mbarrier.  Addresses and sizes must
+// be multiples of 16 bytes (positions are 16- or 32-byte records).
+__device__ __forceinline__ unsigned int smem_u32(const void* p) {
+    return static_cast<unsigned int>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned int bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned int bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned int phase) {
+    unsigned int ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0u;
+}
+// bounded wait on phase `phase`; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned int phase, unsigned int limit) {
+    for (unsigned int it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
 }  // namespace pd

@@ -38,6 +38,8 @@ enum : unsigned int {
     ERR_NN_OVERFLOW = 2u,   // a Verlet row longer than the list capacity
     ERR_CELL_RANGE = 4u,    // a particle outside the cell grid (clamped)
     ERR_CAP_OVERFLOW = 8u,  // real + images beyond the particle capacity
+    ERR_TIMEOUT = 16u,      // a bounded wait on a bulk copy gave up
+    ERR_TILE_CAP = 32u,     // a tile's staged neighbourhood exceeded the shared-memory capacity
 };
 
 // Control block resident in device memory: sizes that change on the device and
@@ -50,6 +52,8 @@ struct Ctrl {
     unsigned long long maxdisp2; // bits of the largest squared displacement (non-negative double)
     unsigned long long steps;
     unsigned long long builds;
+    unsigned int tile_max;         // largest staged neighbourhood of a tile (records)
+    unsigned int tile_center_max;  // largest number of domain particles of a tile
 };
 
 // Growable device buffer
@@ -161,7 +165,10 @@ int ensure_capacity(pd_vd h, long need, cudaStream_t st);
 int set_ctrl_n_img(pd_vd h, long n_img, cudaStream_t st);
 int read_ctrl(pd_vd h, cudaStream_t st);
 int cl_geometry(pd_cl cl, pd_vd h, double r_cut, double enlarge, int nn_box);
-int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st);
+// counting sort of the particles [first, first + n_part) (ids relative to `first`)
+int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st, long first = 0);
+// gather src[ids[k]] -> dst[k] for k < n of 4/8/16/32-byte elements (dst may not alias src)
+int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, cudaStream_t st);
 int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
                cudaStream_t st);
 int ghost_boxes_upload(pd_vd h, cudaStream_t st);

@@ -1,0 +1,49 @@
+// pd_lj.cuh -- Lennard-Jones 12-6 pair term shared by the LJ kernels.
+//   F_i += 24 eps (2 (s/r)^12 - (s/r)^6) / r^2 * (x_i - x_j)      (r < r_cut)
+//   U   += 4 eps ((s/r)^12 - (s/r)^6),  W += F.r
+#pragma once
+#include "pd_device.cuh"
+
+namespace pd {
+
+template <class T> struct LJP {
+    T eps24, eps4, sig2, rc2;
+};
+
+// Reciprocal by Newton-Raphson refinement (Newton's method for f(y) = 1/y - x,
+// y' = y (2 - x y), written as e = 1 - x y, y' = y + y e; each step doubles the
+// correct bits; Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000", IBM J. Res. Dev. 34, 1990).  The seed is the hardware
+// approximation rcp.approx.ftz.f64 (relative error below 2^-20), so two steps
+// reach full double precision (within 2 ulp of 1/x; tests/test_gpu_recip.py).
+// Valid for normal positive arguments, which is what squared pair distances are.
+__device__ __forceinline__ double recip(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+// FP32: hardware approximation (rcp.approx.ftz.f32, ~1 ulp) plus one refinement step
+__device__ __forceinline__ float recip(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    float e = fmaf(-x, y, 1.0f);
+    return fmaf(y, e, y);
+}
+
+template <class T>
+__device__ __forceinline__ void lj_acc(const LJP<T>& P, T r2, T dx, T dy, T dz, T& fx, T& fy, T& fz, T& e, T& w) {
+    T ir2 = recip(r2);
+    T s2 = P.sig2 * ir2;
+    T s6 = s2 * s2 * s2;
+    T ff = P.eps24 * ir2 * s6 * (T(2) * s6 - T(1));
+    fx += ff * dx;
+    fy += ff * dy;
+    fz += ff * dz;
+    e += P.eps4 * s6 * (s6 - T(1));
+    w += ff * r2;
+}
+
+}  // namespace pd

@@ -11,27 +11,12 @@
 // fixed block order (deterministic).
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
+#include "pd_lj.cuh"
+#include "pd_tile.cuh"
 
 namespace pd {
 
 static constexpr int FBLOCK = 256;
-
-template <class T> struct LJP {
-    T eps24, eps4, sig2, rc2;
-};
-
-template <class T>
-__device__ __forceinline__ void lj_acc(const LJP<T>& P, T r2, T dx, T dy, T dz, T& fx, T& fy, T& fz, T& e, T& w) {
-    T ir2 = T(1) / r2;
-    T s2 = P.sig2 * ir2;
-    T s6 = s2 * s2 * s2;
-    T ff = P.eps24 * ir2 * s6 * (T(2) * s6 - T(1));
-    fx += ff * dx;
-    fy += ff * dy;
-    fz += ff * dz;
-    e += P.eps4 * s6 * (s6 - T(1));
-    w += ff * r2;
-}
 
 template <class T>
 __global__ void __launch_bounds__(FBLOCK) k_lj_verlet(const typename V4<T>::type* __restrict__ pos, long n,
@@ -47,11 +32,10 @@ __global__ void __launch_bounds__(FBLOCK) k_lj_verlet(const typename V4<T>::type
 #pragma unroll 4
         for (int k = 0; k < m; ++k) {
             int q = __ldg(row + (long)k * stride);
-            if (q == (int)i) continue;
             typename V4<T>::type xq = ld4(pos, q);
             T dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
             T r2 = dist2(dx, dy, dz);
-            if (r2 < P.rc2) lj_acc(P, r2, dx, dy, dz, fx, fy, fz, e, w);
+            if (r2 < P.rc2 && q != (int)i) lj_acc(P, r2, dx, dy, dz, fx, fy, fz, e, w);
         }
         f[i] = fx;
         f[fcap + i] = fy;
@@ -187,13 +171,34 @@ __global__ void __launch_bounds__(FBLOCK) k_ke(const T* __restrict__ v, long cap
     if (threadIdx.x == 0) part[blockIdx.x] = ke;
 }
 
+template <class T> __global__ void k_recip_check(const T* __restrict__ x, T* __restrict__ y, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        y[i] = recip(x[i]);
+}
+
+// first stage of a fixed-order sum of (pe, vir) pairs: block b sums a fixed chunk
+__global__ void k_sum_pairs(const double* __restrict__ in, long n, long chunk, double* __restrict__ out) {
+    double a = 0, b = 0;
+    long beg = (long)blockIdx.x * chunk, end = min(beg + chunk, n);
+    for (long i = beg + threadIdx.x; i < end; i += 256) {
+        a += in[2 * i];
+        b += in[2 * i + 1];
+    }
+    a = block_sum<double, 256>(a);
+    b = block_sum<double, 256>(b);
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = a;
+        out[2 * blockIdx.x + 1] = b;
+    }
+}
+
 // E[s] = (KE, PE, virial, rebuilt) from the fixed-order partials
-__global__ void k_energy(const double* __restrict__ fpart, const double* __restrict__ kpart, int nb,
+__global__ void k_energy(const double* __restrict__ fpart, int nbf, const double* __restrict__ kpart, int nbk,
                          const unsigned int* __restrict__ rebuilt, double* __restrict__ E) {
     __shared__ double sh[3][256];
     double a = 0, b = 0, c = 0;
-    for (int i = threadIdx.x; i < nb; i += 256) {
-        a += kpart[i];
+    for (int i = threadIdx.x; i < nbk; i += 256) a += kpart[i];
+    for (int i = threadIdx.x; i < nbf; i += 256) {
         b += fpart[2 * i];
         c += fpart[2 * i + 1];
     }
@@ -225,6 +230,17 @@ struct pd_md_s {
     pd::Buf xb, fpart, kpart, E;
     int nblk = 0;
     bool ready = false;
+    // tiled neighbour structure (pd_tile.cu)
+    bool use_tiles = true;
+    int tile_tx = 0;  // cells per tile along x (0: from the mean occupancy)
+    int tile_p = 2;   // threads per domain particle in the pair kernel
+    bool tiles_active = false;
+    pd::TileGeom tg;
+    long ntiles = 0;
+    unsigned int tcap = 0;
+    long tstride = 0;
+    int tmax_nn = 0;
+    pd::Buf csR, csI, tnbr, tnn, tpart;
     long builds = 0, steps = 0;
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
@@ -303,6 +319,43 @@ static int force_blocks(long n) {
     return (int)want;
 }
 
+// Tiled structure: the real particles are already in cell order (sort_cl holds
+// their cell starts); sort the images by cell too, then build the tile-local rows.
+static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
+    pd_vd h = md->h;
+    long nc1 = cl->ncells + 1;
+    PD_TRY(md->csR.ensure(sizeof(unsigned int) * nc1));
+    PD_TRY(md->csI.ensure(sizeof(unsigned int) * nc1));
+    PD_CUDA(cudaMemcpyAsync(md->csR.p, cl->cell_start.p, sizeof(unsigned int) * nc1, cudaMemcpyDeviceToDevice, st));
+    long m = h->n_img, n = h->n_real;
+    PD_TRY(cl_build(h, cl, m, nullptr, st, n));
+    PD_CUDA(cudaMemcpyAsync(md->csI.p, cl->cell_start.p, sizeof(unsigned int) * nc1, cudaMemcpyDeviceToDevice, st));
+    if (m > 0) {
+        const int* ids = cl->sorted.as<int>();
+        size_t need = std::max((size_t)m * h->pos_bytes, (size_t)m * sizeof(int));
+        PD_TRY(h->tmp2.ensure(need));
+        char* pos_img = (char*)h->pos + (size_t)n * h->pos_bytes;
+        PD_TRY(gather_bytes(pos_img, h->tmp2.p, ids, m, h->pos_bytes, st));
+        PD_CUDA(cudaMemcpyAsync(pos_img, h->tmp2.p, (size_t)m * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
+        PD_TRY(gather_bytes(h->gid + n, h->tmp2.p, ids, m, 4, st));
+        PD_CUDA(cudaMemcpyAsync(h->gid + n, h->tmp2.p, sizeof(int) * m, cudaMemcpyDeviceToDevice, st));
+        PD_TRY(gather_bytes(h->img_src.p, h->tmp2.p, ids, m, 4, st));
+        PD_CUDA(cudaMemcpyAsync(h->img_src.p, h->tmp2.p, sizeof(int) * m, cudaMemcpyDeviceToDevice, st));
+        PD_TRY(gather_bytes(h->img_shift.p, h->tmp2.p, ids, m, 1, st));
+        PD_CUDA(cudaMemcpyAsync(h->img_shift.p, h->tmp2.p, (size_t)m, cudaMemcpyDeviceToDevice, st));
+    }
+    PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
+    unsigned int tmax = 0, cmax = 0;
+    PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax, cmax, st));
+    if (!tile_fits(h, tmax)) return PD_OK;  // stays on the global-index list
+    md->tcap = tmax;
+    PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
+                      md->vl->r_cut, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
+    PD_TRY(md->tpart.ensure(sizeof(double) * 2 * ((md->ntiles > 0 ? md->ntiles : 1) + 256)));
+    md->tiles_active = true;
+    return PD_OK;
+}
+
 // wrap, sort the real particles into cell order, periodic images, neighbour structure
 static int md_rebuild(pd_md md, cudaStream_t st) {
     pd_vd h = md->h;
@@ -318,7 +371,9 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
     if (md->mp.use_cell_list) {
         PD_TRY(cl_build(h, md->cl, h->n_total, nullptr, st));
     } else {
-        PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
+        md->tiles_active = false;
+        if (md->use_tiles) PD_TRY(md_tiles(md, sort_cl, st));
+        if (!md->tiles_active) PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
         PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
     }
     h->epoch++;
@@ -327,6 +382,10 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
 }
 
 static int md_forces(pd_md md, cudaStream_t st) {
+    if (md->tiles_active)
+        return tile_lj(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
+                       md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop, md->tpart.as<double>(), true,
+                       md->tile_p, st);
     return lj_launch(md->h, md->mp.use_cell_list ? nullptr : md->vl, md->mp.use_cell_list ? md->cl : nullptr, md->lj,
                      md->mp.force_prop, md->fpart.as<double>(), md->nblk, st);
 }
@@ -336,6 +395,23 @@ static int md_forces(pd_md md, cudaStream_t st) {
 using namespace pd;
 
 extern "C" {
+
+int pd_selftest_recip(int dtype, const void* x_host, void* out_host, long n) {
+    if ((dtype != PD_F32 && dtype != PD_F64) || !x_host || !out_host || n < 0) return PD_EINVAL;
+    if (n == 0) return PD_OK;
+    size_t es = dtype == PD_F64 ? 8 : 4;
+    Buf a, b;
+    PD_TRY(a.ensure(es * n));
+    PD_TRY(b.ensure(es * n));
+    PD_CUDA(cudaMemcpy(a.p, x_host, es * n, cudaMemcpyHostToDevice));
+    if (dtype == PD_F64) pd::launch(k_recip_check<double>, grid_for(n, 256), 256, 0, (cudaStream_t)0, a.as<const double>(), b.as<double>(), n);
+    else pd::launch(k_recip_check<float>, grid_for(n, 256), 256, 0, (cudaStream_t)0, a.as<const float>(), b.as<float>(), n);
+    PD_LAUNCH_CHECK();
+    PD_CUDA(cudaMemcpy(out_host, b.p, es * n, cudaMemcpyDeviceToHost));
+    a.release();
+    b.release();
+    return PD_OK;
+}
 
 int pd_lj_forces(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t* lj, int force_prop, void* stream,
                  double* energy) {
@@ -424,6 +500,11 @@ int pd_md_destroy(pd_md md) {
     md->fpart.release();
     md->kpart.release();
     md->E.release();
+    md->csR.release();
+    md->csI.release();
+    md->tnbr.release();
+    md->tnn.release();
+    md->tpart.release();
     for (int i = 0; i < 8; ++i)
         if (md->ev[i]) cudaEventDestroy(md->ev[i]);
     delete md;
@@ -488,8 +569,18 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         PD_LAUNCH_CHECK();
         h->ctrl_h->rebuild = rebuilt;
         PD_CUDA(cudaMemcpyAsync(&h->ctrl->rebuild, &h->ctrl_h->rebuild, sizeof(unsigned int), cudaMemcpyHostToDevice, st));
-        pd::launch(k_energy, 1, 256, 0, st, md->fpart.as<double>(), md->kpart.as<double>(), md->nblk, &h->ctrl->rebuild,
-                                     md->E.as<double>() + 4 * s);
+        if (md->tiles_active) {
+            const int nb2 = 256;
+            long chunk = (md->ntiles + nb2 - 1) / nb2;
+            double* stage = md->tpart.as<double>() + 2 * md->ntiles;
+            pd::launch(k_sum_pairs, nb2, 256, 0, st, (const double*)md->tpart.as<double>(), md->ntiles, chunk, stage);
+            pd::launch(k_energy, 1, 256, 0, st, (const double*)stage, nb2, (const double*)md->kpart.as<double>(),
+                       md->nblk, (const unsigned int*)&h->ctrl->rebuild, md->E.as<double>() + 4 * s);
+        }
+        else
+            pd::launch(k_energy, 1, 256, 0, st, (const double*)md->fpart.as<double>(), md->nblk,
+                       (const double*)md->kpart.as<double>(), md->nblk, (const unsigned int*)&h->ctrl->rebuild,
+                       md->E.as<double>() + 4 * s);
         PD_LAUNCH_CHECK();
         md->steps++;
         if (md->timing) {
@@ -541,14 +632,60 @@ int pd_md_timers(pd_md md, double* ms, long* counts) {
     return PD_OK;
 }
 
+int pd_md_set_tiles(pd_md md, int on, int tx, int threads_per_particle) {
+    if (!md || tx < 0 || tx > TXMAX) return PD_EINVAL;
+    int p = threads_per_particle <= 0 ? 2 : threads_per_particle;
+    if (p != 1 && p != 2 && p != 4) return PD_EINVAL;
+    md->use_tiles = on != 0;
+    md->tile_tx = tx;
+    md->tile_p = p;
+    md->ready = false;  // rebuild with the new structure at the next run
+    return PD_OK;
+}
+
+int pd_md_verlet_get(pd_md md, int* counts, int* idx, long idx_cap, int* tiled) {
+    if (!md || !counts) return PD_EINVAL;
+    if (tiled) *tiled = md->tiles_active ? 1 : 0;
+    if (!md->tiles_active) {
+        if (!md->vl) return PD_ESTATE;
+        return pd_verlet_get(md->vl, counts, idx, idx_cap, nullptr);
+    }
+    pd_vd h = md->h;
+    long n = h->n_real;
+    if (n == 0) return PD_OK;
+    PD_CUDA(cudaMemcpy(counts, md->tnn.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (!idx) return PD_OK;
+    long tot = 0;
+    int mx = 0;
+    for (long i = 0; i < n; ++i) {
+        tot += counts[i];
+        mx = std::max(mx, counts[i]);
+    }
+    if (tot > idx_cap) return PD_EINVAL;
+    Buf out;
+    PD_TRY(out.ensure(sizeof(int) * (size_t)md->tstride * (mx > 0 ? mx : 1)));
+    PD_TRY(tile_translate(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tnbr,
+                          md->tnn, md->tstride, mx, out.as<int>(), 0));
+    std::vector<int> col((size_t)md->tstride * mx);
+    if (mx > 0) PD_CUDA(cudaMemcpy(col.data(), out.p, sizeof(int) * col.size(), cudaMemcpyDeviceToHost));
+    out.release();
+    long o = 0;
+    for (long i = 0; i < n; ++i)
+        for (int k = 0; k < counts[i]; ++k) idx[o++] = col[(size_t)k * md->tstride + i];
+    return PD_OK;
+}
+
 int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn) {
     if (!md || !n_dom || !mean_nn || !max_nn) return PD_EINVAL;
     *n_dom = 0;
     *mean_nn = 0;
     *max_nn = 0;
-    if (!md->vl || md->vl->n_dom == 0) return PD_OK;
-    std::vector<int> c(md->vl->n_dom);
-    PD_CUDA(cudaMemcpy(c.data(), md->vl->nn.p, sizeof(int) * c.size(), cudaMemcpyDeviceToHost));
+    if (!md->vl) return PD_OK;
+    long nd = md->tiles_active ? md->h->n_real : md->vl->n_dom;
+    if (nd == 0) return PD_OK;
+    std::vector<int> c(nd);
+    PD_CUDA(cudaMemcpy(c.data(), md->tiles_active ? md->tnn.p : md->vl->nn.p, sizeof(int) * c.size(),
+                       cudaMemcpyDeviceToHost));
     double s = 0;
     int m = 0;
     for (int x : c) {

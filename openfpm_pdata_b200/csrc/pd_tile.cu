@@ -1,0 +1,454 @@
+// pd_tile.cu -- tiled neighbour structure of the integrator: Verlet rows as
+// tile-local 16-bit indices into a shared-memory staging of the neighbour cells.
+//
+// Layout after a rebuild (cell grid of side r_cut + skin):
+//   real particles [0, n_real)        sorted by cell, cell starts csR[ncells+1]
+//   periodic images [n_real, n_total) sorted by cell, cell starts csI (relative)
+// A tile is TX consecutive cells along x of one cell row (y, z).  Its
+// neighbourhood is 9 rows (dy, dz in {-1,0,1}) x cells x0-1 .. x0+TX, i.e. 9
+// contiguous ranges of real particles and 9 of images.  One CTA per tile copies
+// those 18 ranges into shared memory with 1-D TMA bulk copies
+// (cp.async.bulk global -> shared, mbarrier completion, no multicast), in the
+// order R0, I0, R1, I1, ... R8, I8.  The Verlet row of a domain particle of the
+// tile stores positions in that staging (uint16), column-major
+// nbr[k*stride + i]; the force kernel stages the same ranges and reads every
+// neighbour from shared memory.  Compared with global int32 indices this halves
+// the list bytes and replaces dependent global gathers by shared-memory loads.
+// Walk order per row: the real cells x-1..x+1, then the image cells x-1..x+1.
+#include "pd_device.cuh"
+#include "pd_internal.cuh"
+#include "pd_lj.cuh"
+#include "pd_tile.cuh"
+
+namespace pd {
+
+// Rows hold two 16-bit entries per 32-bit word: entries 2w and 2w+1 of particle
+// i share word w*stride + i (column-major over words).
+__device__ __forceinline__ long pair_slot(int k, long stride, unsigned int i) {
+    return (((long)(k >> 1) * stride + i) << 1) | (k & 1);
+}
+
+struct TileSh {
+    unsigned int cR[9][TXMAX + 3];
+    unsigned int cI[9][TXMAX + 3];
+    unsigned int oR[9], oI[9];
+    unsigned int total;
+    int ncol;
+    unsigned long long bar;
+};
+
+__device__ __forceinline__ void tile_layout(const TileGeom& tg, long t, const unsigned int* __restrict__ csR,
+                                            const unsigned int* __restrict__ csI, TileSh& S) {
+    int tx = (int)(t % tg.ntx);
+    long rest = t / tg.ntx;
+    int y = (int)(rest % tg.ny) + tg.pad;
+    int z = (int)(rest / tg.ny) + tg.pad;
+    int x0 = tg.pad + tx * tg.TX;
+    int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
+    int ncol = x1 - x0 + 3;
+    for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+        int img = e >= 9 * ncol;
+        int ee = img ? e - 9 * ncol : e;
+        int r = ee / ncol, j = ee % ncol;
+        int dz = r / 3 - 1, dy = r % 3 - 1;
+        long c = (long)(x0 - 1 + j) + (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
+        if (img) S.cI[r][j] = csI[c];
+        else S.cR[r][j] = csR[c];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int off = 0;
+        for (int r = 0; r < 9; ++r) {
+            S.oR[r] = off;
+            off += S.cR[r][ncol - 1] - S.cR[r][0];
+            S.oI[r] = off;
+            off += S.cI[r][ncol - 1] - S.cI[r][0];
+        }
+        S.total = off;
+        S.ncol = ncol;
+    }
+    __syncthreads();
+}
+
+// Stage the tile's 18 ranges; false (uniformly) if the tile does not fit or the
+// bounded wait gave up (error bit set).
+template <class T>
+__device__ __forceinline__ bool tile_stage(const typename V4<T>::type* __restrict__ preal,
+                                           const typename V4<T>::type* __restrict__ pimg, TileSh& S,
+                                           typename V4<T>::type* sm, unsigned int cap, unsigned int* err) {
+    typedef typename V4<T>::type T4;
+    if (S.total > cap) {
+        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+        return false;
+    }
+    if (S.total == 0) return true;
+    if (threadIdx.x == 0) mbar_init(&S.bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(T4));
+        const int nc = S.ncol - 1;
+        for (int r = 0; r < 9; ++r) {
+            unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+            if (lr) bulk_g2s(sm + S.oR[r], preal + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
+            unsigned int li = S.cI[r][nc] - S.cI[r][0];
+            if (li) bulk_g2s(sm + S.oI[r], pimg + S.cI[r][0], li * (unsigned int)sizeof(T4), &S.bar);
+        }
+    }
+    bool ok = mbar_wait_bounded(&S.bar, 0, 1u << 24);
+    if (!ok) {
+        atomicOr(err, ERR_TIMEOUT);
+        mbar_wait_bounded(&S.bar, 0, 1u << 24);  // let copies in flight land before the CTA exits
+    }
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// largest staged neighbourhood and largest centre count over the tiles
+__global__ void k_tile_sizes(TileGeom tg, long ntiles, const unsigned int* __restrict__ csR,
+                             const unsigned int* __restrict__ csI, unsigned int* __restrict__ tmax,
+                             unsigned int* __restrict__ cmax) {
+    unsigned int mt = 0, mc = 0;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ntiles; t += (long)gridDim.x * blockDim.x) {
+        int tx = (int)(t % tg.ntx);
+        long rest = t / tg.ntx;
+        int y = (int)(rest % tg.ny) + tg.pad;
+        int z = (int)(rest / tg.ny) + tg.pad;
+        int x0 = tg.pad + tx * tg.TX;
+        int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
+        unsigned int tot = 0;
+        for (int r = 0; r < 9; ++r) {
+            int dz = r / 3 - 1, dy = r % 3 - 1;
+            long rb = (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
+            tot += csR[rb + x1 + 1] - csR[rb + x0 - 1];
+            tot += csI[rb + x1 + 1] - csI[rb + x0 - 1];
+            if (r == 4) mc = max(mc, csR[rb + x1] - csR[rb + x0]);
+        }
+        mt = max(mt, tot);
+    }
+    mt = warp_max(mt);
+    mc = warp_max(mc);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(tmax, mt);
+        atomicMax(cmax, mc);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::type* __restrict__ pos, long n_real,
+                                                        TileGeom tg, const unsigned int* __restrict__ csR,
+                                                        const unsigned int* __restrict__ csI, unsigned int cap, T r2,
+                                                        unsigned short* __restrict__ nbr, int* __restrict__ nn,
+                                                        long stride, int max_nn, unsigned int* __restrict__ err,
+                                                        unsigned int* __restrict__ nn_max) {
+    typedef typename V4<T>::type T4;
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    T4* sm = reinterpret_cast<T4*>(tile_raw);
+    __shared__ TileSh S;
+    tile_layout(tg, blockIdx.x, csR, csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    if (ib == ie) return;
+    if (!tile_stage<T>(pos, pos + n_real, S, sm, cap, err)) return;
+    const int ncol = S.ncol;
+    for (unsigned int i = ib + threadIdx.x; i < ie; i += blockDim.x) {
+        T4 xi = sm[S.oR[4] + (i - S.cR[4][0])];
+        int j = 1;
+        while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
+        int cnt = 0;
+#pragma unroll 1
+        for (int r = 0; r < 9; ++r) {
+#pragma unroll 1
+            for (int part = 0; part < 2; ++part) {
+                const unsigned int* cc = part ? S.cI[r] : S.cR[r];
+                unsigned int a = cc[j - 1], e = cc[j + 2];
+                unsigned int base = (part ? S.oI[r] : S.oR[r]) - cc[0];
+#pragma unroll 4
+                for (unsigned int q = a; q < e; ++q) {
+                    T4 xq = sm[base + q];
+                    T d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
+                    if (d2 < r2) {
+                        if (cnt < max_nn) nbr[pair_slot(cnt, stride, i)] = (unsigned short)(base + q);
+                        cnt++;
+                    }
+                }
+            }
+        }
+        // odd rows end with the particle itself, which the pair kernel skips
+        if ((cnt & 1) && cnt < max_nn) nbr[pair_slot(cnt, stride, i)] = (unsigned short)(S.oR[4] + (i - S.cR[4][0]));
+        if (cnt > max_nn) {
+            atomicOr(err, ERR_NN_OVERFLOW);
+            atomicMax(nn_max, (unsigned int)cnt);
+            cnt = max_nn;
+        }
+        nn[i] = cnt;
+    }
+}
+
+// P threads per domain particle split its row (words w = sub, sub+P, ...; two
+// entries per word); partial sums meet through shuffles.  Energies: one FP64
+// partial per block (fixed-order tree), reduced in fixed order afterwards.
+template <class T, bool ENERGY, int P>
+__global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::type* __restrict__ pos, long n_real,
+                                                       TileGeom tg, const unsigned int* __restrict__ csR,
+                                                       const unsigned int* __restrict__ csI, unsigned int cap,
+                                                       const unsigned int* __restrict__ nbr,
+                                                       const int* __restrict__ nn, long stride, LJP<T> Pr,
+                                                       T* __restrict__ f, long fcap, double* __restrict__ part,
+                                                       unsigned int* __restrict__ err) {
+    typedef typename V4<T>::type T4;
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    T4* sm = reinterpret_cast<T4*>(tile_raw);
+    __shared__ TileSh S;
+    tile_layout(tg, blockIdx.x, csR, csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    double pe = 0, vir = 0;
+    bool staged = ib != ie && tile_stage<T>(pos, pos + n_real, S, sm, cap, err);
+    if (staged) {
+        const unsigned int base = S.oR[4] - S.cR[4][0];
+        const int sub = threadIdx.x % P;
+        // whole warps iterate together (the shuffles below need all 32 lanes)
+        const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
+        for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
+            const unsigned int i = ib + t / P;
+            const bool active = i < ie;
+            const unsigned int li = base + i;
+            T4 xi = sm[active ? li : 0];
+            const int words = active ? (nn[i] + 1) >> 1 : 0;
+            T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
+            const unsigned int* row = nbr + i;
+#pragma unroll 2
+            for (int k = sub; k < words; k += P) {
+                const unsigned int pair = __ldg(row + (long)k * stride);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
+                    T4 xq = sm[l];
+                    T dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
+                    T r2 = dist2(dx, dy, dz);
+                    if (r2 < Pr.rc2 && l != li) {
+                        T ir2 = recip(r2);
+                        T s2 = Pr.sig2 * ir2;
+                        T s6 = s2 * s2 * s2;
+                        T ff = Pr.eps24 * ir2 * s6 * (T(2) * s6 - T(1));
+                        fx += ff * dx;
+                        fy += ff * dy;
+                        fz += ff * dz;
+                        if (ENERGY) {
+                            e += Pr.eps4 * s6 * (s6 - T(1));
+                            w += ff * r2;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < P; o <<= 1) {
+                fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                if (ENERGY) {
+                    e += __shfl_xor_sync(0xffffffffu, e, o);
+                    w += __shfl_xor_sync(0xffffffffu, w, o);
+                }
+            }
+            if (active && sub == 0) {
+                f[i] = fx;
+                f[fcap + i] = fy;
+                f[2 * fcap + i] = fz;
+                if (ENERGY) {
+                    pe += 0.5 * (double)e;
+                    vir += 0.5 * (double)w;
+                }
+            }
+        }
+    }
+    if (ENERGY) {
+        pe = block_sum<double, FBLOCK_T>(pe);
+        vir = block_sum<double, FBLOCK_T>(vir);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = pe;
+            part[2 * blockIdx.x + 1] = vir;
+        }
+    }
+}
+
+// tile-local rows -> global particle indices (for checks and downloads)
+__global__ void __launch_bounds__(TBLOCK) k_vtile_translate(long n_real, TileGeom tg,
+                                                            const unsigned int* __restrict__ csR,
+                                                            const unsigned int* __restrict__ csI,
+                                                            const unsigned short* __restrict__ nbr,
+                                                            const int* __restrict__ nn, long stride,
+                                                            int* __restrict__ out) {
+    __shared__ TileSh S;
+    tile_layout(tg, blockIdx.x, csR, csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    const int nc = S.ncol - 1;
+    for (unsigned int i = ib + threadIdx.x; i < ie; i += blockDim.x) {
+        int m = nn[i];
+        for (int k = 0; k < m; ++k) {
+            unsigned int l = nbr[pair_slot(k, stride, i)];
+            int g = -1;
+            for (int r = 0; r < 9; ++r) {
+                unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
+                if (l >= S.oR[r] && l < S.oR[r] + lr) g = (int)(S.cR[r][0] + (l - S.oR[r]));
+                if (l >= S.oI[r] && l < S.oI[r] + li) g = (int)(n_real + S.cI[r][0] + (l - S.oI[r]));
+            }
+            out[(long)k * stride + i] = g;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+static const int SMEM_LIMIT = 200 * 1024;
+
+int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles) {
+    tg.gs0 = cl->gs[0];
+    tg.gs1 = cl->gs[1];
+    tg.gs2 = cl->gs[2];
+    tg.pad = cl->pad;
+    int nxi = tg.gs0 - 2 * tg.pad;
+    int TX = TX_req;
+    if (TX <= 0) {
+        double cells = (double)cl->div[0] * cl->div[1] * cl->div[2];
+        double occ = cells > 0 ? (double)n_real / cells : 1.0;
+        TX = (int)(120.0 / (occ > 1e-3 ? occ : 1e-3) + 0.5);
+    }
+    if (TX < 1) TX = 1;
+    if (TX > TXMAX) TX = TXMAX;
+    if (TX > nxi) TX = nxi;
+    tg.TX = TX;
+    tg.ntx = (nxi + TX - 1) / TX;
+    tg.ny = tg.gs1 - 2 * tg.pad;
+    tg.nz = tg.gs2 - 2 * tg.pad;
+    ntiles = (long)tg.ntx * tg.ny * tg.nz;
+    if (cl->pad != 1) {
+        set_error("tile plan: the tiled list needs one padding layer");
+        return PD_EINVAL;
+    }
+    return PD_OK;
+}
+
+int tile_sizes(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+               unsigned int& tmax, unsigned int& cmax, cudaStream_t st) {
+    PD_CUDA(cudaMemsetAsync(&h->ctrl->tile_max, 0, 2 * sizeof(unsigned int), st));
+    pd::launch(k_tile_sizes, grid_for(ntiles, 256), 256, 0, st, tg, ntiles, csR, csI, &h->ctrl->tile_max,
+               &h->ctrl->tile_center_max);
+    PD_LAUNCH_CHECK();
+    PD_TRY(read_ctrl(h, st));
+    tmax = h->ctrl_h->tile_max;
+    cmax = h->ctrl_h->tile_center_max;
+    return PD_OK;
+}
+
+template <class K> static int allow_smem(K kernel, int bytes) {
+    PD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return PD_OK;
+}
+
+bool tile_fits(pd_vd h, unsigned int tmax) {
+    return (long)tmax * h->pos_bytes <= SMEM_LIMIT && tmax <= 65535u;
+}
+
+int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+               unsigned int cap, double r_list, Buf& nbr, Buf& nn, long& stride, int& max_nn, cudaStream_t st) {
+    long n = h->n_real;
+    stride = ((n + 31) / 32) * 32;
+    if (stride < 32) stride = 32;
+    int smem = (int)(cap * h->pos_bytes);
+    if (smem < 16) smem = 16;
+    if (max_nn <= 0) {
+        double vol = (h->hi[0] - h->lo[0]) * (h->hi[1] - h->lo[1]) * (h->hi[2] - h->lo[2]);
+        double mean = (double)n / vol * 4.18879 * r_list * r_list * r_list;
+        max_nn = (int)(mean * 1.5 + 32);
+    }
+    max_nn = (max_nn + 1) & ~1;  // whole 32-bit words
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        PD_TRY(nbr.ensure(sizeof(unsigned short) * (size_t)stride * max_nn));
+        PD_TRY(nn.ensure(sizeof(int) * (size_t)stride));
+        PD_CUDA(cudaMemsetAsync(nn.p, 0, sizeof(int) * (size_t)stride, st));
+        if (h->dtype == PD_F64) {
+            PD_TRY(allow_smem(k_vtile_build<double>, smem));
+            pd::launch(k_vtile_build<double>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const double4*)h->pos, n, tg,
+                       csR, csI, cap, r_list * r_list, nbr.as<unsigned short>(), nn.as<int>(), stride, max_nn,
+                       &h->ctrl->err, &h->ctrl->nn_max);
+        } else {
+            float rl = (float)r_list;
+            PD_TRY(allow_smem(k_vtile_build<float>, smem));
+            pd::launch(k_vtile_build<float>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const float4*)h->pos, n, tg,
+                       csR, csI, cap, rl * rl, nbr.as<unsigned short>(), nn.as<int>(), stride, max_nn,
+                       &h->ctrl->err, &h->ctrl->nn_max);
+        }
+        PD_LAUNCH_CHECK();
+        PD_TRY(read_ctrl(h, st));
+        if (h->ctrl_h->err & (ERR_TILE_CAP | ERR_TIMEOUT)) {
+            set_error("tiled Verlet build failed (err=0x%x)", h->ctrl_h->err);
+            return PD_EOVERFLOW;
+        }
+        if (!(h->ctrl_h->err & ERR_NN_OVERFLOW)) return PD_OK;
+        max_nn = ((int)(h->ctrl_h->nn_max * 1.15 + 8) + 1) & ~1;
+        h->ctrl_h->err &= ~ERR_NN_OVERFLOW;
+        h->ctrl_h->nn_max = 0;
+        PD_CUDA(cudaMemcpyAsync(&h->ctrl->err, &h->ctrl_h->err, sizeof(unsigned int) * 2, cudaMemcpyHostToDevice, st));
+    }
+    set_error("tiled Verlet build: row capacity did not converge");
+    return PD_EOVERFLOW;
+}
+
+template <class T, bool E, int P>
+static int launch_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                       unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<T>& LP, T* f,
+                       double* part, int smem, cudaStream_t st) {
+    PD_TRY(allow_smem(k_vtile_lj<T, E, P>, smem));
+    pd::launch(k_vtile_lj<T, E, P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
+               (const typename V4<T>::type*)h->pos, h->n_real, tg, csR, csI, cap, nbr.as<unsigned int>(),
+               nn.as<int>(), stride, LP, f, h->cap, part, &h->ctrl->err);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+template <class T>
+static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                     unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, T* f,
+                     double* part, bool energy, int P, int smem, cudaStream_t st) {
+    LJP<T> LP;
+    LP.eps24 = (T)(24.0 * lj.eps);
+    LP.eps4 = (T)(4.0 * lj.eps);
+    LP.sig2 = (T)(lj.sigma * lj.sigma);
+    T rc = (T)lj.r_cut;
+    LP.rc2 = rc * rc;
+#define PD_LJ_CASE(E, PP)                                                                                         \
+    if (energy == E && P == PP)                                                                                   \
+        return launch_lj_t<T, E, PP>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, smem, st);
+    PD_LJ_CASE(true, 1)
+    PD_LJ_CASE(true, 2)
+    PD_LJ_CASE(true, 4)
+    PD_LJ_CASE(false, 1)
+    PD_LJ_CASE(false, 2)
+    PD_LJ_CASE(false, 4)
+#undef PD_LJ_CASE
+    set_error("tile_lj: threads per particle must be 1, 2 or 4");
+    return PD_EINVAL;
+}
+
+int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+            unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
+            double* part, bool energy, int P, cudaStream_t st) {
+    Prop& F = h->props[force_prop];
+    int smem = (int)(cap * h->pos_bytes);
+    if (smem < 16) smem = 16;
+    if (h->dtype == PD_F64)
+        return tile_lj_t<double>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (double*)F.d, part, energy, P,
+                                 smem, st);
+    return tile_lj_t<float>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (float*)F.d, part, energy, P, smem,
+                            st);
+}
+
+int tile_translate(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                   const Buf& nbr, const Buf& nn, long stride, int max_nn, int* out_dev, cudaStream_t st) {
+    pd::launch(k_vtile_translate, (unsigned)ntiles, TBLOCK, 0, st, h->n_real, tg, csR, csI, nbr.as<unsigned short>(),
+               nn.as<int>(), stride, out_dev);
+    PD_LAUNCH_CHECK();
+    (void)max_nn;
+    return PD_OK;
+}
+
+}  // namespace pd

@@ -1,0 +1,28 @@
+// pd_tile.cuh -- tiled Verlet structure shared by the integrator (see pd_tile.cu).
+#pragma once
+#include "pd_internal.cuh"
+
+namespace pd {
+
+static constexpr int TXMAX = 32;   // cells per tile along x, at most
+static constexpr int TBLOCK = 128;   // threads per tile CTA of the list build
+static constexpr int FBLOCK_T = 256; // threads per tile CTA of the pair kernels
+
+struct TileGeom {
+    int gs0, gs1, gs2, pad;
+    int TX, ntx, ny, nz;
+};
+
+int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles);
+int tile_sizes(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+               unsigned int& tmax, unsigned int& cmax, cudaStream_t st);
+bool tile_fits(pd_vd h, unsigned int tmax);
+int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+               unsigned int cap, double r_list, Buf& nbr, Buf& nn, long& stride, int& max_nn, cudaStream_t st);
+int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+            unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
+            double* part, bool energy, int P, cudaStream_t st);
+int tile_translate(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                   const Buf& nbr, const Buf& nn, long stride, int max_nn, int* out_dev, cudaStream_t st);
+
+}  // namespace pd

@@ -119,6 +119,9 @@ def lib():
             "pd_launch_count": ([], ctypes.c_ulonglong),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
+            "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
+            "pd_selftest_recip": ([ip, vp, vp, lp], ip),
+            "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -146,6 +149,15 @@ def _ptr(a):
 def launch_count():
     """Kernels launched by libpdgpu.so so far."""
     return int(lib().pd_launch_count())
+
+
+def selftest_recip(x):
+    """The pair kernels' reciprocal evaluated on the GPU for the values x."""
+    x = np.ascontiguousarray(x)
+    code = PD_F64 if x.dtype == np.float64 else PD_F32
+    out = np.zeros_like(x)
+    check(lib().pd_selftest_recip(code, _ptr(x), _ptr(out), int(x.size)))
+    return out
 
 
 def device_info():
@@ -388,6 +400,21 @@ class MD:
         cnt = (ctypes.c_long * 4)()
         check(lib().pd_md_timers(self.h, ms, cnt))
         return {k: (ms[i], cnt[i]) for i, k in enumerate(("integrate", "rebuild", "images", "force"))}
+
+    def set_tiles(self, on=True, tx=0, threads_per_particle=0):
+        check(lib().pd_md_set_tiles(self.h, int(bool(on)), int(tx), int(threads_per_particle)))
+
+    def verlet(self):
+        """(offsets, idx, tiled) of the driver's current Verlet rows (global indices)."""
+        n = self.vd.size_local()
+        counts = np.zeros(max(n, 1), np.int32)
+        tiled = ctypes.c_int(0)
+        check(lib().pd_md_verlet_get(self.h, _ptr(counts), None, 0, ctypes.byref(tiled)))
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum(counts[:n])
+        idx = np.zeros(max(int(off[-1]), 1), np.int32)
+        check(lib().pd_md_verlet_get(self.h, _ptr(counts), _ptr(idx), int(idx.shape[0]), ctypes.byref(tiled)))
+        return off, idx[: off[-1]], bool(tiled.value)
 
     def list_stats(self):
         """(domain particles, mean Verlet row length, longest row) of the last build."""

@@ -313,3 +313,45 @@ def test_md_lj_matches_oracle(pd, orc, cell_list):
     assert np.max(np.abs(d)) < 1e-8
     b, s, err = md.stats()
     assert s == 100 and err == 0
+
+
+@pytest.mark.parametrize("tx", [0, 1, 3, 8])
+def test_md_tiled_rows_equal_oracle_sets(pd, orc, tx):
+    """The driver's tile-local Verlet rows, translated to global indices, hold
+    exactly the oracle's neighbour sets (d2 < (r_cut+skin)^2, self included)
+    for the particles and images as stored after the build."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(14, 1.1, 0.05, seed=31)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = make_vd(pd, x, lo, hi, bc, 2.8, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
+    md.set_tiles(True, tx)
+    md.run(0)
+    off, idx, tiled = md.verlet()
+    assert tiled
+    allp = vd.deviceToHostPos()
+    n = x.shape[0]
+    G = orc.cl_geometry(lo, hi, 2.8, 2.8, verlet=True)
+    eoff, eidx = orc.verlet(allp, n, G, 2.8)
+    assert np.array_equal(np.diff(off), np.diff(eoff))
+    for i in range(n):
+        assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), np.sort(eidx[eoff[i]:eoff[i + 1]]))
+
+
+def test_md_tiled_equals_global_rows(pd):
+    """Tiled shared-memory rows and global-index rows give the same trajectory
+    energies (different summation order only)."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(16, 1.1, 0.05, seed=32)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    out = []
+    for tiles in (True, False):
+        vd = make_vd(pd, x, lo, hi, bc, 2.8, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+        vd.hostToDeviceProp(0, v)
+        md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
+        md.set_tiles(tiles)
+        out.append(md.run(40))
+        assert md.verlet()[2] == tiles
+    np.testing.assert_allclose(out[0][:, :3], out[1][:, :3], rtol=1e-10, atol=1e-10)
+    assert np.array_equal(out[0][:, 3], out[1][:, 3])
