@@ -240,7 +240,7 @@ struct pd_md_s {
     unsigned int tcap = 0;
     long tstride = 0;
     int tmax_nn = 0;
-    pd::Buf csR, csI, tnbr, tnn, tpart;
+    pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
     long builds = 0, steps = 0;
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
@@ -350,7 +350,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     if (!tile_fits(h, tmax)) return PD_OK;  // stays on the global-index list
     md->tcap = tmax;
     PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
-                      md->vl->r_cut, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
+                      md->vl->r_cut, md->pos32, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
     PD_TRY(md->tpart.ensure(sizeof(double) * 2 * ((md->ntiles > 0 ? md->ntiles : 1) + 256)));
     md->tiles_active = true;
     return PD_OK;
@@ -505,6 +505,7 @@ int pd_md_destroy(pd_md md) {
     md->tnbr.release();
     md->tnn.release();
     md->tpart.release();
+    md->pos32.release();
     for (int i = 0; i < 8; ++i)
         if (md->ev[i]) cudaEventDestroy(md->ev[i]);
     delete md;

@@ -20,6 +20,8 @@
 #include "pd_lj.cuh"
 #include "pd_tile.cuh"
 
+#include <cmath>
+
 namespace pd {
 
 // Rows hold two 16-bit entries per 32-bit word: entries 2w and 2w+1 of particle
@@ -132,47 +134,79 @@ __global__ void k_tile_sizes(TileGeom tg, long ntiles, const unsigned int* __res
     }
 }
 
+// pos32[k] = (float)pos[k] (x, y, z) with the slot index in w: the staged copy of
+// the list build, half the bytes of the FP64 records
 template <class T>
-__global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::type* __restrict__ pos, long n_real,
+__global__ void k_pos32(const typename V4<T>::type* __restrict__ pos, long n, float4* __restrict__ out) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        typename V4<T>::type r = ld4(pos, k);
+        out[k] = make_float4((float)r.x, (float)r.y, (float)r.z, __int_as_float((int)k));
+    }
+}
+
+// exact predicate for the rare candidates inside the FP32 uncertainty band
+template <class T>
+__device__ __noinline__ bool exact_in(const typename V4<T>::type* __restrict__ pos, unsigned int i, int q, T r2) {
+    typename V4<T>::type a = ld4(pos, (long)i), b = ld4(pos, (long)q);
+    return dist2(a.x - b.x, a.y - b.y, a.z - b.z) < r2;
+}
+
+// List build.  The candidates are staged as FP32 copies; d2 in FP32 decides
+// every pair farther than `band` from r^2 (|d2_f32 - d2_exact| < band by the
+// error bound computed on the host), the few inside the band are decided
+// exactly in the position type T from global memory -- so the rows equal the
+// exact predicate d2 < r^2.  Entries are stored a 32-bit word (two entries) at
+// a time.
+template <class T>
+__global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::type* __restrict__ pos,
+                                                        const float4* __restrict__ pos32, long n_real,
                                                         TileGeom tg, const unsigned int* __restrict__ csR,
                                                         const unsigned int* __restrict__ csI, unsigned int cap, T r2,
-                                                        unsigned short* __restrict__ nbr, int* __restrict__ nn,
-                                                        long stride, int max_nn, unsigned int* __restrict__ err,
+                                                        float lo_thr, float hi_thr, unsigned int* __restrict__ nbr,
+                                                        int* __restrict__ nn, long stride, int max_nn,
+                                                        unsigned int* __restrict__ err,
                                                         unsigned int* __restrict__ nn_max) {
-    typedef typename V4<T>::type T4;
     extern __shared__ __align__(128) unsigned char tile_raw[];
-    T4* sm = reinterpret_cast<T4*>(tile_raw);
+    float4* sm = reinterpret_cast<float4*>(tile_raw);
     __shared__ TileSh S;
+    __shared__ unsigned int segb[18][TXMAX + 3];  // absolute staging index of every cell start, per segment
     tile_layout(tg, blockIdx.x, csR, csI, S);
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     if (ib == ie) return;
-    if (!tile_stage<T>(pos, pos + n_real, S, sm, cap, err)) return;
     const int ncol = S.ncol;
+    for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+        int sg = e / ncol, j = e % ncol, r = sg >> 1;
+        segb[sg][j] = (sg & 1) ? S.oI[r] + (S.cI[r][j] - S.cI[r][0]) : S.oR[r] + (S.cR[r][j] - S.cR[r][0]);
+    }
+    if (!tile_stage<float>(pos32, pos32 + n_real, S, sm, cap, err)) return;  // (its barrier also covers segb)
+    const unsigned int self_base = S.oR[4] - S.cR[4][0];
     for (unsigned int i = ib + threadIdx.x; i < ie; i += blockDim.x) {
-        T4 xi = sm[S.oR[4] + (i - S.cR[4][0])];
+        const float4 xi = sm[self_base + i];
         int j = 1;
         while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
         int cnt = 0;
+        unsigned int pend = 0;
+        unsigned int* out = nbr + i;
 #pragma unroll 1
-        for (int r = 0; r < 9; ++r) {
-#pragma unroll 1
-            for (int part = 0; part < 2; ++part) {
-                const unsigned int* cc = part ? S.cI[r] : S.cR[r];
-                unsigned int a = cc[j - 1], e = cc[j + 2];
-                unsigned int base = (part ? S.oI[r] : S.oR[r]) - cc[0];
+        for (int sg = 0; sg < 18; ++sg) {
+            const unsigned int qe = segb[sg][j + 2];
 #pragma unroll 4
-                for (unsigned int q = a; q < e; ++q) {
-                    T4 xq = sm[base + q];
-                    T d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
-                    if (d2 < r2) {
-                        if (cnt < max_nn) nbr[pair_slot(cnt, stride, i)] = (unsigned short)(base + q);
+            for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
+                const float4 xq = sm[q];
+                const float d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
+                if (d2 < hi_thr) {
+                    if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
+                        if (cnt < max_nn) {
+                            if (cnt & 1) out[(long)(cnt >> 1) * stride] = pend | (q << 16);
+                            else pend = q;
+                        }
                         cnt++;
                     }
                 }
             }
         }
         // odd rows end with the particle itself, which the pair kernel skips
-        if ((cnt & 1) && cnt < max_nn) nbr[pair_slot(cnt, stride, i)] = (unsigned short)(S.oR[4] + (i - S.cR[4][0]));
+        if ((cnt & 1) && cnt < max_nn) out[(long)(cnt >> 1) * stride] = pend | ((self_base + i) << 16);
         if (cnt > max_nn) {
             atomicOr(err, ERR_NN_OVERFLOW);
             atomicMax(nn_max, (unsigned int)cnt);
@@ -214,9 +248,11 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             const unsigned int* row = nbr + i;
+            unsigned int nxt = sub < words ? __ldg(row + (long)sub * stride) : 0u;
 #pragma unroll 2
             for (int k = sub; k < words; k += P) {
-                const unsigned int pair = __ldg(row + (long)k * stride);
+                const unsigned int pair = nxt;
+                if (k + P < words) nxt = __ldg(row + (long)(k + P) * stride);
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
@@ -348,13 +384,33 @@ bool tile_fits(pd_vd h, unsigned int tmax) {
     return (long)tmax * h->pos_bytes <= SMEM_LIMIT && tmax <= 65535u;
 }
 
+// |d2_f32 - d2| for pairs near r: coordinates rounded to FP32 (relative 2^-24)
+// at magnitude <= X, differences and the 3-term sum rounded once more each.
+static double fp32_band(pd_vd h, double r) {
+    double X = 0;
+    for (int d = 0; d < 3; ++d)
+        X = std::max(X, std::max(std::fabs(h->lo[d] - 2 * h->g[d]), std::fabs(h->hi[d] + 2 * h->g[d])));
+    const double u = std::ldexp(1.0, -24);
+    double D = 2 * u * X + u * r;                       // per-component error of the FP32 difference
+    double e = 2 * std::sqrt(3.0) * r * D + 3 * D * D + 4 * u * (r * r + 1.0);
+    return 4 * e;                                       // safety factor 4
+}
+
 int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
-               unsigned int cap, double r_list, Buf& nbr, Buf& nn, long& stride, int& max_nn, cudaStream_t st) {
+               unsigned int cap, double r_list, Buf& pos32, Buf& nbr, Buf& nn, long& stride, int& max_nn,
+               cudaStream_t st) {
     long n = h->n_real;
     stride = ((n + 31) / 32) * 32;
     if (stride < 32) stride = 32;
-    int smem = (int)(cap * h->pos_bytes);
-    if (smem < 16) smem = 16;
+    long nt = h->n_total;
+    PD_TRY(pos32.ensure(sizeof(float4) * (size_t)(nt > 0 ? nt : 1)));
+    if (h->dtype == PD_F64)
+        pd::launch(k_pos32<double>, grid_for(nt, 256), 256, 0, st, (const double4*)h->pos, nt, pos32.as<float4>());
+    else
+        pd::launch(k_pos32<float>, grid_for(nt, 256), 256, 0, st, (const float4*)h->pos, nt, pos32.as<float4>());
+    PD_LAUNCH_CHECK();
+    double band = fp32_band(h, r_list);
+    float lo_thr = (float)(r_list * r_list - band), hi_thr = (float)(r_list * r_list + band);
     if (max_nn <= 0) {
         double vol = (h->hi[0] - h->lo[0]) * (h->hi[1] - h->lo[1]) * (h->hi[2] - h->lo[2]);
         double mean = (double)n / vol * 4.18879 * r_list * r_list * r_list;
@@ -362,20 +418,22 @@ int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR
     }
     max_nn = (max_nn + 1) & ~1;  // whole 32-bit words
     for (int attempt = 0; attempt < 3; ++attempt) {
+        int smem = (int)(cap * sizeof(float4));
+        if (smem < 16) smem = 16;
         PD_TRY(nbr.ensure(sizeof(unsigned short) * (size_t)stride * max_nn));
         PD_TRY(nn.ensure(sizeof(int) * (size_t)stride));
         PD_CUDA(cudaMemsetAsync(nn.p, 0, sizeof(int) * (size_t)stride, st));
         if (h->dtype == PD_F64) {
             PD_TRY(allow_smem(k_vtile_build<double>, smem));
-            pd::launch(k_vtile_build<double>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const double4*)h->pos, n, tg,
-                       csR, csI, cap, r_list * r_list, nbr.as<unsigned short>(), nn.as<int>(), stride, max_nn,
-                       &h->ctrl->err, &h->ctrl->nn_max);
+            pd::launch(k_vtile_build<double>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const double4*)h->pos,
+                       (const float4*)pos32.as<float4>(), n, tg, csR, csI, cap, r_list * r_list, lo_thr, hi_thr,
+                       nbr.as<unsigned int>(), nn.as<int>(), stride, max_nn, &h->ctrl->err, &h->ctrl->nn_max);
         } else {
             float rl = (float)r_list;
             PD_TRY(allow_smem(k_vtile_build<float>, smem));
-            pd::launch(k_vtile_build<float>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const float4*)h->pos, n, tg,
-                       csR, csI, cap, rl * rl, nbr.as<unsigned short>(), nn.as<int>(), stride, max_nn,
-                       &h->ctrl->err, &h->ctrl->nn_max);
+            pd::launch(k_vtile_build<float>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const float4*)h->pos,
+                       (const float4*)pos32.as<float4>(), n, tg, csR, csI, cap, rl * rl, lo_thr, hi_thr,
+                       nbr.as<unsigned int>(), nn.as<int>(), stride, max_nn, &h->ctrl->err, &h->ctrl->nn_max);
         }
         PD_LAUNCH_CHECK();
         PD_TRY(read_ctrl(h, st));

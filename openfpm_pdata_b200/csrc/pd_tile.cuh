@@ -16,9 +16,10 @@ struct TileGeom {
 int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles);
 int tile_sizes(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                unsigned int& tmax, unsigned int& cmax, cudaStream_t st);
-bool tile_fits(pd_vd h, unsigned int tmax);
+bool tile_fits(pd_vd h, unsigned int tmax);  // FP64/FP32 staging of the pair kernel fits
 int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
-               unsigned int cap, double r_list, Buf& nbr, Buf& nn, long& stride, int& max_nn, cudaStream_t st);
+               unsigned int cap, double r_list, Buf& pos32, Buf& nbr, Buf& nn, long& stride, int& max_nn,
+               cudaStream_t st);
 int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
             unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
             double* part, bool energy, int P, cudaStream_t st);
