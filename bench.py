@@ -113,16 +113,18 @@ def make_workload():
     return x, v, L
 
 
-TUNE = {"tiles": 1, "tx": 0, "tpp": 0}
+TUNE = {"tiles": 1, "tx": 0, "tpp": 0, "precision": "fp64"}
 
 
 def build_system(pd, x, v, L):
     lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
-    vd = pd.VectorDist(x.shape[0], lo, hi, bc, R_CUT + SKIN, dtype=np.float64,
-                       props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    mixed = TUNE["precision"] == "mixed"
+    pt = pd.PD_F32 if mixed else pd.PD_F64
+    vd = pd.VectorDist(x.shape[0], lo, hi, bc, R_CUT + SKIN, dtype=np.float64, props=[(pt, 3), (pt, 3)])
     vd.hostToDevicePos(x)
     vd.hostToDeviceProp(0, v)
-    md = pd.MD(vd, 0, 1, dt=DT, mass=MASS, skin=SKIN, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+    md = pd.MD(vd, 0, 1, dt=DT, mass=MASS, skin=SKIN, eps=EPS, sigma=SIGMA, r_cut=R_CUT,
+               precision=pd.PREC_MIXED if mixed else pd.PREC_FP64)
     md.set_tiles(bool(TUNE["tiles"]), TUNE["tx"], TUNE["tpp"])
     return vd, md
 
@@ -158,8 +160,11 @@ def main():
     ap.add_argument("--tiles", type=int, default=1, help="1: tiled shared-memory rows, 0: global-index rows")
     ap.add_argument("--tx", type=int, default=0, help="cells per tile along x (0: automatic)")
     ap.add_argument("--tpp", type=int, default=0, help="threads per particle in the pair kernel (0: 2)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64: plain FP64 path; mixed: FP32 cell-local positions, Kahan sums, FP64 wrap/energies")
     a = ap.parse_args()
-    TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp)
+    TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp, precision=a.precision)
+    mixed = a.precision == "mixed"
     if a.warmup < 3:
         a.warmup = 3
     world, rank, local = dist_setup(a.gpus)
@@ -231,8 +236,12 @@ def main():
     # = N * (32 B position record + 4 B row length + 4 B * mean row + 24 B force)
     f_ms, f_cnt = timers["force"]
     f_avg_s = f_ms / max(f_cnt, 1) / 1000.0
-    # tiled rows: 2-byte entries, the position record is staged once per tile (counted once)
-    alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
+    # tiled rows: 2-byte entries, the position record is staged once per tile (counted once);
+    # mixed form: 16-byte FP32 offset records and FP32 forces
+    if mixed:
+        alg_bytes = n * (16 + 4 + 2 * mean_nn + 12)
+    else:
+        alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
     traffic = read_traffic()
@@ -240,13 +249,16 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": n, "parallelism": "replicas" if world > 1 else "single",
+        "dtype": "f32+kahan/f64-energy" if mixed else "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD if not mixed else WORKLOAD.replace("FP64", "mixed-precision"),
+                   "particles": n, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (positions 131 MB + Verlet list ~1.1 GB per replica)",
                    "list_rebuilds_in_timed_region": builds, "mean_verlet_row": round(mean_nn, 2),
                    "max_verlet_row": max_nn},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_vtile_lj<double>" if a.tiles else "k_lj_verlet<double>",
+                     "traffic": traffic,
+                     "kernel": "k_vtile_lj_mixed" if mixed else ("k_vtile_lj<double>" if a.tiles else
+                                                                  "k_lj_verlet<double>"),
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0},
         "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in timers.items()},

@@ -108,12 +108,17 @@ typedef struct {
     double eps, sigma, r_cut;
 } pd_lj_params_t;
 
+/* integrator precision */
+#define PD_PREC_FP64 0  /* positions, velocities, forces in the vector's dtype */
+#define PD_PREC_MIXED 1 /* FP32 cell-local positions and pair math, Kahan sums, FP64 wrap and energies */
+
 /* velocity-Verlet parameters */
 typedef struct {
     double dt, mass, skin;
-    int vel_prop;   /* property id holding velocities (3 comps, dtype of the vector) */
-    int force_prop; /* property id receiving forces   (3 comps, dtype of the vector) */
+    int vel_prop;   /* property id holding velocities (3 comps; PD_F32 in the mixed form) */
+    int force_prop; /* property id receiving forces   (3 comps; PD_F32 in the mixed form) */
     int use_cell_list; /* 1: force from the cell list every step (no Verlet list) */
+    int precision;     /* PD_PREC_FP64 or PD_PREC_MIXED (the vector must then be PD_F64) */
 } pd_md_params_t;
 
 /* ---- library ------------------------------------------------------------ */

@@ -13,6 +13,7 @@
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
 #include "pd_tile.cuh"
+#include "pd_mixed.cuh"
 
 namespace pd {
 
@@ -241,6 +242,11 @@ struct pd_md_s {
     long tstride = 0;
     int tmax_nn = 0;
     pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
+    // precision form: FP32 cell-local offsets (all particles), their value at the
+    // last build (real particles) and the constant parts of the image offsets
+    bool mixed = false;
+    bool off_valid = false;  // `off` holds the authoritative state (after the first build)
+    pd::Buf off, offb, offK;
     long builds = 0, steps = 0;
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
@@ -359,6 +365,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
 // wrap, sort the real particles into cell order, periodic images, neighbour structure
 static int md_rebuild(pd_md md, cudaStream_t st) {
     pd_vd h = md->h;
+    if (md->mixed && md->off_valid) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));
     h->n_total = h->n_real;
     h->img_valid = false;
     PD_TRY(wrap_positions(h, h->n_real, st));
@@ -372,9 +379,20 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
         PD_TRY(cl_build(h, md->cl, h->n_total, nullptr, st));
     } else {
         md->tiles_active = false;
-        if (md->use_tiles) PD_TRY(md_tiles(md, sort_cl, st));
-        if (!md->tiles_active) PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
-        PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
+        if (md->use_tiles || md->mixed) PD_TRY(md_tiles(md, sort_cl, st));
+        if (md->mixed) {
+            if (!md->tiles_active) {
+                set_error("precision form: a tile's neighbourhood does not fit in shared memory");
+                return PD_EOVERFLOW;
+            }
+            PD_TRY(mixed_from_positions(h, md->vl->cl, md->off, md->offK, st));
+            md->off_valid = true;
+            PD_TRY(md->offb.ensure(sizeof(float4) * (size_t)(h->n_real > 0 ? h->n_real : 1)));
+            PD_CUDA(cudaMemcpyAsync(md->offb.p, md->off.p, sizeof(float4) * h->n_real, cudaMemcpyDeviceToDevice, st));
+        } else {
+            if (!md->tiles_active) PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
+            PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
+        }
     }
     h->epoch++;
     md->builds++;
@@ -382,6 +400,10 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
 }
 
 static int md_forces(pd_md md, cudaStream_t st) {
+    if (md->mixed)
+        return mixed_lj(md->h, md->vl->cl, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(),
+                        md->tcap, md->off, md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop,
+                        md->tpart.as<double>(), md->tile_p, st);
     if (md->tiles_active)
         return tile_lj(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                        md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop, md->tpart.as<double>(), true,
@@ -455,9 +477,16 @@ int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* mp, pd
         set_error("pd_md_create: bad property ids");
         return PD_EINVAL;
     }
-    if (h->props[mp->vel_prop].type != h->dtype || h->props[mp->vel_prop].ncomp != 3 ||
-        h->props[mp->force_prop].type != h->dtype || h->props[mp->force_prop].ncomp != 3) {
-        set_error("pd_md_create: velocity and force must be 3-component properties of the vector's dtype");
+    if (mp->precision != PD_PREC_FP64 && mp->precision != PD_PREC_MIXED) return PD_EINVAL;
+    int want = mp->precision == PD_PREC_MIXED ? PD_F32 : h->dtype;
+    if (h->props[mp->vel_prop].type != want || h->props[mp->vel_prop].ncomp != 3 ||
+        h->props[mp->force_prop].type != want || h->props[mp->force_prop].ncomp != 3) {
+        set_error("pd_md_create: velocity and force must be 3-component properties of the vector's dtype "
+                  "(PD_F32 in the mixed form)");
+        return PD_EINVAL;
+    }
+    if (mp->precision == PD_PREC_MIXED && (h->dtype != PD_F64 || mp->use_cell_list)) {
+        set_error("pd_md_create: the mixed form needs a PD_F64 vector and the Verlet list");
         return PD_EINVAL;
     }
     if (!(mp->dt > 0) || !(mp->mass > 0) || !(lj->r_cut > 0) || !(lj->sigma > 0)) return PD_EINVAL;
@@ -471,6 +500,7 @@ int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* mp, pd
     md->h = h;
     md->lj = *lj;
     md->mp = *mp;
+    md->mixed = mp->precision == PD_PREC_MIXED;
     int r;
     if (mp->use_cell_list) {
         r = pd_celllist_create(h, lj->r_cut, PD_CL_NON_SYMMETRIC, 1, (double)1.013f, &md->cl);
@@ -506,6 +536,9 @@ int pd_md_destroy(pd_md md) {
     md->tnn.release();
     md->tpart.release();
     md->pos32.release();
+    md->off.release();
+    md->offb.release();
+    md->offK.release();
     for (int i = 0; i < 8; ++i)
         if (md->ev[i]) cudaEventDestroy(md->ev[i]);
     delete md;
@@ -532,7 +565,10 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         unsigned int rebuilt = 0;
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[0], st));
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-        if (h->dtype == PD_F64)
+        if (md->mixed)
+            PD_TRY(mixed_kick_drift(h, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+                                    md->mp.dt, st));
+        else if (h->dtype == PD_F64)
             pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,
                                                               (const double*)F.d, h->cap, n, half, md->mp.dt,
                                                               &h->ctrl->maxdisp2);
@@ -555,13 +591,18 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         if (rb) {
             PD_TRY(md_rebuild(md, st));
             rebuilt = 1;
+        } else if (md->mixed) {
+            PD_TRY(mixed_replay(h, md->off, md->offK, st));
         } else {
             PD_TRY(ghost_replay(h, 0ul, true, nullptr, h->n_img, st));
         }
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[3], st));
         PD_TRY(md_forces(md, st));
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[4], st));
-        if (h->dtype == PD_F64)
+        if (md->mixed)
+            PD_TRY(mixed_kick(h, md->mp.vel_prop, md->mp.force_prop, md->nblk, half, md->mp.mass,
+                              md->kpart.as<double>(), st));
+        else if (h->dtype == PD_F64)
             pd::launch(k_kick<double>, md->nblk, FBLOCK, 0, st, (double*)V.d, (const double*)F.d, h->cap, n, half,
                                                         md->mp.mass, md->kpart.as<double>());
         else
@@ -600,6 +641,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             md->cnt[3] += 1;
         }
     }
+    if (md->mixed) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));  // the vector's positions are current
     if (E && steps > 0) {
         PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));
     }

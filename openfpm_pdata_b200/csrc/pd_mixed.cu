@@ -1,0 +1,414 @@
+// pd_mixed.cu -- precision form of the LJ integrator: FP32 cell-local positions,
+// FP32 pair math with compensated (Kahan) sums, FP64 only for the periodic wrap
+// at rebuilds and for the global energy / virial reductions.
+//
+// State between rebuilds (all particles, images included, in the tiled order):
+//   off[k] = (x - c, y - c, z - c, cell id) : FP32 offset from the centre of the
+//            particle's cell at the last rebuild (cell grid of side r_cut+skin);
+//   v, f   : FP32 properties of the vector.
+// A pair displacement is formed from the offsets and the cell difference
+// (dx = (o_i - o_j) + (c_i - c_j) * s), so its rounding error is set by the
+// offset magnitude (<= 1.5 s), not by the box size.  In a tile, staged records
+// are rewritten once in shared memory: y and z are shifted by the row's cell
+// difference to the tile's centre row (|.| <= 2.5 s) and w holds the record's
+// cell column in the tile, so the pair loop forms
+//   dx = fma(col_i - col_j, s_x, x_i - x_j), dy = y_i - y_j, dz = z_i - z_j.
+// Per-particle force, energy and virial sums are accumulated in FP32 over the
+// two entries of a row word and added to a Kahan-compensated FP32 accumulator
+// (Kahan 1965); lanes sharing a particle combine in FP64; block energies in FP64.
+#include "pd_device.cuh"
+#include "pd_internal.cuh"
+#include "pd_lj.cuh"
+#include "pd_mixed.cuh"
+#include "pd_tile.cuh"
+
+namespace pd {
+
+struct TileShM {
+    unsigned int cR[9][TXMAX + 3];
+    unsigned int cI[9][TXMAX + 3];
+    unsigned int oR[9], oI[9];
+    unsigned int total;
+    int ncol;
+    unsigned long long bar;
+    unsigned int segb[18][TXMAX + 3];
+};
+
+// cell centres of the grid
+struct CellGeom {
+    double lo[3], sp[3];
+    int gs[3], pad;
+    __device__ __forceinline__ void centre(unsigned int c, double& cx, double& cy, double& cz) const {
+        int i0 = (int)(c % (unsigned)gs[0]);
+        int i1 = (int)((c / (unsigned)gs[0]) % (unsigned)gs[1]);
+        int i2 = (int)(c / ((unsigned)gs[0] * (unsigned)gs[1]));
+        cx = lo[0] + ((double)(i0 - pad) + 0.5) * sp[0];
+        cy = lo[1] + ((double)(i1 - pad) + 0.5) * sp[1];
+        cz = lo[2] + ((double)(i2 - pad) + 0.5) * sp[2];
+    }
+};
+
+// positions -> offsets from the cell centre (all n particles)
+__global__ void k_x64_to_off(const double4* __restrict__ pos, long n, Grid<double> G, CellGeom C,
+                             float4* __restrict__ off, unsigned int* __restrict__ err) {
+    unsigned int bad = 0;
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        double4 r = ld4(pos, k);
+        unsigned int c = (unsigned int)G.cell(r.x, r.y, r.z, bad);
+        double cx, cy, cz;
+        C.centre(c, cx, cy, cz);
+        off[k] = make_float4((float)(r.x - cx), (float)(r.y - cy), (float)(r.z - cz), __uint_as_float(c));
+    }
+    if (bad) atomicOr(err, ERR_CELL_RANGE);
+}
+
+// offsets -> positions (real particles)
+__global__ void k_off_to_x64(const float4* __restrict__ off, long n, CellGeom C, double4* __restrict__ pos) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        float4 o = off[k];
+        double cx, cy, cz;
+        C.centre(__float_as_uint(o.w), cx, cy, cz);
+        st4(pos, k, make_double4(cx + (double)o.x, cy + (double)o.y, cz + (double)o.z, 0.0));
+    }
+}
+
+// image offset = source offset + K, K formed in FP64 at the rebuild
+__global__ void k_image_k(const double4* __restrict__ pos, const float4* __restrict__ off, long n_real, long m,
+                          const int* __restrict__ src, CellGeom C, float4* __restrict__ K) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < m; k += (long)gridDim.x * blockDim.x) {
+        int s = src[k];
+        double4 xi = ld4(pos, n_real + k), xs = ld4(pos, s);
+        double ci[3], cs[3];
+        C.centre(__float_as_uint(off[n_real + k].w), ci[0], ci[1], ci[2]);
+        C.centre(__float_as_uint(off[s].w), cs[0], cs[1], cs[2]);
+        K[k] = make_float4((float)((xi.x - ci[0]) - (xs.x - cs[0])), (float)((xi.y - ci[1]) - (xs.y - cs[1])),
+                           (float)((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
+    }
+}
+
+__global__ void k_replay32(float4* __restrict__ off, long n_real, long m, const int* __restrict__ src,
+                           const float4* __restrict__ K) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < m; k += (long)gridDim.x * blockDim.x) {
+        float4 o = off[src[k]], q = K[k];
+        float4 r = off[n_real + k];
+        r.x = o.x + q.x;
+        r.y = o.y + q.y;
+        r.z = o.z + q.z;
+        off[n_real + k] = r;
+    }
+}
+
+// v += h f ; o += dt v ; largest |o - o_build|^2
+__global__ void __launch_bounds__(256) k_kick_drift32(float4* __restrict__ off, const float4* __restrict__ ob,
+                                                      float* __restrict__ v, const float* __restrict__ f, long cap,
+                                                      long n, float half, float dt,
+                                                      unsigned long long* __restrict__ maxd2) {
+    double mx = 0;
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
+        float4 o = off[i];
+        float vx = v[i] + half * f[i];
+        float vy = v[cap + i] + half * f[cap + i];
+        float vz = v[2 * cap + i] + half * f[2 * cap + i];
+        o.x += dt * vx;
+        o.y += dt * vy;
+        o.z += dt * vz;
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        off[i] = o;
+        float4 b = ob[i];
+        float dx = o.x - b.x, dy = o.y - b.y, dz = o.z - b.z;
+        mx = fmax(mx, (double)dist2(dx, dy, dz));
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
+}
+
+__global__ void __launch_bounds__(256) k_kick32(float* __restrict__ v, const float* __restrict__ f, long cap, long n,
+                                                float half, double mass, double* __restrict__ part) {
+    double ke = 0;
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
+        float vx = v[i] + half * f[i];
+        float vy = v[cap + i] + half * f[cap + i];
+        float vz = v[2 * cap + i] + half * f[2 * cap + i];
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        ke += 0.5 * mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+    }
+    ke = block_sum<double, 256>(ke);
+    if (threadIdx.x == 0) part[blockIdx.x] = ke;
+}
+
+struct Kahan {
+    float s, c;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+template <int P>
+__global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj_mixed(const float4* __restrict__ off, long n_real,
+                                                             TileGeom tg, const unsigned int* __restrict__ csR,
+                                                             const unsigned int* __restrict__ csI, unsigned int cap,
+                                                             const unsigned int* __restrict__ nbr,
+                                                             const int* __restrict__ nn, long stride, float sx,
+                                                             float sy, float sz, LJP<float> Pr, float* __restrict__ f,
+                                                             long fcap, double* __restrict__ part,
+                                                             unsigned int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    float4* sm = reinterpret_cast<float4*>(tile_raw);
+    __shared__ TileShM S;
+    {
+        long t = blockIdx.x;
+        int tx = (int)(t % tg.ntx);
+        long rest = t / tg.ntx;
+        int y = (int)(rest % tg.ny) + tg.pad;
+        int z = (int)(rest / tg.ny) + tg.pad;
+        int x0 = tg.pad + tx * tg.TX;
+        int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
+        int ncol = x1 - x0 + 3;
+        for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+            int img = e >= 9 * ncol;
+            int ee = img ? e - 9 * ncol : e;
+            int r = ee / ncol, j = ee % ncol;
+            int dz = r / 3 - 1, dy = r % 3 - 1;
+            long c = (long)(x0 - 1 + j) + (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
+            if (img) S.cI[r][j] = csI[c];
+            else S.cR[r][j] = csR[c];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int o = 0;
+            for (int r = 0; r < 9; ++r) {
+                S.oR[r] = o;
+                o += S.cR[r][ncol - 1] - S.cR[r][0];
+                S.oI[r] = o;
+                o += S.cI[r][ncol - 1] - S.cI[r][0];
+            }
+            S.total = o;
+            S.ncol = ncol;
+        }
+        __syncthreads();
+    }
+    const int ncol = S.ncol;
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][ncol - 2];
+    double pe = 0, vir = 0;
+    bool ok = ib != ie && S.total <= cap;
+    if (ib != ie && S.total > cap && threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+    if (ok) {
+        for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+            int sg = e / ncol, j = e % ncol, r = sg >> 1;
+            S.segb[sg][j] = (sg & 1) ? S.oI[r] + (S.cI[r][j] - S.cI[r][0]) : S.oR[r] + (S.cR[r][j] - S.cR[r][0]);
+        }
+        if (threadIdx.x == 0) mbar_init(&S.bar, 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(float4));
+            const int nc = ncol - 1;
+            for (int r = 0; r < 9; ++r) {
+                unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+                if (lr) bulk_g2s(sm + S.oR[r], off + S.cR[r][0], lr * (unsigned int)sizeof(float4), &S.bar);
+                unsigned int li = S.cI[r][nc] - S.cI[r][0];
+                if (li) bulk_g2s(sm + S.oI[r], off + n_real + S.cI[r][0], li * (unsigned int)sizeof(float4), &S.bar);
+            }
+        }
+        bool waited = mbar_wait_bounded(&S.bar, 0, 1u << 24);
+        if (!waited) {
+            atomicOr(err, ERR_TIMEOUT);
+            mbar_wait_bounded(&S.bar, 0, 1u << 24);
+        }
+        ok = __syncthreads_and(waited ? 1 : 0) != 0;
+    }
+    if (ok) {
+        // rewrite the staged records: y/z relative to the centre row, w = cell column
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int sg = warp; sg < 18; sg += FBLOCK_T / 32) {
+            const int r = sg >> 1;
+            const float shy = (float)(r % 3 - 1) * sy, shz = (float)(r / 3 - 1) * sz;
+            for (unsigned int k = S.segb[sg][0] + lane; k < S.segb[sg][ncol - 1]; k += 32) {
+                int j = 0;
+                while (j < ncol - 2 && S.segb[sg][j + 1] <= k) ++j;
+                float4 q = sm[k];
+                q.y += shy;
+                q.z += shz;
+                q.w = (float)j;
+                sm[k] = q;
+            }
+        }
+        __syncthreads();
+        const unsigned int base = S.oR[4] - S.cR[4][0];
+        const int sub = threadIdx.x % P;
+        const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
+        for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
+            const unsigned int i = ib + t / P;
+            const bool active = i < ie;
+            const unsigned int li = base + i;
+            const float4 xi = sm[active ? li : 0];
+            const int words = active ? (nn[i] + 1) >> 1 : 0;
+            Kahan kx = {0.f, 0.f}, ky = {0.f, 0.f}, kz = {0.f, 0.f}, ke = {0.f, 0.f}, kw = {0.f, 0.f};
+            const unsigned int* row = nbr + i;
+            unsigned int nxt = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+#pragma unroll 2
+            for (int k = sub; k < words; k += P) {
+                const unsigned int pair = nxt;
+                if (k + P < words) nxt = __ldg(row + (long)(k + P) * stride);
+                float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
+                    const float4 xq = sm[l];
+                    const float dx = fmaf(xi.w - xq.w, sx, xi.x - xq.x);
+                    const float dy = xi.y - xq.y, dz = xi.z - xq.z;
+                    const float r2 = dist2(dx, dy, dz);
+                    if (r2 < Pr.rc2 && l != li) {
+                        float ir2 = recip(r2);
+                        float s2 = Pr.sig2 * ir2;
+                        float s6 = s2 * s2 * s2;
+                        float ff = Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f);
+                        fx += ff * dx;
+                        fy += ff * dy;
+                        fz += ff * dz;
+                        e += Pr.eps4 * s6 * (s6 - 1.f);
+                        w += ff * r2;
+                    }
+                }
+                kx.add(fx);
+                ky.add(fy);
+                kz.add(fz);
+                ke.add(e);
+                kw.add(w);
+            }
+            double Fx = kx.value(), Fy = ky.value(), Fz = kz.value(), Ee = ke.value(), Ww = kw.value();
+#pragma unroll
+            for (int o = 1; o < P; o <<= 1) {
+                Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+                Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+                Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+                Ee += __shfl_xor_sync(0xffffffffu, Ee, o);
+                Ww += __shfl_xor_sync(0xffffffffu, Ww, o);
+            }
+            if (active && sub == 0) {
+                f[i] = (float)Fx;
+                f[fcap + i] = (float)Fy;
+                f[2 * fcap + i] = (float)Fz;
+                pe += 0.5 * Ee;
+                vir += 0.5 * Ww;
+            }
+        }
+    }
+    pe = block_sum<double, FBLOCK_T>(pe);
+    vir = block_sum<double, FBLOCK_T>(vir);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = pe;
+        part[2 * blockIdx.x + 1] = vir;
+    }
+}
+
+// ---------------------------------------------------------------------------
+static CellGeom cell_geom(pd_cl cl) {
+    CellGeom C;
+    for (int d = 0; d < 3; ++d) {
+        C.lo[d] = cl->box_lo[d];
+        C.sp[d] = cl->spacing[d];
+        C.gs[d] = cl->gs[d];
+    }
+    C.pad = cl->pad;
+    return C;
+}
+
+int mixed_from_positions(pd_vd h, pd_cl cl, Buf& off, Buf& K, cudaStream_t st) {
+    long nt = h->n_total, m = h->n_img;
+    PD_TRY(off.ensure(sizeof(float4) * (size_t)(h->cap > 0 ? h->cap : 1)));
+    PD_TRY(K.ensure(sizeof(float4) * (size_t)(m > 0 ? m : 1)));
+    Grid<double> G;
+    for (int d = 0; d < 3; ++d) {
+        G.lo[d] = cl->box_lo[d];
+        G.sp[d] = cl->spacing[d];
+        G.gs[d] = cl->gs[d];
+    }
+    G.pad = cl->pad;
+    CellGeom C = cell_geom(cl);
+    if (nt > 0)
+        pd::launch(k_x64_to_off, grid_for(nt, 256), 256, 0, st, (const double4*)h->pos, nt, G, C, off.as<float4>(),
+                   &h->ctrl->err);
+    if (m > 0)
+        pd::launch(k_image_k, grid_for(m, 256), 256, 0, st, (const double4*)h->pos, (const float4*)off.as<float4>(),
+                   h->n_real, m, (const int*)h->img_src.as<int>(), C, K.as<float4>());
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_to_positions(pd_vd h, pd_cl cl, const Buf& off, cudaStream_t st) {
+    long n = h->n_real;
+    if (n > 0)
+        pd::launch(k_off_to_x64, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n, cell_geom(cl),
+                   (double4*)h->pos);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_replay(pd_vd h, Buf& off, const Buf& K, cudaStream_t st) {
+    long m = h->n_img;
+    if (m > 0)
+        pd::launch(k_replay32, grid_for(m, 256), 256, 0, st, off.as<float4>(), h->n_real, m,
+                   (const int*)h->img_src.as<int>(), (const float4*)K.as<float4>());
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
+                     double dt, cudaStream_t st) {
+    Prop& V = h->props[vel_prop];
+    Prop& F = h->props[force_prop];
+    pd::launch(k_kick_drift32, nblk, 256, 0, st, off.as<float4>(), (const float4*)ob.as<float4>(), (float*)V.d,
+               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, &h->ctrl->maxdisp2);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_kick(pd_vd h, int vel_prop, int force_prop, int nblk, double half, double mass, double* kpart,
+               cudaStream_t st) {
+    Prop& V = h->props[vel_prop];
+    Prop& F = h->props[force_prop];
+    pd::launch(k_kick32, nblk, 256, 0, st, (float*)V.d, (const float*)F.d, h->cap, h->n_real, (float)half, mass,
+               kpart);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+template <int P>
+static int launch_mixed(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                        unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, float sx,
+                        float sy, float sz, const LJP<float>& LP, float* f, double* part, cudaStream_t st) {
+    int smem = (int)(cap * sizeof(float4));
+    if (smem < 16) smem = 16;
+    PD_CUDA(cudaFuncSetAttribute(k_vtile_lj_mixed<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    pd::launch(k_vtile_lj_mixed<P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st, (const float4*)off.as<float4>(),
+               h->n_real, tg, csR, csI, cap, (const unsigned int*)nbr.as<unsigned int>(), (const int*)nn.as<int>(),
+               stride, sx, sy, sz, LP, f, h->cap, part, &h->ctrl->err);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+             unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj,
+             int force_prop, double* part, int P, cudaStream_t st) {
+    LJP<float> LP;
+    LP.eps24 = (float)(24.0 * lj.eps);
+    LP.eps4 = (float)(4.0 * lj.eps);
+    LP.sig2 = (float)(lj.sigma * lj.sigma);
+    float rc = (float)lj.r_cut;
+    LP.rc2 = rc * rc;
+    float* f = (float*)h->props[force_prop].d;
+    float sx = (float)cl->spacing[0], sy = (float)cl->spacing[1], sz = (float)cl->spacing[2];
+    if (P == 1) return launch_mixed<1>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
+    if (P == 4) return launch_mixed<4>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
+    return launch_mixed<2>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
+}
+
+}  // namespace pd

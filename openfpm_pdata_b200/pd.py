@@ -59,9 +59,13 @@ class LJParams(ctypes.Structure):
     _fields_ = [("eps", ctypes.c_double), ("sigma", ctypes.c_double), ("r_cut", ctypes.c_double)]
 
 
+PREC_FP64, PREC_MIXED = 0, 1
+
+
 class MDParams(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("mass", ctypes.c_double), ("skin", ctypes.c_double),
-                ("vel_prop", ctypes.c_int), ("force_prop", ctypes.c_int), ("use_cell_list", ctypes.c_int)]
+                ("vel_prop", ctypes.c_int), ("force_prop", ctypes.c_int), ("use_cell_list", ctypes.c_int),
+                ("precision", ctypes.c_int)]
 
 
 _lib = None
@@ -378,10 +382,10 @@ class MD:
     """Velocity-Verlet LJ driver over a VectorDist holding only real particles."""
 
     def __init__(self, vd, vel_prop, force_prop, dt=0.005, mass=1.0, skin=0.3, eps=1.0, sigma=1.0, r_cut=2.5,
-                 use_cell_list=False):
+                 use_cell_list=False, precision=PREC_FP64):
         self.vd = vd
         self.lj = LJParams(eps, sigma, r_cut)
-        self.mp = MDParams(dt, mass, skin, vel_prop, force_prop, int(bool(use_cell_list)))
+        self.mp = MDParams(dt, mass, skin, vel_prop, force_prop, int(bool(use_cell_list)), int(precision))
         h = ctypes.c_void_p()
         check(lib().pd_md_create(vd.h, ctypes.byref(self.lj), ctypes.byref(self.mp), ctypes.byref(h)))
         self.h = h

@@ -31,7 +31,7 @@ int main(int argc, char** argv) {
     vl.download(counts, off, idx);
     printf("pairs %ld\n", off.empty() ? 0L : off.back());
     vd.map();  // drop the ghost before handing the vector to the integrator
-    pd::md_lj md(vd, pd_lj_params_t{1.0, 1.0, 2.5}, pd_md_params_t{0.005, 1.0, 0.3, 0, 1, 0});
+    pd::md_lj md(vd, pd_lj_params_t{1.0, 1.0, 2.5}, pd_md_params_t{0.005, 1.0, 0.3, 0, 1, 0, PD_PREC_FP64});
     std::vector<double> E = md.run(steps);
     for (int s = 0; s < steps; ++s) printf("E %.17g %.17g %.17g %.0f\n", E[4 * s], E[4 * s + 1], E[4 * s + 2], E[4 * s + 3]);
     return 0;
