@@ -121,6 +121,15 @@ typedef struct {
     int precision;     /* PD_PREC_FP64 or PD_PREC_MIXED (the vector must then be PD_F64) */
 } pd_md_params_t;
 
+/* weakly compressible SPH parameters (cubic spline of support 2h, Tait EOS,
+ * Monaghan artificial viscosity, gravity along z); property ids of the vector */
+typedef struct {
+    double h, mass, c0, rho0, alpha, gz;
+    int rho_prop;  /* density (1 comp, dtype of the vector)            */
+    int drho_prop; /* density rate (1 comp, dtype of the vector)       */
+    int type_prop; /* PD_I32: 0 fluid, 1 fixed wall particle           */
+} pd_sph_params_t;
+
 /* ---- library ------------------------------------------------------------ */
 const char* pd_last_error(void);
 /* number of CUDA kernels this library has launched so far (all handles) */
@@ -240,6 +249,13 @@ int pd_selftest_recip(int dtype, const void* x_host, void* out_host, long n);
  * skin/2 (skin <= 0: every step). */
 int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* md, pd_md* out);
 int pd_md_destroy(pd_md md);
+/* WCSPH driver on the same integrator (no reference counterpart; the reference's
+ * pair-functor pattern is vector_dist_gpu_unit_tests.cu:46-119): kick-drift-kick
+ * of velocity and density, fluid particles move, wall particles are fixed and
+ * their density evolves.  mp: dt, skin, vel_prop, force_prop (= acceleration);
+ * the box must be non-periodic.  pd_md_run's E then holds KE of the fluid,
+ * sum of densities, 0, rebuilt. */
+int pd_sph_create(pd_vd h, const pd_sph_params_t* sp, const pd_md_params_t* mp, pd_md* out);
 /* run `steps` steps; E (if non-NULL) receives [steps][4] = KE, PE, virial, rebuilt */
 int pd_md_run(pd_md md, int steps, void* stream, double* E);
 /* statistics: builds so far, steps so far, device-side error word */

@@ -14,6 +14,7 @@
 #include "pd_lj.cuh"
 #include "pd_tile.cuh"
 #include "pd_mixed.cuh"
+#include "pd_sph.cuh"
 
 namespace pd {
 
@@ -244,6 +245,9 @@ struct pd_md_s {
     pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
     // precision form: FP32 cell-local offsets (all particles), their value at the
     // last build (real particles) and the constant parts of the image offsets
+    int physics = 0;  // 0: Lennard-Jones, 1: WCSPH
+    pd_sph_params_t sp;
+    pd::Buf aux, rpart;
     bool mixed = false;
     bool off_valid = false;  // `off` holds the authoritative state (after the first build)
     pd::Buf off, offb, offK;
@@ -353,7 +357,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
     unsigned int tmax = 0, cmax = 0;
     PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax, cmax, st));
-    if (!tile_fits(h, tmax)) return PD_OK;  // stays on the global-index list
+    if (md->physics == 1 ? !sph_tile_fits(h, tmax) : !tile_fits(h, tmax)) return PD_OK;  // stays on global rows
     md->tcap = tmax;
     PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                       md->vl->r_cut, md->pos32, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
@@ -372,6 +376,7 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
     pd_cl sort_cl = md->mp.use_cell_list ? md->cl : md->vl->cl;
     PD_TRY(cl_build(h, sort_cl, h->n_real, nullptr, st));
     unsigned long mask = 1ul << md->mp.vel_prop;
+    if (md->physics == 1) mask |= (1ul << md->sp.rho_prop) | (1ul << md->sp.type_prop);
     PD_TRY(cl_reorder(h, sort_cl, h->n_real, mask, true, true, st));
     if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
     PD_TRY(ghost_generate(h, 0, true, st));
@@ -379,7 +384,14 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
         PD_TRY(cl_build(h, md->cl, h->n_total, nullptr, st));
     } else {
         md->tiles_active = false;
-        if (md->use_tiles || md->mixed) PD_TRY(md_tiles(md, sort_cl, st));
+        if (md->use_tiles || md->mixed || md->physics == 1) PD_TRY(md_tiles(md, sort_cl, st));
+        if (md->physics == 1) {
+            if (!md->tiles_active) {
+                set_error("SPH: a tile's neighbourhood does not fit in shared memory");
+                return PD_EOVERFLOW;
+            }
+            PD_TRY(sph_pack(h, md->sp, md->mp.vel_prop, md->aux, st));
+        }
         if (md->mixed) {
             if (!md->tiles_active) {
                 set_error("precision form: a tile's neighbourhood does not fit in shared memory");
@@ -400,6 +412,9 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
 }
 
 static int md_forces(pd_md md, cudaStream_t st) {
+    if (md->physics == 1)
+        return sph_rates(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->tcap, md->tnbr, md->tnn,
+                         md->tstride, md->aux, md->sp, md->mp.force_prop, md->tile_p, st);
     if (md->mixed)
         return mixed_lj(md->h, md->vl->cl, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(),
                         md->tcap, md->off, md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop,
@@ -522,6 +537,52 @@ int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* mp, pd
     return PD_OK;
 }
 
+int pd_sph_create(pd_vd h, const pd_sph_params_t* sp, const pd_md_params_t* mp, pd_md* out) {
+    if (!h || !sp || !mp || !out) return PD_EINVAL;
+    int np = (int)h->props.size();
+    auto okp = [&](int p, int type, int nc) {
+        return p >= 0 && p < np && h->props[p].type == type && h->props[p].ncomp == nc;
+    };
+    int D = h->dtype;
+    if (!okp(mp->vel_prop, D, 3) || !okp(mp->force_prop, D, 3) || !okp(sp->rho_prop, D, 1) ||
+        !okp(sp->drho_prop, D, 1) || !okp(sp->type_prop, PD_I32, 1)) {
+        set_error("pd_sph_create: velocity/acceleration (3 comps), density and its rate (1 comp) in the vector's "
+                  "dtype, type as PD_I32");
+        return PD_EINVAL;
+    }
+    for (int d = 0; d < 3; ++d)
+        if (h->bc[d] == PD_PERIODIC) {
+            set_error("pd_sph_create: the SPH driver supports non-periodic boxes (walls) only");
+            return PD_EINVAL;
+        }
+    if (!(mp->dt > 0) || !(sp->h > 0) || !(sp->mass > 0) || !(sp->rho0 > 0) || mp->use_cell_list ||
+        mp->precision != PD_PREC_FP64)
+        return PD_EINVAL;
+    pd_md md = new pd_md_s();
+    md->h = h;
+    md->mp = *mp;
+    md->sp = *sp;
+    md->physics = 1;
+    md->lj.eps = md->lj.sigma = 1.0;
+    md->lj.r_cut = 2.0 * sp->h;
+    double rlist = 2.0 * sp->h + (mp->skin > 0 ? mp->skin : 0);
+    int r = pd_verlet_create(h, rlist, &md->vl);
+    if (r != PD_OK) {
+        delete md;
+        return r;
+    }
+    md->nblk = force_blocks(h->n_real);
+    if ((r = md->fpart.ensure(sizeof(double) * 2 * md->nblk)) != PD_OK ||
+        (r = md->kpart.ensure(sizeof(double) * md->nblk)) != PD_OK ||
+        (r = md->rpart.ensure(sizeof(double) * 2 * md->nblk)) != PD_OK ||
+        (r = md->xb.ensure((size_t)(h->n_real > 0 ? h->n_real : 1) * h->pos_bytes)) != PD_OK) {
+        pd_md_destroy(md);
+        return r;
+    }
+    *out = md;
+    return PD_OK;
+}
+
 int pd_md_destroy(pd_md md) {
     if (!md) return PD_EINVAL;
     if (md->vl) pd_verlet_destroy(md->vl);
@@ -539,6 +600,8 @@ int pd_md_destroy(pd_md md) {
     md->off.release();
     md->offb.release();
     md->offK.release();
+    md->aux.release();
+    md->rpart.release();
     for (int i = 0; i < 8; ++i)
         if (md->ev[i]) cudaEventDestroy(md->ev[i]);
     delete md;
@@ -565,7 +628,10 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         unsigned int rebuilt = 0;
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[0], st));
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-        if (md->mixed)
+        if (md->physics == 1)
+            PD_TRY(sph_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
+                                  md->mp.dt, st));
+        else if (md->mixed)
             PD_TRY(mixed_kick_drift(h, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
                                     md->mp.dt, st));
         else if (h->dtype == PD_F64)
@@ -599,7 +665,10 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[3], st));
         PD_TRY(md_forces(md, st));
         if (md->timing) PD_CUDA(cudaEventRecord(md->ev[4], st));
-        if (md->mixed)
+        if (md->physics == 1)
+            PD_TRY(sph_kick(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->nblk, md->mp.dt,
+                            md->kpart.as<double>(), md->rpart.as<double>(), st));
+        else if (md->mixed)
             PD_TRY(mixed_kick(h, md->mp.vel_prop, md->mp.force_prop, md->nblk, half, md->mp.mass,
                               md->kpart.as<double>(), st));
         else if (h->dtype == PD_F64)
@@ -611,7 +680,11 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         PD_LAUNCH_CHECK();
         h->ctrl_h->rebuild = rebuilt;
         PD_CUDA(cudaMemcpyAsync(&h->ctrl->rebuild, &h->ctrl_h->rebuild, sizeof(unsigned int), cudaMemcpyHostToDevice, st));
-        if (md->tiles_active) {
+        if (md->physics == 1) {
+            pd::launch(k_energy, 1, 256, 0, st, (const double*)md->rpart.as<double>(), md->nblk,
+                       (const double*)md->kpart.as<double>(), md->nblk, (const unsigned int*)&h->ctrl->rebuild,
+                       md->E.as<double>() + 4 * s);
+        } else if (md->tiles_active) {
             const int nb2 = 256;
             long chunk = (md->ntiles + nb2 - 1) / nb2;
             double* stage = md->tpart.as<double>() + 2 * md->ntiles;

@@ -62,6 +62,12 @@ class LJParams(ctypes.Structure):
 PREC_FP64, PREC_MIXED = 0, 1
 
 
+class SPHParams(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_double), ("mass", ctypes.c_double), ("c0", ctypes.c_double),
+                ("rho0", ctypes.c_double), ("alpha", ctypes.c_double), ("gz", ctypes.c_double),
+                ("rho_prop", ctypes.c_int), ("drho_prop", ctypes.c_int), ("type_prop", ctypes.c_int)]
+
+
 class MDParams(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("mass", ctypes.c_double), ("skin", ctypes.c_double),
                 ("vel_prop", ctypes.c_int), ("force_prop", ctypes.c_int), ("use_cell_list", ctypes.c_int),
@@ -124,6 +130,7 @@ def lib():
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
+            "pd_sph_create": ([vp, P(SPHParams), P(MDParams), P(vp)], ip),
             "pd_selftest_recip": ([ip, vp, vp, lp], ip),
             "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
@@ -435,3 +442,17 @@ class MD:
         if getattr(self, "h", None) and _lib is not None:
             _lib.pd_md_destroy(self.h)
             self.h = None
+
+
+class SPH(MD):
+    """WCSPH driver: props of `vd` are velocity (vel_prop), acceleration
+    (acc_prop), density, density rate and type (0 fluid, 1 wall)."""
+
+    def __init__(self, vd, vel_prop, acc_prop, rho_prop, drho_prop, type_prop, h, mass, c0=20.0, rho0=1000.0,
+                 alpha=0.1, gz=-9.81, dt=1e-4, skin=0.0):
+        self.vd = vd
+        self.sp = SPHParams(h, mass, c0, rho0, alpha, gz, rho_prop, drho_prop, type_prop)
+        self.mp = MDParams(dt, mass, skin, vel_prop, acc_prop, 0, PREC_FP64)
+        hh = ctypes.c_void_p()
+        check(lib().pd_sph_create(vd.h, ctypes.byref(self.sp), ctypes.byref(self.mp), ctypes.byref(hh)))
+        self.h = hh

@@ -687,6 +687,8 @@ static void sph_rates_impl(const T* pos, const T* vel, const T* rho, const int* 
                            const long* counts, const int* idx, T h, T m, T c0, T rho0, T alpha, T gz, T* acc,
                            T* drho) {
     SPHP<T> P = sph_params(h, m, c0, rho0, alpha, gz);
+    const T two_h = T(2) * h;
+    const T r2c = two_h * two_h;
 #pragma omp parallel for schedule(static)
     for (long a = 0; a < n; ++a) {
         const T* xa = pos + 3 * a;
@@ -700,7 +702,7 @@ static void sph_rates_impl(const T* pos, const T* vel, const T* rho, const int* 
             const T* xb = pos + 3 * b;
             T dx = xa[0] - xb[0], dy = xa[1] - xb[1], dz = xa[2] - xb[2];
             T r2 = std::fma(dz, dz, std::fma(dy, dy, dx * dx));
-            if (r2 >= T(4) * h * h || r2 == T(0)) continue;
+            if (r2 >= r2c || r2 == T(0)) continue;
             T r = std::sqrt(r2);
             T dwr = sph_dwdr_over_r(P, r);
             T vx = va[0] - vel[3 * b], vy = va[1] - vel[3 * b + 1], vz = va[2] - vel[3 * b + 2];
@@ -729,7 +731,71 @@ static void sph_rates_impl(const T* pos, const T* vel, const T* rho, const int* 
     }
 }
 
+// WCSPH time integration (kick-drift-kick, the same scheme as the GPU driver):
+//   v' = v + dt/2 a ; rho' = rho + dt/2 drho ; x += dt v' (fluid only) ;
+//   (a, drho) = rates(x, v', rho') over pairs with r < 2h (cell-list walk) ;
+//   v = v' + dt/2 a ; rho = rho' + dt/2 drho.
+// Wall particles (type 1) keep v = 0 and do not move; their density evolves.
+// E[s] = (kinetic energy of the fluid, sum of densities, 0, 0) after step s.
+template <class T>
+static int md_sph_impl(T* x, T* v, T* rho, const int* type, long n, const T* lo, const T* hi, T h, T m, T c0, T rho0,
+                       T alpha, T gz, T dt, int steps, double* E) {
+    const int bc[3] = {0, 0, 0};
+    const T g0[3] = {0, 0, 0};
+    T r = T(2) * h;
+    T blo[3], sp[3];
+    int dv[3], gs[3];
+    long nc;
+    cl_geometry_impl(lo, hi, g0, r, (T)1.013, 1, blo, sp, dv, gs, &nc);
+    std::vector<long> cnt(n), off(n + 1);
+    std::vector<int> idx;
+    std::vector<T> acc(3 * n), drho(n);
+    auto rates = [&]() {
+        verlet_impl(x, n, n, blo, sp, dv, 1, r, cnt.data(), (const long*)nullptr, (int*)nullptr);
+        off[0] = 0;
+        for (long i = 0; i < n; ++i) off[i + 1] = off[i] + cnt[i];
+        idx.assign(off[n], 0);
+        verlet_impl(x, n, n, blo, sp, dv, 1, r, (long*)nullptr, off.data(), idx.data());
+        sph_rates_impl(x, v, rho, type, n, off.data(), cnt.data(), idx.data(), h, m, c0, rho0, alpha, gz, acc.data(),
+                       drho.data());
+    };
+    (void)bc;
+    rates();
+    T half = T(0.5) * dt;
+    for (int s = 0; s < steps; ++s) {
+        for (long i = 0; i < n; ++i) {
+            if (type[i] == 0) {
+                for (int d = 0; d < 3; ++d) v[3 * i + d] += half * acc[3 * i + d];
+                for (int d = 0; d < 3; ++d) x[3 * i + d] += dt * v[3 * i + d];
+            }
+            rho[i] += half * drho[i];
+        }
+        rates();
+        double ke = 0, rs = 0;
+        for (long i = 0; i < n; ++i) {
+            if (type[i] == 0) {
+                for (int d = 0; d < 3; ++d) v[3 * i + d] += half * acc[3 * i + d];
+                ke += 0.5 * (double)m *
+                      ((double)v[3 * i] * v[3 * i] + (double)v[3 * i + 1] * v[3 * i + 1] +
+                       (double)v[3 * i + 2] * v[3 * i + 2]);
+            }
+            rho[i] += half * drho[i];
+            rs += rho[i];
+        }
+        E[4 * s] = ke;
+        E[4 * s + 1] = rs;
+        E[4 * s + 2] = 0;
+        E[4 * s + 3] = 0;
+    }
+    return 0;
+}
+
 extern "C" {
+
+int or_md_sph_d(double* x, double* v, double* rho, const int* type, long n, const double* lo, const double* hi,
+                double h, double m, double c0, double rho0, double alpha, double gz, double dt, int steps, double* E) {
+    return md_sph_impl(x, v, rho, type, n, lo, hi, h, m, c0, rho0, alpha, gz, dt, steps, E);
+}
 
 // -- periodic wrap
 void or_wrap_d(double* pos, long n, const double* lo, const double* hi, const int* bc) { wrap_impl(pos, n, lo, hi, bc); }

@@ -63,6 +63,8 @@ def lib():
         L.or_md_lj_d.argtypes = [_dp, _dp, _L, _dp, _dp, _ip, _dp, _D, _D, _D, _D, _D, _D, _I, _dp,
                                  ctypes.POINTER(ctypes.c_double)]
         L.or_md_lj_d.restype = _I
+        L.or_md_sph_d.argtypes = [_dp, _dp, _dp, _ip, _L, _dp, _dp, _D, _D, _D, _D, _D, _D, _D, _I, _dp]
+        L.or_md_sph_d.restype = _I
         L.or_num_threads.restype = _I
         L.or_set_threads.argtypes = [_I]
         _LIB = L
@@ -253,6 +255,18 @@ def sph_rates(pos, vel, rho, typ, off, idx, h, m, c0, rho0, alpha, gz):
     lib().or_sph_rates_d(_a(pos, np.float64), _a(vel, np.float64), _a(rho, np.float64), _a(typ, np.int32), n,
                          _a(off[:-1], np.int64), counts, _a(idx, np.int32), h, m, c0, rho0, alpha, gz, acc, drho)
     return acc, drho
+
+
+def md_sph(x, v, rho, typ, lo, hi, h, m, c0, rho0, alpha, gz, dt, steps):
+    """WCSPH kick-drift-kick with fixed walls; returns (x, v, rho, E[steps, 4] = KE, sum rho, 0, 0)."""
+    x = _a(x, np.float64).copy()
+    v = _a(v, np.float64).copy()
+    rho = _a(rho, np.float64).copy()
+    E = np.zeros((max(steps, 1), 4))
+    rc_ = lib().or_md_sph_d(x, v, rho, _a(typ, np.int32), x.shape[0], _a(lo, np.float64), _a(hi, np.float64), h, m,
+                            c0, rho0, alpha, gz, dt, steps, E)
+    assert rc_ == 0
+    return x, v, rho, E[:steps]
 
 
 def md_lj(x, v, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps, timing=False):
