@@ -274,6 +274,34 @@ int pd_md_verlet_get(pd_md md, int* counts, int* idx, long idx_cap, int* tiled);
 int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn);
 int pd_md_timers(pd_md md, double* ms, long* counts);
 
+/* ---- serving loop -------------------------------------------------------- */
+/* Many independent periodic LJ systems (precision form, FP32 forces / FP64
+ * energies) resident on one GPU and stepped together by persistent batched
+ * kernels captured as CUDA graphs.  No reference counterpart: the reference's
+ * many-systems idiom is an array of kernel views passed to one kernel
+ * (Vector/cuda/vector_dist_gpu_MP_tests.cu:427-781).  Requests are admitted in
+ * FIFO order as slots and HBM (budget and free memory) allow; each tick advances
+ * every admitted system by one velocity-Verlet step and retires finished ones. */
+typedef struct pd_srv_s* pd_srv;
+int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj, double dt, double skin,
+                  pd_srv* out);
+int pd_srv_destroy(pd_srv s);
+/* autotune != 0: tile width chosen per size bucket by timing; else the fixed tx */
+int pd_srv_set_tuning(pd_srv s, int autotune, int tx);
+/* queue a system: n particles in a periodic cube of side `box`, host AoS x, v */
+int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const double* v_host, int steps,
+                  long* ticket);
+int pd_srv_tick(pd_srv s, int* n_active, int* n_queued);
+/* 0 queued, 1 running, 2 done, 3 failed */
+int pd_srv_state(pd_srv s, long ticket, int* state);
+/* final positions (submission order), E[steps][4] = KE, PE, virial, rebuilt;
+ * times[3] = submit, admit, done (seconds since the server was created) */
+int pd_srv_result(pd_srv s, long ticket, double* x_out, double* E_out, double* times);
+int pd_srv_release(pd_srv s, long ticket);
+int pd_srv_stats(pd_srv s, long* particle_steps, long* systems_done, long* ticks, long* rebuilds, double* tune_ms);
+/* autotuner table: size bucket (floor(log2 N)) -> tile width */
+int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int cap, int* n);
+
 #ifdef __cplusplus
 }
 #endif

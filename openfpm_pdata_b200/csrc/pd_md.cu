@@ -15,6 +15,7 @@
 #include "pd_tile.cuh"
 #include "pd_mixed.cuh"
 #include "pd_sph.cuh"
+#include "pd_md.cuh"
 
 namespace pd {
 
@@ -223,41 +224,6 @@ __global__ void k_energy(const double* __restrict__ fpart, int nbf, const double
 
 }  // namespace pd
 
-struct pd_md_s {
-    pd_vd h = nullptr;
-    pd_lj_params_t lj;
-    pd_md_params_t mp;
-    pd_vl vl = nullptr;   // Verlet list (r_cut + skin)
-    pd_cl cl = nullptr;   // cell list of side r_cut (cell-list mode)
-    pd::Buf xb, fpart, kpart, E;
-    int nblk = 0;
-    bool ready = false;
-    // tiled neighbour structure (pd_tile.cu)
-    bool use_tiles = true;
-    int tile_tx = 0;  // cells per tile along x (0: from the mean occupancy)
-    int tile_p = 2;   // threads per domain particle in the pair kernel
-    bool tiles_active = false;
-    pd::TileGeom tg;
-    long ntiles = 0;
-    unsigned int tcap = 0;
-    long tstride = 0;
-    int tmax_nn = 0;
-    pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
-    // precision form: FP32 cell-local offsets (all particles), their value at the
-    // last build (real particles) and the constant parts of the image offsets
-    int physics = 0;  // 0: Lennard-Jones, 1: WCSPH
-    pd_sph_params_t sp;
-    pd::Buf aux, rpart;
-    bool mixed = false;
-    bool off_valid = false;  // `off` holds the authoritative state (after the first build)
-    pd::Buf off, offb, offK;
-    long builds = 0, steps = 0;
-    // optional per-phase device timing (CUDA events on the run's stream)
-    bool timing = false;
-    cudaEvent_t ev[8] = {};
-    double ms[4] = {0, 0, 0, 0};   // integrate, rebuild, images, force
-    long cnt[4] = {0, 0, 0, 0};
-};
 
 namespace pd {
 
@@ -318,7 +284,7 @@ static int lj_launch(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t& lj, int 
     return PD_OK;
 }
 
-static int force_blocks(long n) {
+int force_blocks(long n) {
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -367,7 +333,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
 }
 
 // wrap, sort the real particles into cell order, periodic images, neighbour structure
-static int md_rebuild(pd_md md, cudaStream_t st) {
+int md_rebuild(pd_md md, cudaStream_t st) {
     pd_vd h = md->h;
     if (md->mixed && md->off_valid) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));
     h->n_total = h->n_real;
@@ -411,7 +377,7 @@ static int md_rebuild(pd_md md, cudaStream_t st) {
     return PD_OK;
 }
 
-static int md_forces(pd_md md, cudaStream_t st) {
+int md_forces(pd_md md, cudaStream_t st) {
     if (md->physics == 1)
         return sph_rates(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->tcap, md->tnbr, md->tnn,
                          md->tstride, md->aux, md->sp, md->mp.force_prop, md->tile_p, st);

@@ -1,0 +1,49 @@
+// pd_md.cuh -- the integrator handle, shared by the single-system driver
+// (pd_md.cu) and the serving loop (pd_serve.cu).
+#pragma once
+#include "pd_internal.cuh"
+#include "pd_tile.cuh"
+
+struct pd_md_s {
+    pd_vd h = nullptr;
+    pd_lj_params_t lj;
+    pd_md_params_t mp;
+    pd_vl vl = nullptr;   // Verlet list (r_cut + skin)
+    pd_cl cl = nullptr;   // cell list of side r_cut (cell-list mode)
+    pd::Buf xb, fpart, kpart, E;
+    int nblk = 0;
+    bool ready = false;
+    // tiled neighbour structure (pd_tile.cu)
+    bool use_tiles = true;
+    int tile_tx = 0;  // cells per tile along x (0: from the mean occupancy)
+    int tile_p = 2;   // threads per domain particle in the pair kernel
+    bool tiles_active = false;
+    pd::TileGeom tg;
+    long ntiles = 0;
+    unsigned int tcap = 0;
+    long tstride = 0;
+    int tmax_nn = 0;
+    pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
+    // precision form: FP32 cell-local offsets (all particles), their value at the
+    // last build (real particles) and the constant parts of the image offsets
+    int physics = 0;  // 0: Lennard-Jones, 1: WCSPH
+    pd_sph_params_t sp;
+    pd::Buf aux, rpart;
+    bool mixed = false;
+    bool off_valid = false;  // `off` holds the authoritative state (after the first build)
+    pd::Buf off, offb, offK;
+    long builds = 0, steps = 0;
+    // optional per-phase device timing (CUDA events on the run's stream)
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    double ms[4] = {0, 0, 0, 0};   // integrate, rebuild, images, force
+    long cnt[4] = {0, 0, 0, 0};
+};
+
+namespace pd {
+int force_blocks(long n);
+// wrap, sort, periodic images, neighbour structure (and the mixed-form offsets)
+int md_rebuild(pd_md md, cudaStream_t st);
+// forces of the current state into the force property
+int md_forces(pd_md md, cudaStream_t st);
+}  // namespace pd

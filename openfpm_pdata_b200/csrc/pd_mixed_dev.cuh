@@ -1,0 +1,197 @@
+// pd_mixed_dev.cuh -- device code of the mixed-form LJ tile kernel, shared by the
+// single-system kernel (pd_mixed.cu) and the batched kernels (pd_serve.cu).
+#pragma once
+#include "pd_device.cuh"
+#include "pd_internal.cuh"
+#include "pd_lj.cuh"
+#include "pd_tile.cuh"
+
+namespace pd {
+
+struct TileShM {
+    unsigned int cR[9][TXMAX + 3];
+    unsigned int cI[9][TXMAX + 3];
+    unsigned int oR[9], oI[9];
+    unsigned int total;
+    int ncol;
+    unsigned int segb[18][TXMAX + 3];
+};
+
+// cell centres of the grid
+struct CellGeom {
+    double lo[3], sp[3];
+    int gs[3], pad;
+    __device__ __forceinline__ void centre(unsigned int c, double& cx, double& cy, double& cz) const {
+        int i0 = (int)(c % (unsigned)gs[0]);
+        int i1 = (int)((c / (unsigned)gs[0]) % (unsigned)gs[1]);
+        int i2 = (int)(c / ((unsigned)gs[0] * (unsigned)gs[1]));
+        cx = lo[0] + ((double)(i0 - pad) + 0.5) * sp[0];
+        cy = lo[1] + ((double)(i1 - pad) + 0.5) * sp[1];
+        cz = lo[2] + ((double)(i2 - pad) + 0.5) * sp[2];
+    }
+};
+
+struct Kahan {
+    float s, c;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// One tile of the mixed-form LJ kernel, shared by the single-system kernel and
+// the batched persistent kernel of the serving loop.  The mbarrier `bar` is
+// initialised by the caller; `uses` counts its completed phases (the parity of
+// the next wait).  Returns the thread's partial potential energy and virial.
+template <int P>
+__device__ __forceinline__ void mixed_tile(long tile, const float4* __restrict__ off, long n_real, const TileGeom& tg,
+                                           const unsigned int* __restrict__ csR,
+                                           const unsigned int* __restrict__ csI, unsigned int cap,
+                                           const unsigned int* __restrict__ nbr, const int* __restrict__ nn,
+                                           long stride, float sx, float sy, float sz, const LJP<float>& Pr,
+                                           float* __restrict__ f, long fcap, unsigned int* __restrict__ err,
+                                           float4* sm, TileShM& S, unsigned long long* bar, unsigned int& uses,
+                                           double& pe, double& vir) {
+    {
+        long t = tile;
+        int tx = (int)(t % tg.ntx);
+        long rest = t / tg.ntx;
+        int y = (int)(rest % tg.ny) + tg.pad;
+        int z = (int)(rest / tg.ny) + tg.pad;
+        int x0 = tg.pad + tx * tg.TX;
+        int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
+        int ncol = x1 - x0 + 3;
+        for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+            int img = e >= 9 * ncol;
+            int ee = img ? e - 9 * ncol : e;
+            int r = ee / ncol, j = ee % ncol;
+            int dz = r / 3 - 1, dy = r % 3 - 1;
+            long c = (long)(x0 - 1 + j) + (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
+            if (img) S.cI[r][j] = csI[c];
+            else S.cR[r][j] = csR[c];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int o = 0;
+            for (int r = 0; r < 9; ++r) {
+                S.oR[r] = o;
+                o += S.cR[r][ncol - 1] - S.cR[r][0];
+                S.oI[r] = o;
+                o += S.cI[r][ncol - 1] - S.cI[r][0];
+            }
+            S.total = o;
+            S.ncol = ncol;
+        }
+        __syncthreads();
+    }
+    const int ncol = S.ncol;
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][ncol - 2];
+    bool ok = ib != ie && S.total <= cap;
+    if (ib != ie && S.total > cap && threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+    if (ok) {
+        for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
+            int sg = e / ncol, j = e % ncol, r = sg >> 1;
+            S.segb[sg][j] = (sg & 1) ? S.oI[r] + (S.cI[r][j] - S.cI[r][0]) : S.oR[r] + (S.cR[r][j] - S.cR[r][0]);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(bar, S.total * (unsigned int)sizeof(float4));
+            const int nc = ncol - 1;
+            for (int r = 0; r < 9; ++r) {
+                unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+                if (lr) bulk_g2s(sm + S.oR[r], off + S.cR[r][0], lr * (unsigned int)sizeof(float4), bar);
+                unsigned int li = S.cI[r][nc] - S.cI[r][0];
+                if (li) bulk_g2s(sm + S.oI[r], off + n_real + S.cI[r][0], li * (unsigned int)sizeof(float4), bar);
+            }
+        }
+        bool waited = mbar_wait_bounded(bar, uses & 1u, 1u << 24);
+        if (!waited) {
+            atomicOr(err, ERR_TIMEOUT);
+            mbar_wait_bounded(bar, uses & 1u, 1u << 24);
+        }
+        ++uses;
+        ok = __syncthreads_and(waited ? 1 : 0) != 0;
+    }
+    if (ok) {
+        // rewrite the staged records: y/z relative to the centre row, w = cell column
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int sg = warp; sg < 18; sg += FBLOCK_T / 32) {
+            const int r = sg >> 1;
+            const float shy = (float)(r % 3 - 1) * sy, shz = (float)(r / 3 - 1) * sz;
+            for (unsigned int k = S.segb[sg][0] + lane; k < S.segb[sg][ncol - 1]; k += 32) {
+                int j = 0;
+                while (j < ncol - 2 && S.segb[sg][j + 1] <= k) ++j;
+                float4 q = sm[k];
+                q.y += shy;
+                q.z += shz;
+                q.w = (float)j;
+                sm[k] = q;
+            }
+        }
+        __syncthreads();
+        const unsigned int base = S.oR[4] - S.cR[4][0];
+        const int sub = threadIdx.x % P;
+        const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
+        for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
+            const unsigned int i = ib + t / P;
+            const bool active = i < ie;
+            const unsigned int li = base + i;
+            const float4 xi = sm[active ? li : 0];
+            const int words = active ? (nn[i] + 1) >> 1 : 0;
+            Kahan kx = {0.f, 0.f}, ky = {0.f, 0.f}, kz = {0.f, 0.f}, ke = {0.f, 0.f}, kw = {0.f, 0.f};
+            const unsigned int* row = nbr + i;
+            unsigned int nxt = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+#pragma unroll 2
+            for (int k = sub; k < words; k += P) {
+                const unsigned int pair = nxt;
+                if (k + P < words) nxt = __ldg(row + (long)(k + P) * stride);
+                float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
+                    const float4 xq = sm[l];
+                    const float dx = fmaf(xi.w - xq.w, sx, xi.x - xq.x);
+                    const float dy = xi.y - xq.y, dz = xi.z - xq.z;
+                    const float r2 = dist2(dx, dy, dz);
+                    if (r2 < Pr.rc2 && l != li) {
+                        float ir2 = recip(r2);
+                        float s2 = Pr.sig2 * ir2;
+                        float s6 = s2 * s2 * s2;
+                        float ff = Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f);
+                        fx += ff * dx;
+                        fy += ff * dy;
+                        fz += ff * dz;
+                        e += Pr.eps4 * s6 * (s6 - 1.f);
+                        w += ff * r2;
+                    }
+                }
+                kx.add(fx);
+                ky.add(fy);
+                kz.add(fz);
+                ke.add(e);
+                kw.add(w);
+            }
+            double Fx = kx.value(), Fy = ky.value(), Fz = kz.value(), Ee = ke.value(), Ww = kw.value();
+#pragma unroll
+            for (int o = 1; o < P; o <<= 1) {
+                Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+                Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+                Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+                Ee += __shfl_xor_sync(0xffffffffu, Ee, o);
+                Ww += __shfl_xor_sync(0xffffffffu, Ww, o);
+            }
+            if (active && sub == 0) {
+                f[i] = (float)Fx;
+                f[fcap + i] = (float)Fy;
+                f[2 * fcap + i] = (float)Fz;
+                pe += 0.5 * Ee;
+                vir += 0.5 * Ww;
+            }
+        }
+    }
+}
+
+}  // namespace pd

@@ -131,6 +131,17 @@ def lib():
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
             "pd_sph_create": ([vp, P(SPHParams), P(MDParams), P(vp)], ip),
+            "pd_srv_create": ([lp, ip, P(LJParams), ctypes.c_double, ctypes.c_double, P(vp)], ip),
+            "pd_srv_destroy": ([vp], ip),
+            "pd_srv_set_tuning": ([vp, ip, ip], ip),
+            "pd_srv_submit": ([vp, lp, ctypes.c_double, vp, vp, ip, P(ctypes.c_long)], ip),
+            "pd_srv_tick": ([vp, P(ctypes.c_int), P(ctypes.c_int)], ip),
+            "pd_srv_state": ([vp, lp, P(ctypes.c_int)], ip),
+            "pd_srv_result": ([vp, lp, vp, vp, vp], ip),
+            "pd_srv_release": ([vp, lp], ip),
+            "pd_srv_stats": ([vp, P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long),
+                              P(ctypes.c_double)], ip),
+            "pd_srv_tuned": ([vp, vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_selftest_recip": ([ip, vp, vp, lp], ip),
             "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
@@ -456,3 +467,76 @@ class SPH(MD):
         hh = ctypes.c_void_p()
         check(lib().pd_sph_create(vd.h, ctypes.byref(self.sp), ctypes.byref(self.mp), ctypes.byref(hh)))
         self.h = hh
+
+
+class Server:
+    """Serving loop: independent periodic LJ systems batched on one GPU."""
+
+    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, hbm_budget_bytes, max_slots=64, dt=0.005, skin=0.3, eps=1.0, sigma=1.0, r_cut=2.5,
+                 autotune=True, tx=0):
+        self.lj = LJParams(eps, sigma, r_cut)
+        h = ctypes.c_void_p()
+        check(lib().pd_srv_create(int(hbm_budget_bytes), int(max_slots), ctypes.byref(self.lj), float(dt),
+                                  float(skin), ctypes.byref(h)))
+        self.h = h
+        self.info = {}
+        check(lib().pd_srv_set_tuning(self.h, int(bool(autotune)), int(tx)))
+
+    def submit(self, x, v, box, steps):
+        x = np.ascontiguousarray(x, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        t = ctypes.c_long(0)
+        check(lib().pd_srv_submit(self.h, x.shape[0], float(box), _ptr(x), _ptr(v), int(steps), ctypes.byref(t)))
+        self.info[t.value] = (x.shape[0], int(steps))
+        return t.value
+
+    def tick(self):
+        a, q = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().pd_srv_tick(self.h, ctypes.byref(a), ctypes.byref(q)))
+        return a.value, q.value
+
+    def state(self, ticket):
+        st = ctypes.c_int(0)
+        check(lib().pd_srv_state(self.h, int(ticket), ctypes.byref(st)))
+        return st.value
+
+    def result(self, ticket):
+        """(x_final[N,3] in submission order, E[steps,4], (t_submit, t_admit, t_done))."""
+        n, steps = self.info[ticket]
+        x = np.zeros((n, 3))
+        E = np.zeros((steps, 4))
+        t = np.zeros(3)
+        check(lib().pd_srv_result(self.h, int(ticket), _ptr(x), _ptr(E), _ptr(t)))
+        return x, E, tuple(t)
+
+    def release(self, ticket):
+        check(lib().pd_srv_release(self.h, int(ticket)))
+        self.info.pop(ticket, None)
+
+    def stats(self):
+        ps, sd, tk, rb, tm = ctypes.c_long(0), ctypes.c_long(0), ctypes.c_long(0), ctypes.c_long(0), ctypes.c_double(0)
+        check(lib().pd_srv_stats(self.h, ctypes.byref(ps), ctypes.byref(sd), ctypes.byref(tk), ctypes.byref(rb),
+                                 ctypes.byref(tm)))
+        return {"particle_steps": ps.value, "systems_done": sd.value, "ticks": tk.value, "rebuilds": rb.value,
+                "tune_ms": tm.value}
+
+    def tuned(self):
+        b = np.zeros(64, np.int32)
+        w = np.zeros(64, np.int32)
+        n = ctypes.c_int(0)
+        check(lib().pd_srv_tuned(self.h, _ptr(b), _ptr(w), 64, ctypes.byref(n)))
+        return dict(zip(b[:n.value].tolist(), w[:n.value].tolist()))
+
+    def run_until_done(self, tickets, max_ticks=100000):
+        for _ in range(max_ticks):
+            if all(self.state(t) in (self.DONE, self.FAILED) for t in tickets):
+                return
+            self.tick()
+        raise RuntimeError("serving loop did not finish")
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pd_srv_destroy(self.h)
+            self.h = None

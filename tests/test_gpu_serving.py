@@ -1,0 +1,99 @@
+"""Serving loop: continuous batching of independent LJ systems.
+
+* a system's result is the same alone and in a mix (fixed tile width: bit-exact;
+  autotuned widths: energies within 1e-10 relative, positions within 1e-6);
+* the batched path agrees with the single-system mixed-precision driver and,
+  within the precision form's bounds, with the FP64 oracle;
+* admission respects the HBM budget (requests wait in FIFO order).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pd():
+    from openfpm_pdata_b200 import pd as _pd
+    _pd.lib()
+    return _pd
+
+
+def _sys(n, seed):
+    from openfpm_pdata_b200 import workloads
+    return workloads.serving_system(n, density=0.8, seed=seed)
+
+
+def _serve(pd, systems, steps=20, autotune=False, tx=5, budget=8 << 30, slots=16):
+    srv = pd.Server(budget, max_slots=slots, dt=0.005, skin=0.3, autotune=autotune, tx=tx)
+    tickets = [srv.submit(x, v, L, steps) for (x, v, L) in systems]
+    srv.run_until_done(tickets)
+    out = [srv.result(t) for t in tickets]
+    assert all(srv.state(t) == srv.DONE for t in tickets)
+    _serve.last = srv
+    return out, srv
+
+
+def test_alone_equals_in_mix_bit_exact(pd):
+    a = _sys(3000, 1)
+    others = [_sys(n, 10 + k) for k, n in enumerate([700, 9000, 1500, 20000, 600])]
+    (xa, Ea, _), = _serve(pd, [a])[0]
+    mix, _ = _serve(pd, others[:2] + [a] + others[2:])
+    xm, Em, _ = mix[2]
+    assert np.array_equal(Ea, Em)
+    assert np.array_equal(xa, xm)
+
+
+def test_alone_vs_mix_autotuned(pd):
+    a = _sys(4000, 2)
+    others = [_sys(n, 20 + k) for k, n in enumerate([3500, 12000, 800])]
+    (xa, Ea, _), = _serve(pd, [a], autotune=True)[0][:1]
+    s1 = _serve.last
+    mix, srv = _serve(pd, others + [a], autotune=True)
+    xm, Em, _ = mix[-1]
+    bucket = int(np.floor(np.log2(4000)))
+    if s1.tuned()[bucket] == srv.tuned()[bucket]:
+        assert np.array_equal(Ea, Em) and np.array_equal(xa, xm)
+    else:
+        # another tile width changes the FP32 summation order only
+        np.testing.assert_allclose(Em[:, :3], Ea[:, :3], rtol=1e-6)
+        d = xm - xa
+        L = a[2]
+        assert np.max(np.abs(d - np.round(d / L) * L)) < 1e-4
+    assert len(srv.tuned()) >= 2
+
+
+def test_served_matches_single_driver_and_oracle(pd, orc):
+    x, v, L = _sys(6000, 3)
+    (xs, Es, _), = _serve(pd, [(x, v, L)], steps=25, tx=5)[0]
+    vd = pd.VectorDist(x.shape[0], np.zeros(3), np.full(3, L), np.ones(3, np.int32), 2.8, dtype=np.float64,
+                       props=[(pd.PD_F32, 3), (pd.PD_F32, 3)])
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3, precision=pd.PREC_MIXED)
+    md.set_tiles(True, tx=5, threads_per_particle=2)
+    E1 = md.run(25)
+    # same tile width and lanes: the same trajectory; sums of the energies differ in order only
+    np.testing.assert_allclose(Es[:, :3], E1[:, :3], rtol=1e-12, atol=1e-12)
+    assert np.array_equal(Es[:, 3], E1[:, 3])
+    x1 = np.zeros_like(x)
+    x1[vd.gid(with_ghost=False)] = vd.deviceToHostPos(with_ghost=False)
+    assert np.array_equal(x1, xs)
+    _, _, Eo = orc.md_lj(x, v, np.zeros(3), np.full(3, L), np.ones(3, np.int32), 2.8, 2.5, 0.3, 1.0, 1.0, 0.005,
+                         1.0, 25)
+    tot = Es[:, 0] + Es[:, 1]
+    toto = Eo[1:, 0] + Eo[1:, 1]
+    assert np.max(np.abs(tot - toto) / np.abs(toto)) < 2e-5
+
+
+def test_admission_by_budget(pd):
+    systems = [_sys(n, 30 + k) for k, n in enumerate([20000, 20000, 20000])]
+    # a budget for about one system at a time: the others wait, all finish
+    srv = pd.Server(int(20000 * 700 * 1.5) + (8 << 20), max_slots=8, dt=0.005, skin=0.3, autotune=False, tx=5)
+    tickets = [srv.submit(x, v, L, 10) for (x, v, L) in systems]
+    active, queued = srv.tick()
+    assert active == 1 and queued == 2
+    srv.run_until_done(tickets)
+    times = [srv.result(t)[2] for t in tickets]
+    assert times[0][2] <= times[1][1] and times[1][2] <= times[2][1]   # FIFO, one at a time
+    assert srv.stats()["systems_done"] == 3
