@@ -33,6 +33,14 @@ WORKLOAD = "LJ MD 3D FP64, N=4,096,000 (160^3 lattice, spacing 1.1, jitter 0.05)
            "Verlet skin 0.3 (rebuild at max displacement > skin/2), velocity Verlet dt 0.005"
 
 
+def workload_name(nside, mixed):
+    w = WORKLOAD if not mixed else WORKLOAD.replace("FP64", "mixed-precision")
+    if nside != N_SIDE:
+        w = w.replace("N=4,096,000 (160^3", f"N={nside ** 3:,} ({nside}^3").replace(
+            "box 176", f"box {nside * SPACING:g}") + " [profiling case]"
+    return w
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -41,9 +49,9 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic():
-    """dram bytes per force launch from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "k_lj_verlet_lj4M.md")
+def read_traffic(kernel_file):
+    """dram bytes per force launch (scaled to the full workload) from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", kernel_file)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -107,9 +115,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def make_workload():
+def make_workload(nside=N_SIDE):
     from openfpm_pdata_b200 import workloads
-    x, v, L = workloads.lj_lattice(N_SIDE, SPACING, JITTER, seed=SEED)
+    x, v, L = workloads.lj_lattice(nside, SPACING, JITTER, seed=SEED)
     return x, v, L
 
 
@@ -160,6 +168,8 @@ def main():
     ap.add_argument("--tiles", type=int, default=1, help="1: tiled shared-memory rows, 0: global-index rows")
     ap.add_argument("--tx", type=int, default=0, help="cells per tile along x (0: automatic)")
     ap.add_argument("--tpp", type=int, default=0, help="threads per particle in the pair kernel (0: 2)")
+    ap.add_argument("--nside", type=int, default=N_SIDE,
+                    help="lattice side (default 160: 4,096,000 particles; smaller sides are profiling cases)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="fp64: plain FP64 path; mixed: FP32 cell-local positions, Kahan sums, FP64 wrap/energies")
     a = ap.parse_args()
@@ -197,7 +207,7 @@ def main():
 
     from openfpm_pdata_b200 import pd
     pd.lib()
-    x, v, L = make_workload()
+    x, v, L = make_workload(a.nside)
     n = x.shape[0]
     vd, md = build_system(pd, x, v, L)
 
@@ -244,13 +254,14 @@ def main():
         alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
-    traffic = read_traffic()
+    kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_f64" if a.tiles else "k_lj_verlet_f64")
+    traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
 
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+kahan/f64-energy" if mixed else "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD if not mixed else WORKLOAD.replace("FP64", "mixed-precision"),
+        "config": {"workload": workload_name(a.nside, mixed),
                    "particles": n, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (positions 131 MB + Verlet list ~1.1 GB per replica)",
                    "list_rebuilds_in_timed_region": builds, "mean_verlet_row": round(mean_nn, 2),
