@@ -150,6 +150,198 @@ def cpu_reference(x, v, L, steps, budget_s=30.0):
     return x.shape[0] * k / t, threads, k, rebuilds, t
 
 
+def _timed(md, steps, torch):
+    """Run `steps` steps between two CUDA events on torch's current stream (the library's
+    launches go to the legacy default stream, which synchronises with it); returns (ms, E)."""
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    E = md.run(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), E
+
+
+def form_precision(pd, torch, x, v, L, steps, warmup, fp64_value):
+    """Precision form on the 4,096,000-particle lattice: throughput, ratio to the FP64
+    path and the force error against the FP64 GPU path on the final positions."""
+    TUNE["precision"] = "mixed"
+    vd, md = build_system(pd, x, v, L)
+    md.run(warmup, energies=False)
+    md.set_timing(True)
+    ms, E = _timed(md, steps, torch)
+    t = md.timers()
+    n = x.shape[0]
+    val = n * steps / (ms / 1e3)
+    # forces of the FP64 path on the same (final) positions
+    xf = vd.deviceToHostPos(with_ghost=False)
+    f32 = vd.deviceToHostProp(1, with_ghost=False).astype(np.float64)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd64 = pd.VectorDist(n, lo, hi, bc, R_CUT, dtype=np.float64, props=[(pd.PD_F64, 3)])
+    vd64.hostToDevicePos(xf)
+    vd64.map()
+    vd64.ghost_get()
+    cl = vd64.getCellListGPU(R_CUT)
+    vd64.updateCellListGPU(cl)
+    vd64.lj_forces(0, cl=cl, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+    f64 = vd64.deviceToHostProp(0, with_ghost=False)  # same order as xf (map on one domain keeps it)
+    frms = np.sqrt((f64 ** 2).sum(axis=1).mean())
+    err = np.sqrt(((f32 - f64) ** 2).sum(axis=1)) / frms
+    TUNE["precision"] = "fp64"
+    return {"workload": workload_name(N_SIDE, True), "value": val, "unit": METRIC, "steps": steps,
+            "ms_per_step": ms / steps, "vs_fp64_path": val / fp64_value,
+            "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in t.items()},
+            "list_rebuilds": int(E[:, 3].sum()),
+            "force_error_vs_fp64": {"mean": float(err.mean()), "max": float(err.max()),
+                                    "norm": "|F32 - F64| / F_rms(F64), per particle, final positions"}}
+
+
+def form_cell_list_every_step(pd, torch, steps=100, warmup=5):
+    """N = 4096 (16^3 lattice, spacing 1, box 16), cell list rebuilt every step, FP64."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(16, 1.0, 0.05, seed=1)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(x.shape[0], lo, hi, bc, R_CUT, dtype=np.float64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=DT, mass=MASS, skin=0.0, eps=EPS, sigma=SIGMA, r_cut=R_CUT, use_cell_list=True)
+    md.run(warmup, energies=False)
+    l0 = pd.launch_count()
+    ms, E = _timed(md, steps, torch)
+    return {"workload": "LJ MD FP64, N=4096 (16^3 lattice, spacing 1, jitter 0.05), box 16, r_cut 2.5, "
+                        "cell list rebuilt every step, dt 0.005",
+            "value": x.shape[0] * steps / (ms / 1e3), "unit": METRIC, "steps": steps, "ms_per_step": ms / steps,
+            "gpu_launches_per_step": (pd.launch_count() - l0) / steps}
+
+
+def form_sph(pd, torch, steps=200, warmup=5, dp=1.0 / 180):
+    """WCSPH dam break, FP64 and FP32 storage."""
+    from openfpm_pdata_b200 import workloads
+    x, typ, m, lo, hi = workloads.sph_dam(dp)
+    h = 1.3 * dp
+    out = {"workload": f"WCSPH dam break, fluid block [0,0.4]x[0,1]x[0,0.6] + 3 wall layers, dp=1/{round(1 / dp)}, "
+                       f"N={x.shape[0]:,}, h=1.3dp, c0=20, rho0=1000, alpha=0.1, dt=1e-4, Verlet skin 0.3dp",
+           "particles": int(x.shape[0])}
+    for name, dt_ in (("fp64", np.float64), ("fp32", np.float32)):
+        ft = pd.PD_F64 if dt_ == np.float64 else pd.PD_F32
+        vd = pd.VectorDist(x.shape[0], lo, hi, np.zeros(3, np.int32), 0.0, dtype=dt_,
+                           props=[(ft, 3), (ft, 3), (ft, 1), (ft, 1), (pd.PD_I32, 1)])
+        vd.hostToDevicePos(x.astype(dt_))
+        vd.hostToDeviceProp(0, np.zeros((x.shape[0], 3)))
+        vd.hostToDeviceProp(2, np.full(x.shape[0], 1000.0))
+        vd.hostToDeviceProp(4, typ)
+        sph = pd.SPH(vd, 0, 1, 2, 3, 4, h, m, 20.0, 1000.0, 0.1, -9.81, 1e-4, skin=0.3 * dp)
+        sph.run(warmup, energies=False)
+        sph.set_timing(True)
+        ms, E = _timed(sph, steps, torch)
+        t = sph.timers()
+        out[name] = {"value": x.shape[0] * steps / (ms / 1e3), "unit": METRIC, "steps": steps,
+                     "ms_per_step": ms / steps, "list_rebuilds": int(E[:, 3].sum()),
+                     "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in t.items()}}
+        del sph, vd
+    return out
+
+
+def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
+    """Serving form: a bounded sample of the stream of independent LJ systems
+    (N log-uniform in [512, 262144], density 0.8, 50 steps each).
+    (1) capacity: the first half of the sample submitted at once;
+    (2) Poisson arrivals of the second half at 0.8 x that capacity: p50/p99 latency
+        (arrival -> result) and aggregate throughput;
+    (3) plain: a subset run one after another through the single-system driver."""
+    from openfpm_pdata_b200 import workloads
+    sizes = workloads.serving_sizes(n_systems, seed=seed)
+    systems = [workloads.serving_system(int(n), 0.8, seed=1000 + k) for k, n in enumerate(sizes)]
+    free, _ = torch.cuda.mem_get_info()
+    srv = pd.Server(int(0.6 * free), max_slots=slots, dt=DT, skin=SKIN, autotune=True)
+    # tune every size bucket on throw-away systems first (untimed)
+    for b in range(9, 19):
+        n = int(min(2 ** b * 1.4, 262144))
+        x, v, L = workloads.serving_system(n, 0.8, seed=77 + b)
+        t = srv.submit(x, v, L, 2)
+        srv.run_until_done([t])
+        srv.release(t)
+    half = n_systems // 2
+    # (1) capacity
+    st0 = srv.stats()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tickets = [srv.submit(x, v, L, steps) for (x, v, L) in systems[:half]]
+    srv.run_until_done(tickets)
+    t_cap = time.perf_counter() - t0
+    st1 = srv.stats()
+    tm_cap = srv.timers()
+    for t in tickets:
+        srv.release(t)
+    cap_ps = (st1["particle_steps"] - st0["particle_steps"]) / t_cap
+    cap_sys = half / t_cap
+    # (2) Poisson arrivals at 0.8 x capacity
+    rng = np.random.default_rng(seed + 1)
+    lam = 0.8 * cap_sys
+    arr = np.cumsum(rng.exponential(1.0 / lam, size=n_systems - half))
+    pend = list(range(n_systems - half))
+    live = {}
+    lat = []
+    t0 = time.perf_counter()
+    st0 = srv.stats()
+    while pend or live:
+        now = time.perf_counter() - t0
+        while pend and arr[pend[0]] <= now:
+            k = pend.pop(0)
+            x, v, L = systems[half + k]
+            live[srv.submit(x, v, L, steps)] = arr[k]
+        if not live:
+            time.sleep(max(0.0, min(arr[pend[0]] - now, 0.01)))
+            continue
+        srv.tick()
+        now = time.perf_counter() - t0
+        for t in [t for t in live if srv.state(t) >= srv.DONE]:
+            lat.append(now - live.pop(t))
+            srv.release(t)
+    t_run = time.perf_counter() - t0
+    st1 = srv.stats()
+    srv_ps = (st1["particle_steps"] - st0["particle_steps"]) / t_run
+    lat = np.array(lat)
+    tuned = srv.tuned()
+    tm_all = srv.timers()
+    del srv
+    # (3) plain: the single-system mixed-precision driver, one system after another
+    plain_lat, plain_ps = [], 0
+    sub = systems[half: half + 40]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for (x, v, L) in sub:
+        t1 = time.perf_counter()
+        lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+        vd = pd.VectorDist(x.shape[0], lo, hi, bc, R_CUT + SKIN, dtype=np.float64,
+                           props=[(pd.PD_F32, 3), (pd.PD_F32, 3)])
+        vd.hostToDevicePos(x)
+        vd.hostToDeviceProp(0, v)
+        md = pd.MD(vd, 0, 1, dt=DT, skin=SKIN, precision=pd.PREC_MIXED)
+        md.run(steps)
+        vd.deviceToHostPos(with_ghost=False)
+        plain_lat.append(time.perf_counter() - t1)
+        plain_ps += x.shape[0] * steps
+        del md, vd
+    t_plain = time.perf_counter() - t0
+    return {"workload": f"{n_systems} systems of the serving stream (N log-uniform in [512, 262144], density 0.8, "
+                        f"r_cut 2.5, skin 0.3, {steps} velocity-Verlet steps, FP32 forces + Kahan, FP64 energies); "
+                        f"first {half} submitted at once (capacity), last {n_systems - half} Poisson at 0.8 x capacity",
+            "max_slots": slots, "mean_particles": float(sizes.mean()),
+            "capacity": {"value": cap_ps, "unit": METRIC, "systems_per_s": cap_sys},
+            "poisson_0.8": {"value": srv_ps, "unit": METRIC, "vs_capacity": srv_ps / cap_ps,
+                            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50))},
+            "plain_sequential": {"value": plain_ps / t_plain, "unit": METRIC, "systems": len(sub),
+                                 "p50_ms": float(np.percentile(plain_lat, 50) * 1e3),
+                                 "p99_ms": float(np.percentile(plain_lat, 99) * 1e3)},
+            "tuned_tile_width_by_log2_size": {str(k): v for k, v in tuned.items()},
+            "host_ms": {"capacity_phase": tm_cap, "total": tm_all, "ticks": st1["ticks"],
+                        "rebuilds": st1["rebuilds"]}}
+
+
 def dist_setup(n_gpus):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -172,6 +364,10 @@ def main():
                     help="lattice side (default 160: 4,096,000 particles; smaller sides are profiling cases)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="fp64: plain FP64 path; mixed: FP32 cell-local positions, Kahan sums, FP64 wrap/energies")
+    ap.add_argument("--forms", default="all",
+                    help="other workloads reported beside the main line: all, none, or a comma list of "
+                         "precision,c1,sph,serving")
+    ap.add_argument("--serve-systems", type=int, default=400, help="systems in the serving sample")
     a = ap.parse_args()
     TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp, precision=a.precision)
     mixed = a.precision == "mixed"
@@ -297,6 +493,19 @@ def main():
                       "includes": "create, H2D of positions+velocities, first list build, K steps, "
                                   "per-step energies and final state D2H"}
         assert np.isfinite(E2).all()
+
+    if rank == 0 and world == 1 and a.forms != "none":
+        want = a.forms.split(",") if a.forms != "all" else ["precision", "c1", "sph", "serving"]
+        forms = {}
+        if "precision" in want and not mixed:
+            forms["precision"] = form_precision(pd, torch, x, v, L, a.steps, a.warmup, value)
+        if "c1" in want:
+            forms["cell_list_every_step"] = form_cell_list_every_step(pd, torch)
+        if "sph" in want:
+            forms["sph"] = form_sph(pd, torch)
+        if "serving" in want:
+            forms["serving"] = form_serving(pd, torch, n_systems=a.serve_systems)
+        out["forms"] = forms
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         val, threads, k, rebuilds, t = cpu_reference(x, v, L, 20, budget_s=20.0)

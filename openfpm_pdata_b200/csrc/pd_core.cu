@@ -28,13 +28,30 @@ void set_error(const char* fmt, ...) {
     g_err = buf;
 }
 
+thread_local AllocCtx* g_alloc_ctx = nullptr;
+
+// Device allocations of the library.  Inside an AllocScope (the serving loop) they
+// come from the scope's memory pool, ordered on the scope's stream (freed memory
+// is reused without a device-wide synchronisation); elsewhere plain cudaMalloc /
+// cudaFree, which synchronise.
+cudaError_t dev_alloc(void** p, size_t b) {
+    if (g_alloc_ctx) return cudaMallocFromPoolAsync(p, b, g_alloc_ctx->pool, g_alloc_ctx->st);
+    return cudaMalloc(p, b);
+}
+
+void dev_free(void* p) {
+    if (!p) return;
+    if (g_alloc_ctx) cudaFreeAsync(p, g_alloc_ctx->st);
+    else cudaFree(p);
+}
+
 int Buf::ensure(size_t b) {
     if (b <= bytes && p) return PD_OK;
-    if (p) cudaFree(p);
+    dev_free(p);
     p = nullptr;
     bytes = 0;
     if (b == 0) return PD_OK;
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e = dev_alloc(&p, b);
     if (e != cudaSuccess) {
         p = nullptr;
         set_error("cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
@@ -46,7 +63,7 @@ int Buf::ensure(size_t b) {
 }
 
 void Buf::release() {
-    if (p) cudaFree(p);
+    dev_free(p);
     p = nullptr;
     bytes = 0;
 }
@@ -202,10 +219,10 @@ int ensure_capacity(pd_vd h, long need, cudaStream_t st) {
     if (need <= h->cap) return PD_OK;
     long ncap = need + need / 4 + 1024;
     void* np = nullptr;
-    PD_CUDA(cudaMalloc(&np, (size_t)ncap * h->pos_bytes));
+    PD_CUDA(dev_alloc(&np, (size_t)ncap * h->pos_bytes));
     int* ng = nullptr;
-    if (cudaMalloc(&ng, sizeof(int) * ncap) != cudaSuccess) {
-        cudaFree(np);
+    if (dev_alloc((void**)&ng, sizeof(int) * ncap) != cudaSuccess) {
+        dev_free(np);
         cudaGetLastError();
         set_error("cudaMalloc failed growing to %ld particles", ncap);
         return PD_ENOMEM;
@@ -217,11 +234,11 @@ int ensure_capacity(pd_vd h, long need, cudaStream_t st) {
     std::vector<char*> nprops(h->props.size(), nullptr);
     for (size_t p = 0; p < h->props.size(); ++p) {
         Prop& P = h->props[p];
-        if (cudaMalloc(&nprops[p], (size_t)P.esize * P.ncomp * ncap) != cudaSuccess) {
+        if (dev_alloc((void**)&nprops[p], (size_t)P.esize * P.ncomp * ncap) != cudaSuccess) {
             cudaGetLastError();
-            for (size_t q = 0; q < p; ++q) cudaFree(nprops[q]);
-            cudaFree(np);
-            cudaFree(ng);
+            for (size_t q = 0; q < p; ++q) dev_free(nprops[q]);
+            dev_free(np);
+            dev_free(ng);
             set_error("cudaMalloc failed growing property %zu to %ld particles", p, ncap);
             return PD_ENOMEM;
         }
@@ -231,10 +248,10 @@ int ensure_capacity(pd_vd h, long need, cudaStream_t st) {
                                         (size_t)h->n_total * P.esize, cudaMemcpyDeviceToDevice, st));
     }
     PD_CUDA(cudaStreamSynchronize(st));
-    cudaFree(h->pos);
-    cudaFree(h->gid);
+    dev_free(h->pos);
+    dev_free(h->gid);
     for (size_t p = 0; p < h->props.size(); ++p) {
-        cudaFree(h->props[p].d);
+        dev_free(h->props[p].d);
         h->props[p].d = nprops[p];
     }
     h->pos = np;
@@ -375,9 +392,9 @@ int pd_create(int dim, int dtype, long n, const double* lo, const double* hi, co
 
 int pd_destroy(pd_vd h) {
     if (!h) return PD_EINVAL;
-    cudaFree(h->pos);
-    cudaFree(h->gid);
-    for (auto& P : h->props) cudaFree(P.d);
+    dev_free(h->pos);
+    dev_free(h->gid);
+    for (auto& P : h->props) dev_free(P.d);
     h->img_src.release();
     h->img_shift.release();
     h->img_cnt.release();
@@ -404,7 +421,7 @@ int pd_add_prop(pd_vd h, int type, int ncomp, int* prop_id) {
     P.type = type;
     P.ncomp = ncomp;
     P.esize = type_size(type);
-    PD_CUDA(cudaMalloc(&P.d, (size_t)P.esize * ncomp * h->cap));
+    PD_CUDA(dev_alloc((void**)&P.d, (size_t)P.esize * ncomp * h->cap));
     PD_CUDA(cudaMemset(P.d, 0, (size_t)P.esize * ncomp * h->cap));
     h->props.push_back(P);
     if (prop_id) *prop_id = (int)h->props.size() - 1;

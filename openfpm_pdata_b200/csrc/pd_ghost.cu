@@ -10,17 +10,9 @@
 // round trip, and image records are kept for the replay.
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
+#include "pd_ghost_dev.cuh"
 
 namespace pd {
-
-static constexpr int MAXBOX = 64;
-
-template <class T> struct BoxSet {
-    T lo[MAXBOX][3];
-    T hi[MAXBOX][3];
-    int sv[MAXBOX];
-    int nb;
-};
 
 struct PropCopy {
     char* d[16];
@@ -45,11 +37,6 @@ __device__ __forceinline__ void copy_props(const PropCopy& pc, long from, long t
             }
         }
     }
-}
-
-template <class T> __device__ __forceinline__ bool inside_np(const BoxSet<T>& B, int i, T x, T y, T z) {
-    return !(x < B.lo[i][0] || x >= B.hi[i][0] || y < B.lo[i][1] || y >= B.hi[i][1] || z < B.lo[i][2] ||
-             z >= B.hi[i][2]);
 }
 
 // num_shift_ghost_each_part

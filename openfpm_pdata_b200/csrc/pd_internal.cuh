@@ -56,6 +56,22 @@ struct Ctrl {
     unsigned int tile_center_max;  // largest number of domain particles of a tile
 };
 
+// Allocation context: inside an AllocScope, device allocations of the library are
+// stream-ordered on `st` from `pool` (see dev_alloc in pd_core.cu).
+struct AllocCtx {
+    cudaStream_t st;
+    cudaMemPool_t pool;
+};
+extern thread_local AllocCtx* g_alloc_ctx;
+struct AllocScope {
+    AllocCtx ctx;
+    AllocCtx* prev;
+    AllocScope(cudaStream_t st, cudaMemPool_t pool) : ctx{st, pool}, prev(g_alloc_ctx) { g_alloc_ctx = &ctx; }
+    ~AllocScope() { g_alloc_ctx = prev; }
+};
+cudaError_t dev_alloc(void** p, size_t b);
+void dev_free(void* p);
+
 // Growable device buffer
 struct Buf {
     void* p = nullptr;

@@ -322,8 +322,14 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     }
     PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
     unsigned int tmax = 0, cmax = 0;
-    PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax, cmax, st));
-    if (md->physics == 1 ? !sph_tile_fits(h, tmax) : !tile_fits(h, tmax)) return PD_OK;  // stays on global rows
+    for (;;) {
+        PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax, cmax,
+                          st));
+        if (md->physics == 1 ? sph_tile_fits(h, tmax) : tile_fits(h, tmax)) break;
+        // the densest tile does not fit: narrower tiles (the width is a performance choice only)
+        if (md->tg.TX <= 1) return PD_OK;  // stays on global rows
+        PD_TRY(tile_plan(cl, n, md->tg.TX / 2, md->tg, md->ntiles));
+    }
     md->tcap = tmax;
     PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                       md->vl->r_cut, md->pos32, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));

@@ -3,27 +3,37 @@
 //
 // The reference's only many-systems idiom is a test kernel reading an array of
 // vector_dist / cell-list views (Vector/cuda/vector_dist_gpu_MP_tests.cu:427-781).
-// Here that array is a device table of system descriptors (SysDesc) and every
-// per-step phase is one persistent kernel over the work of all active systems:
-//   kick-drift   256-particle chunks of every system (grid-stride, fixed mapping)
-//   images       256-image chunks (skipped for systems rebuilt this step)
-//   forces       tiles of every system, pulled from an atomic work queue (load
-//                balance over uneven systems); the tile body is the single-system
-//                mixed-form kernel's (pd_mixed_dev.cuh)
+// Here that array is a device table of system descriptors (SysDesc) and one
+// velocity-Verlet step of every active system is ONE CUDA graph of persistent
+// kernels over the work of all systems:
+//   kick-drift   256-particle chunks of every system; largest displacement per system
+//   decide       one block: rebuild flag per system (displacement > skin/2) and the
+//                compacted work lists of the flagged systems
+//   rebuild      flagged systems only, every phase batched over them: offsets ->
+//                FP64 positions + wrap + cell hash, per-system scans, stable
+//                counting sort, reorder, periodic images (count, scan, write),
+//                image cell sort, FP32 staging copies and offsets, tiled Verlet
+//                rows (TMA-staged tiles, the single-system build's row code)
+//   replay       image offsets of the systems that did not rebuild
+//   forces       tiles of every system from an atomic work queue (load balance over
+//                uneven systems); the tile body is the single-system mixed kernel's
 //   kick         chunks, kinetic energy per chunk
-//   energies     one block per system, fixed-order sums of the tile and chunk
-//                partials -> E[step]
-// Partials are indexed by (system, work item), never by CTA, so a system's
-// results do not depend on which other systems share the batch.  The two
-// phase sequences (kick-drift; images..energies) are captured once as CUDA
-// graphs: all sizes live in device memory, so admissions, retirements and
-// rebuilds only rewrite the tables.  The displacement check between them is the
-// one host synchronisation per step; flagged systems are rebuilt individually.
+//   energies     one block per system, fixed-order sums -> E[step]
+// The host synchronises once per step (the graph's end) to read the rebuild
+// flags and error bits and to retire finished systems.  Partials are indexed by
+// (system, work item), never by CTA, and every rebuild phase reproduces the
+// single-system build's arithmetic and orders, so a system's results do not
+// depend on the other systems in the batch and equal the single-system driver's.
 //
-// Admission: FIFO; a request is admitted when a slot is free and its memory
-// estimate fits both the server's HBM budget and cudaMemGetInfo's free memory.
-// Autotuner: per size bucket (floor(log2 N)), the first admitted system times
-// the force kernel for several tile widths and the best one is kept.
+// Slots: a system runs in a slot whose device containers (vector, integrator,
+// build scratch) are kept after the system retires and reused by the next one
+// (buffers only grow), so admission and retirement allocate nothing in steady
+// state.  Admission: FIFO; a request is admitted when a slot is free and its
+// memory estimate fits the server's HBM budget and cudaMemGetInfo's free memory;
+// its first build and forces run through the single-system path, with the slot's
+// image capacity reserved beforehand with a margin for the batched rebuilds.
+// Autotuner: per size bucket (floor(log2 N)), the first admitted system times the
+// force kernel for several tile widths on a throw-away copy; the best is kept.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -33,46 +43,87 @@
 #include <vector>
 
 #include "pd_device.cuh"
+#include "pd_ghost_dev.cuh"
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
 #include "pd_md.cuh"
 #include "pd_mixed.cuh"
 #include "pd_mixed_dev.cuh"
 #include "pd_tile.cuh"
+#include "pd_tile_dev.cuh"
 
 namespace pd {
 
 static constexpr int SRV_P = 2;                       // lanes per particle in the batched force kernel
-static constexpr int SRV_SMEM = 96 * 1024;            // staging bytes per force CTA (fixed: graph-invariant)
-static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged records per tile
-static constexpr int CHUNK = 256;
+static constexpr int SRV_SMEM = 96 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
+static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged FP32 records per tile
+static constexpr int CHUNK = 256;                     // threads per block of the chunked kernels
+static constexpr int SCH = 1024;                      // elements per scan chunk
+static constexpr int MAXS = 1024;                     // slots at most
+
+// rebuild work kinds (items per system)
+// K_P  particle chunks of 256          K_C  cell chunks of 256 (ncell + 1 counters)
+// K_Q  cell scan chunks of 1024        K_QP particle scan chunks of 1024
+// K_I  image chunks of 256 (capacity)  K_A  particle + image chunks of 256 (capacity)
+// K_T  tiles                           K_W  cells, 8 per block (one warp each)
+enum { K_P, K_C, K_Q, K_QP, K_I, K_A, K_T, K_W, NK };
 
 struct SysDesc {
+    // state (slot containers)
     float4* off;
-    const float4* offb;
-    const float4* offK;
-    const int* img_src;
+    float4* offb;
+    float4* offK;
+    double4* pos;
+    int* gid;
+    int* img_src;
+    unsigned char* img_shift;
     float* v;
     float* f;
-    long cap, n_real, n_img;
+    long cap, n_real, img_cap, ncell;
+    unsigned int* n_img;  // device image count of the last build
+    // cell grid (side r_cut + skin) and tiles
+    Grid<double> G;
+    CellGeom C;
+    double L;
     TileGeom tg;
-    const unsigned int* csR;
-    const unsigned int* csI;
-    const unsigned int* nbr;
-    const int* nn;
+    unsigned int* csR;
+    unsigned int* csI;
+    unsigned int* nbr;
+    int* nn;
     long tstride;
-    unsigned int tcap;
+    int max_nn;
     float sx, sy, sz;
+    float lo_thr, hi_thr;
+    double r2;
+    const BoxSet<double>* boxes;
+    const double* shifts;
+    // build scratch
+    unsigned int* cntR;
+    unsigned int* cntI;
+    unsigned int* cell_of;
+    unsigned int* rank;
+    unsigned int* img_cnt;
+    unsigned int* img_start;
+    unsigned int* spart;
+    int* sorted;
+    int* sorted_tmp;
+    double4* scr_pos;
+    int* scr_gid;
+    float* scr_v;
+    int* scr_src;
+    unsigned char* scr_shf;
+    float4* pos32;
+    // step work decomposition (prefixes over the active systems)
     long tile_base, ntiles;
     long chunk_base, nchunk;
     long img_base, nimg_chunk;
     long tpart_base, kpart_base;
-    unsigned long long* maxd2;
+    long cnt[NK];  // rebuild work items per kind
     unsigned int* err;
     double* E;
     int* step;
-    int skip_replay;
     double mass;
+    int slot;
 };
 
 struct BatchHdr {
@@ -81,6 +132,15 @@ struct BatchHdr {
     long tot_tiles, tot_chunks, tot_img;
     unsigned int tile_ctr;
     unsigned int pad1;
+};
+
+// compacted work of the systems flagged for a rebuild this step
+struct RbWork {
+    int nflag;
+    int pad;
+    long tot[NK];
+    int sys[MAXS];
+    long base[NK][MAXS + 1];
 };
 
 __device__ __forceinline__ int find_sys(const SysDesc* __restrict__ D, int nsys, long g, int which) {
@@ -94,13 +154,95 @@ __device__ __forceinline__ int find_sys(const SysDesc* __restrict__ D, int nsys,
     return lo;
 }
 
+// flagged-system index k owning item g of kind K (bases ascending, empty systems skipped)
+__device__ __forceinline__ int find_flagged(const RbWork* __restrict__ W, int K, long g) {
+    int lo = 0, hi = W->nflag - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (W->base[K][mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// grid-stride loop over the items of kind K of the flagged systems; the body sees
+// the system `d` and the item index `c` inside it (block-uniform)
+#define RB_LOOP(K)                                                                                  \
+    for (long g_ = blockIdx.x; g_ < W->tot[K]; g_ += gridDim.x) {                                   \
+        const int k_ = find_flagged(W, K, g_);                                                      \
+        const SysDesc& d = D[W->sys[k_]];                                                           \
+        const long c = g_ - W->base[K][k_];
+
+#define RB_END }
+
+// exclusive scan over a block of 256 threads (valid in every thread); total in `tot`
+__device__ __forceinline__ unsigned int block_scan256(unsigned int v, unsigned int& tot) {
+    __shared__ unsigned int ws[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned int t = lane < 8 ? ws[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            unsigned int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < 8) ws[lane] = t;
+    }
+    __syncthreads();
+    const unsigned int r = x - v + (w ? ws[w - 1] : 0u);
+    tot = ws[7];
+    __syncthreads();
+    return r;
+}
+
+// exclusive scan of longs over a block of 1024 threads
+__device__ __forceinline__ long block_scan1024(long v, long& tot) {
+    __shared__ long ws[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        long t = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            long y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        ws[lane] = t;
+    }
+    __syncthreads();
+    const long r = x - v + (w ? ws[w - 1] : 0L);
+    tot = ws[31];
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// step kernels
+
 __global__ void __launch_bounds__(CHUNK) k_b_kick_drift(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
-                                                        float half, float dt) {
+                                                        float half, float dt, unsigned long long* __restrict__ maxd2,
+                                                        const unsigned int* __restrict__ phase) {
     const int nsys = B->nsys;
     const long tot = B->tot_chunks;
     for (long g = blockIdx.x; g < tot; g += gridDim.x) {
         const int s = find_sys(D, nsys, g, 1);
         const SysDesc& d = D[s];
+        if (phase[d.slot] == 0) continue;  // first build pending: no step yet
         const long i = (g - d.chunk_base) * CHUNK + threadIdx.x;
         double mx = 0;
         if (i < d.n_real) {
@@ -120,19 +262,46 @@ __global__ void __launch_bounds__(CHUNK) k_b_kick_drift(const SysDesc* __restric
             mx = (double)dist2(o.x - b.x, o.y - b.y, o.z - b.z);
         }
         mx = warp_max(mx);
-        if ((threadIdx.x & 31) == 0 && mx > 0) atomic_max_nonneg(d.maxd2, mx);
+        if ((threadIdx.x & 31) == 0 && mx > 0) atomic_max_nonneg(maxd2 + d.slot, mx);
     }
 }
 
-__global__ void __launch_bounds__(CHUNK) k_b_replay(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B) {
+// rebuild flags (first build, or displacement beyond skin/2) and the compacted work
+// of the flagged systems (one block of 1024)
+__global__ void __launch_bounds__(1024) k_b_decide(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
+                                                   const unsigned long long* __restrict__ maxd2, double lim2,
+                                                   int always, unsigned int* __restrict__ flag,
+                                                   const unsigned int* __restrict__ phase, RbWork* __restrict__ W) {
+    const int nsys = B->nsys;
+    const int s = threadIdx.x;
+    int fl = 0;
+    if (s < nsys) {
+        const double d2 = __longlong_as_double((long long)maxd2[D[s].slot]);
+        fl = (always || phase[D[s].slot] == 0 || d2 > lim2) ? 1 : 0;
+        flag[D[s].slot] = (unsigned int)fl;
+    }
+    long nf = 0;
+    const long k = block_scan1024(fl, nf);
+    if (fl) W->sys[k] = s;
+    if (threadIdx.x == 0) W->nflag = (int)nf;
+    for (int K = 0; K < NK; ++K) {
+        long tot = 0;
+        const long b = block_scan1024(fl ? D[s].cnt[K] : 0L, tot);
+        if (fl) W->base[K][k] = b;
+        if (threadIdx.x == 0) W->tot[K] = tot;
+    }
+}
+
+__global__ void __launch_bounds__(CHUNK) k_b_replay(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
+                                                    const unsigned int* __restrict__ flag) {
     const int nsys = B->nsys;
     const long tot = B->tot_img;
     for (long g = blockIdx.x; g < tot; g += gridDim.x) {
         const int s = find_sys(D, nsys, g, 2);
         const SysDesc& d = D[s];
-        if (d.skip_replay) continue;
+        if (flag[d.slot]) continue;
         const long k = (g - d.img_base) * CHUNK + threadIdx.x;
-        if (k < d.n_img) {
+        if (k < (long)*d.n_img) {
             float4 o = d.off[d.img_src[k]], q = d.offK[k];
             float4 r = d.off[d.n_real + k];
             r.x = o.x + q.x;
@@ -156,7 +325,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict_
     const int nsys = B->nsys;
     const long tot = B->tot_tiles;
     for (;;) {
-        // generic-proxy writes of the previous tile are ordered before the next bulk copies
+        // generic-proxy accesses of the previous tile are ordered before the next bulk copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) cur = (long)atomicAdd(&B->tile_ctr, 1u);
@@ -179,12 +348,14 @@ __global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict_
 }
 
 __global__ void __launch_bounds__(CHUNK) k_b_kick(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
-                                                  float half, double* __restrict__ kpart) {
+                                                  float half, double* __restrict__ kpart,
+                                                  const unsigned int* __restrict__ phase) {
     const int nsys = B->nsys;
     const long tot = B->tot_chunks;
     for (long g = blockIdx.x; g < tot; g += gridDim.x) {
         const int s = find_sys(D, nsys, g, 1);
         const SysDesc& d = D[s];
+        if (phase[d.slot] == 0) continue;
         const long c = g - d.chunk_base;
         const long i = c * CHUNK + threadIdx.x;
         double ke = 0;
@@ -203,12 +374,21 @@ __global__ void __launch_bounds__(CHUNK) k_b_kick(const SysDesc* __restrict__ D,
     }
 }
 
-// one block per system: E[step] = (KE, PE, virial, rebuilt) in a fixed order
+// one block per system: E[step] = (KE, PE, virial, rebuilt) in a fixed order; a
+// system whose first build and forces ran in this graph records nothing and steps
+// from the next one
 __global__ void __launch_bounds__(256) k_b_energy(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
-                                                  const double* __restrict__ tpart, const double* __restrict__ kpart) {
+                                                  const double* __restrict__ tpart, const double* __restrict__ kpart,
+                                                  const unsigned int* __restrict__ flag,
+                                                  unsigned int* __restrict__ phase) {
     const int s = blockIdx.x;
     if (s >= B->nsys) return;
     const SysDesc& d = D[s];
+    if (phase[d.slot] == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0) phase[d.slot] = 1;
+        return;
+    }
     double ke = 0, pe = 0, w = 0;
     for (long c = threadIdx.x; c < d.nchunk; c += 256) ke += kpart[d.kpart_base + c];
     for (long t = threadIdx.x; t < d.ntiles; t += 256) {
@@ -223,9 +403,383 @@ __global__ void __launch_bounds__(256) k_b_energy(const SysDesc* __restrict__ D,
         d.E[4 * st] = ke;
         d.E[4 * st + 1] = pe;
         d.E[4 * st + 2] = w;
-        d.E[4 * st + 3] = (double)d.skip_replay;
+        d.E[4 * st + 3] = (double)flag[d.slot];
         *d.step = st + 1;
     }
+}
+
+// ---------------------------------------------------------------------------
+// batched rebuild of the flagged systems.  Each phase restates the arithmetic and
+// the orders of the single-system path (mixed_to_positions + wrap_positions,
+// cl_build + cl_reorder, ghost_generate, md_tiles, mixed_from_positions).
+
+__global__ void __launch_bounds__(CHUNK) k_rb_zero(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_C)
+    const long i = c * CHUNK + threadIdx.x;
+    if (i <= d.ncell) {
+        d.cntR[i] = 0;
+        d.cntI[i] = 0;
+    }
+    RB_END
+}
+
+// offsets -> FP64 positions (first build: the submitted positions), periodic wrap,
+// cell hash with warp-aggregated counts
+__global__ void __launch_bounds__(CHUNK) k_rb_unpack(const SysDesc* __restrict__ D, const RbWork* __restrict__ W,
+                                                     const unsigned int* __restrict__ phase) {
+    RB_LOOP(K_P)
+    const long i = c * CHUNK + threadIdx.x;
+    const bool ok = i < d.n_real;
+    const unsigned int act = __ballot_sync(0xffffffffu, ok);
+    unsigned int bad = 0;
+    if (ok) {
+        double4 r;
+        if (phase[d.slot] == 0) {
+            r = ld4(d.pos, i);
+        } else {
+            float4 o = d.off[i];
+            double cx, cy, cz;
+            d.C.centre(__float_as_uint(o.w), cx, cy, cz);
+            r = make_double4(cx + (double)o.x, cy + (double)o.y, cz + (double)o.z, 0.0);
+        }
+        r.x = periodic_l(r.x, d.L, 0.0);
+        r.y = periodic_l(r.y, d.L, 0.0);
+        r.z = periodic_l(r.z, d.L, 0.0);
+        st4(d.pos, i, r);
+        unsigned int cc = (unsigned int)d.G.cell(r.x, r.y, r.z, bad);
+        d.cell_of[i] = cc;
+        d.rank[i] = warp_agg_inc(d.cntR, cc, act);
+    }
+    if (bad) atomicOr(d.err, ERR_CELL_RANGE);
+    RB_END
+}
+
+// per-system exclusive scans: 0 cntR -> csR (ncell + 1), 1 img_cnt -> img_start (n,
+// total = image count), 2 cntI -> csI (ncell + 1)
+template <int WHICH> struct ScanSel {
+    static __device__ __forceinline__ const unsigned int* in(const SysDesc& d) {
+        return WHICH == 0 ? d.cntR : (WHICH == 1 ? d.img_cnt : d.cntI);
+    }
+    static __device__ __forceinline__ unsigned int* out(const SysDesc& d) {
+        return WHICH == 0 ? d.csR : (WHICH == 1 ? d.img_start : d.csI);
+    }
+    static __device__ __forceinline__ long len(const SysDesc& d) { return WHICH == 1 ? d.n_real : d.ncell + 1; }
+    static constexpr int kind = WHICH == 1 ? K_QP : K_Q;
+};
+
+template <int WHICH>
+__global__ void __launch_bounds__(CHUNK) k_rb_scan_sum(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    typedef ScanSel<WHICH> Sel;
+    RB_LOOP(Sel::kind)
+    const unsigned int* a = Sel::in(d);
+    const long len = Sel::len(d);
+    const long b = c * SCH + 4L * threadIdx.x;
+    unsigned int v = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (b + j < len) v += a[b + j];
+    v = block_sum<unsigned int, CHUNK>(v);
+    if (threadIdx.x == 0) d.spart[c] = v;
+    RB_END
+}
+
+template <int WHICH>
+__global__ void __launch_bounds__(CHUNK) k_rb_scan_mid(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    typedef ScanSel<WHICH> Sel;
+    if ((int)blockIdx.x >= W->nflag) return;
+    const SysDesc& d = D[W->sys[blockIdx.x]];
+    const long len = Sel::len(d);
+    const long np = (len + SCH - 1) / SCH;
+    unsigned int carry = 0;
+    for (long b = 0; b < np; b += CHUNK) {
+        const long i = b + threadIdx.x;
+        const unsigned int v = i < np ? d.spart[i] : 0u;
+        unsigned int tot = 0;
+        const unsigned int e = block_scan256(v, tot);
+        if (i < np) d.spart[i] = carry + e;
+        carry += tot;
+    }
+    if (WHICH == 1 && threadIdx.x == 0) {
+        long m = carry;
+        if (m > d.img_cap || d.n_real + m > d.cap) {
+            atomicOr(d.err, ERR_IMG_OVERFLOW);
+            m = min(d.img_cap, d.cap - d.n_real);
+        }
+        *d.n_img = (unsigned int)m;
+    }
+}
+
+template <int WHICH>
+__global__ void __launch_bounds__(CHUNK) k_rb_scan_apply(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    typedef ScanSel<WHICH> Sel;
+    RB_LOOP(Sel::kind)
+    const unsigned int* a = Sel::in(d);
+    unsigned int* o = Sel::out(d);
+    const long len = Sel::len(d);
+    const long b = c * SCH + 4L * threadIdx.x;
+    unsigned int e[4], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        e[j] = b + j < len ? a[b + j] : 0u;
+        sum += e[j];
+    }
+    unsigned int tot = 0;
+    unsigned int run = d.spart[c] + block_scan256(sum, tot);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (b + j < len) o[b + j] = run;
+        run += e[j];
+    }
+    RB_END
+}
+
+// slot inside the cell (unordered)
+template <int IMG>
+__global__ void __launch_bounds__(CHUNK) k_rb_scatter(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(IMG ? K_I : K_P)
+    const long i = c * CHUNK + threadIdx.x;
+    const long n = IMG ? (long)*d.n_img : d.n_real;
+    const unsigned int* st = IMG ? d.csI : d.csR;
+    if (i < n) d.sorted_tmp[st[d.cell_of[i]] + d.rank[i]] = (int)i;
+    RB_END
+}
+
+// stable order inside every cell: one warp per cell ranks its members by index
+template <int IMG>
+__global__ void __launch_bounds__(CHUNK) k_rb_stabilise(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_W)
+    const long cell = c * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (cell < d.ncell) {
+        const unsigned int* start = IMG ? d.csI : d.csR;
+        const int* in = d.sorted_tmp;
+        int* out = d.sorted;
+        const unsigned int s0 = start[cell], e0 = start[cell + 1];
+        const unsigned int n = e0 - s0;
+        if (n == 1) {
+            if (lane == 0) out[s0] = in[s0];
+        } else if (n > 1 && n <= 32) {
+            int v = lane < (int)n ? in[s0 + lane] : 0x7fffffff;
+            unsigned int rk = 0;
+            for (int j = 0; j < (int)n; ++j) {
+                int o = __shfl_sync(0xffffffffu, v, j);
+                rk += (o < v) ? 1u : 0u;
+            }
+            if (lane < (int)n) out[s0 + rk] = v;
+        } else if (n > 32) {
+            for (unsigned int a = lane; a < n; a += 32) {
+                int v = in[s0 + a];
+                unsigned int rk = 0;
+                for (unsigned int j = 0; j < n; ++j) rk += (in[s0 + j] < v) ? 1u : 0u;
+                out[s0 + rk] = v;
+            }
+        }
+    }
+    RB_END
+}
+
+// reorder of the real particles into cell order: positions, ids, velocities
+__global__ void __launch_bounds__(CHUNK) k_rb_gather(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_P)
+    const long k = c * CHUNK + threadIdx.x;
+    const long n = d.n_real;
+    if (k < n) {
+        const int j = d.sorted[k];
+        d.scr_pos[k] = ld4(d.pos, j);
+        d.scr_gid[k] = d.gid[j];
+        d.scr_v[k] = d.v[j];
+        d.scr_v[n + k] = d.v[d.cap + j];
+        d.scr_v[2 * n + k] = d.v[2 * d.cap + j];
+    }
+    RB_END
+}
+
+// write back + periodic image count per particle (num_shift_ghost_each_part)
+__global__ void __launch_bounds__(CHUNK) k_rb_put_count(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    __shared__ BoxSet<double> Bx;
+    RB_LOOP(K_P)
+    __syncthreads();
+    for (int i = threadIdx.x; i < (int)(sizeof(BoxSet<double>) / 4); i += blockDim.x)
+        reinterpret_cast<int*>(&Bx)[i] = reinterpret_cast<const int*>(d.boxes)[i];
+    __syncthreads();
+    const long k = c * CHUNK + threadIdx.x;
+    const long n = d.n_real;
+    if (k < n) {
+        const double4 r = d.scr_pos[k];
+        st4(d.pos, k, r);
+        d.gid[k] = d.scr_gid[k];
+        d.v[k] = d.scr_v[k];
+        d.v[d.cap + k] = d.scr_v[n + k];
+        d.v[2 * d.cap + k] = d.scr_v[2 * n + k];
+        unsigned int cnt = 0;
+        int old = -1;
+        for (int i = 0; i < Bx.nb; ++i) {
+            int s = Bx.sv[i];
+            if (inside_np(Bx, i, r.x, r.y, r.z) && s != old) {
+                old = s;
+                cnt++;
+            }
+        }
+        d.img_cnt[k] = cnt;
+    }
+    RB_END
+}
+
+// shift_ghost_each_part: image j of particle p goes to slot n + start[p] + j
+__global__ void __launch_bounds__(CHUNK) k_rb_ghost_write(const SysDesc* __restrict__ D,
+                                                          const RbWork* __restrict__ W) {
+    __shared__ BoxSet<double> Bx;
+    RB_LOOP(K_P)
+    __syncthreads();
+    for (int i = threadIdx.x; i < (int)(sizeof(BoxSet<double>) / 4); i += blockDim.x)
+        reinterpret_cast<int*>(&Bx)[i] = reinterpret_cast<const int*>(d.boxes)[i];
+    __syncthreads();
+    const long p = c * CHUNK + threadIdx.x;
+    const long n = d.n_real;
+    if (p < n) {
+        const double4 r = ld4(d.pos, p);
+        long m = d.img_start[p];
+        int old = -1;
+        bool over = false;
+        for (int i = 0; i < Bx.nb; ++i) {
+            int s = Bx.sv[i];
+            if (inside_np(Bx, i, r.x, r.y, r.z) && s != old) {
+                old = s;
+                if (m < d.img_cap && n + m < d.cap) {
+                    double4 q;
+                    q.x = r.x - d.shifts[3 * s];
+                    q.y = r.y - d.shifts[3 * s + 1];
+                    q.z = r.z - d.shifts[3 * s + 2];
+                    q.w = r.w;
+                    st4(d.pos, n + m, q);
+                    d.gid[n + m] = d.gid[p];
+                    d.img_src[m] = (int)p;
+                    d.img_shift[m] = (unsigned char)s;
+                } else {
+                    over = true;
+                }
+                m++;
+            }
+        }
+        if (over) atomicOr(d.err, ERR_IMG_OVERFLOW);
+    }
+    RB_END
+}
+
+// cell hash of the images
+__global__ void __launch_bounds__(CHUNK) k_rb_hash_img(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_I)
+    const long k = c * CHUNK + threadIdx.x;
+    const bool ok = k < (long)*d.n_img;
+    const unsigned int act = __ballot_sync(0xffffffffu, ok);
+    unsigned int bad = 0;
+    if (ok) {
+        const double4 r = ld4(d.pos, d.n_real + k);
+        unsigned int cc = (unsigned int)d.G.cell(r.x, r.y, r.z, bad);
+        d.cell_of[k] = cc;
+        d.rank[k] = warp_agg_inc(d.cntI, cc, act);
+    }
+    if (bad) atomicOr(d.err, ERR_CELL_RANGE);
+    RB_END
+}
+
+__global__ void __launch_bounds__(CHUNK) k_rb_gather_img(const SysDesc* __restrict__ D,
+                                                         const RbWork* __restrict__ W) {
+    RB_LOOP(K_I)
+    const long k = c * CHUNK + threadIdx.x;
+    if (k < (long)*d.n_img) {
+        const int j = d.sorted[k];
+        d.scr_pos[k] = ld4(d.pos, d.n_real + j);
+        d.scr_gid[k] = d.gid[d.n_real + j];
+        d.scr_src[k] = d.img_src[j];
+        d.scr_shf[k] = d.img_shift[j];
+    }
+    RB_END
+}
+
+__global__ void __launch_bounds__(CHUNK) k_rb_put_img(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_I)
+    const long k = c * CHUNK + threadIdx.x;
+    if (k < (long)*d.n_img) {
+        st4(d.pos, d.n_real + k, d.scr_pos[k]);
+        d.gid[d.n_real + k] = d.scr_gid[k];
+        d.img_src[k] = d.scr_src[k];
+        d.img_shift[k] = d.scr_shf[k];
+    }
+    RB_END
+}
+
+// FP32 staging copies of the list build and FP32 offsets of every particle
+__global__ void __launch_bounds__(CHUNK) k_rb_offsets(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_A)
+    const long k = c * CHUNK + threadIdx.x;
+    unsigned int bad = 0;
+    if (k < d.n_real + (long)*d.n_img) {
+        const double4 r = ld4(d.pos, k);
+        d.pos32[k] = make_float4((float)r.x, (float)r.y, (float)r.z, __int_as_float((int)k));
+        unsigned int cc = (unsigned int)d.G.cell(r.x, r.y, r.z, bad);
+        double cx, cy, cz;
+        d.C.centre(cc, cx, cy, cz);
+        d.off[k] = make_float4((float)(r.x - cx), (float)(r.y - cy), (float)(r.z - cz), __uint_as_float(cc));
+    }
+    if (bad) atomicOr(d.err, ERR_CELL_RANGE);
+    RB_END
+}
+
+// offsets at the build (real) and the constant parts of the image offsets
+__global__ void __launch_bounds__(CHUNK) k_rb_image_k(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    RB_LOOP(K_A)
+    const long k = c * CHUNK + threadIdx.x;
+    const long n = d.n_real;
+    if (k < n) {
+        d.offb[k] = d.off[k];
+    } else if (k - n < (long)*d.n_img) {
+        const long m = k - n;
+        const int s = d.img_src[m];
+        double4 xi = ld4(d.pos, n + m), xs = ld4(d.pos, s);
+        double ci[3], cs[3];
+        d.C.centre(__float_as_uint(d.off[n + m].w), ci[0], ci[1], ci[2]);
+        d.C.centre(__float_as_uint(d.off[s].w), cs[0], cs[1], cs[2]);
+        d.offK[m] = make_float4((float)((xi.x - ci[0]) - (xs.x - cs[0])), (float)((xi.y - ci[1]) - (xs.y - cs[1])),
+                                (float)((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
+    }
+    RB_END
+}
+
+// tiled Verlet rows of the flagged systems (persistent CTAs, one mbarrier each)
+__global__ void __launch_bounds__(TBLOCK) k_rb_build(const SysDesc* __restrict__ D, const RbWork* __restrict__ W,
+                                                     unsigned int* __restrict__ nn_max) {
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    float4* sm = reinterpret_cast<float4*>(tile_raw);
+    __shared__ TileSh S;
+    __shared__ unsigned int segb[18][TXMAX + 3];
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    unsigned int parity = 0;
+    RB_LOOP(K_T)
+    // generic-proxy reads of the previous tile are ordered before the next bulk copies
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    tile_layout(d.tg, c, d.csR, d.csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    if (ib == ie) continue;
+    tile_segb(S, segb);
+    const int st = tile_stage_bar<float>(d.pos32, d.pos32 + d.n_real, S, sm, SRV_CAP, d.err, &bar, parity);
+    if (st > 0) parity ^= 1u;
+    if (st < 0) {
+        // the tile does not fit (error bit set; the next tile may), or the bounded
+        // wait gave up: its barrier phase cannot be tracked further, so stop
+        if (S.total <= SRV_CAP) break;
+        continue;
+    }
+    tile_rows<double>(S, segb, sm, d.pos, d.r2, d.lo_thr, d.hi_thr, d.nbr, d.nn, d.tstride, d.max_nn, d.err, nn_max);
+    RB_END
+}
+
+__global__ void k_srv_iota(int* __restrict__ g, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        g[i] = (int)i;
 }
 
 }  // namespace pd
@@ -233,6 +787,23 @@ __global__ void __launch_bounds__(256) k_b_energy(const SysDesc* __restrict__ D,
 using namespace pd;
 
 // ---------------------------------------------------------------------------
+struct SrvSlot {
+    pd_vd h = nullptr;
+    pd_md md = nullptr;
+    int vp = -1, fp = -1;
+    long img_cap = 0;
+    Buf cntI, cell_of, rank, sorted, sorted_tmp, spart, scr_pos, scr_gid, scr_v, scr_src, scr_shf, Edev, step;
+    void release() {
+        Buf* b[] = {&cntI, &cell_of, &rank, &sorted, &sorted_tmp, &spart, &scr_pos,
+                    &scr_gid, &scr_v, &scr_src, &scr_shf, &Edev, &step};
+        for (Buf* x : b) x->release();
+        if (md) pd_md_destroy(md);
+        if (h) pd_destroy(h);
+        md = nullptr;
+        h = nullptr;
+    }
+};
+
 struct SrvReq {
     long ticket = 0;
     long n = 0;
@@ -242,11 +813,10 @@ struct SrvReq {
     std::vector<double> x, v, xo, E;
     double t_submit = 0, t_admit = 0, t_done = 0;
     size_t bytes = 0;
-    pd_vd h = nullptr;
-    pd_md md = nullptr;
-    Buf Edev, step;
     int slot = -1;
     int bucket = 0;
+    int done_steps = 0;
+    bool first = true;  // the next step graph runs its first build and forces
 };
 
 struct pd_srv_s {
@@ -259,24 +829,27 @@ struct pd_srv_s {
     std::map<long, std::unique_ptr<SrvReq>> reqs;
     std::deque<long> queue;
     std::vector<SrvReq*> active;
+    std::vector<SrvSlot> slots;
     size_t used = 0;
     // device tables (fixed capacity: graph-invariant pointers)
-    Buf desc, hdr, maxd2, errs, tpart, kpart;
+    Buf desc, hdr, maxd2, errs, flags, phase, work, nnmax, tpart, kpart;
     long tpart_cap = 0, kpart_cap = 0;
     std::vector<SysDesc> hdesc;
     BatchHdr hhdr;
-    unsigned long long* maxd2_h = nullptr;
+    unsigned int* flags_h = nullptr;  // pinned: rebuild flag and error bits per slot after each step
+    unsigned int* errs_h = nullptr;
     cudaStream_t st = nullptr;
-    cudaGraphExec_t gA = nullptr, gB = nullptr;
-    int grid_force = 0, grid_chunks = 0;
+    cudaMemPool_t pool = nullptr;  // device memory of the slots (stream-ordered on st)
+    cudaGraphExec_t gstep = nullptr;
     bool dirty = true;
     // autotuner: size bucket -> tile width
     bool autotune = true;
     int fixed_tx = 0;
     std::map<int, int> tuned;
     // statistics
-    long particle_steps = 0, systems_done = 0, replays = 0, rebuilds = 0;
+    long particle_steps = 0, systems_done = 0, steps_run = 0, rebuilds = 0;
     double tune_ms = 0;
+    double ms[4] = {0, 0, 0, 0};  // admit, of which slot reset, step, retire
 };
 
 namespace pd {
@@ -286,42 +859,97 @@ static double now_s(pd_srv s) {
 }
 
 static size_t estimate_bytes(long n) {
-    // positions (FP64 record + FP32 offsets + build copies), images (~30% for small
-    // boxes), FP32 velocity / force, rows of ~100 16-bit entries, cell tables
+    // positions (FP64 record + FP32 offsets + staging copies), images (~30% for
+    // mid-size boxes), FP32 velocity / force, rows of ~100 16-bit entries, scratch
     return (size_t)n * 700 + ((size_t)8 << 20);
 }
 
+// periodic images expected for n particles spread over a cubic box of side L, ghost g
+static long image_estimate(long n, double L, double g) {
+    double r = ((L + 2 * g) * (L + 2 * g) * (L + 2 * g)) / (L * L * L) - 1.0;
+    return (long)(n * r);
+}
+
 static void fill_desc(pd_srv s, SrvReq* r, SysDesc& d) {
-    pd_vd h = r->h;
-    pd_md md = r->md;
+    SrvSlot& sl = s->slots[r->slot];
+    pd_vd h = sl.h;
+    pd_md md = sl.md;
+    pd_cl cl = md->vl->cl;
     memset(&d, 0, sizeof(d));
     d.off = md->off.as<float4>();
     d.offb = md->offb.as<float4>();
     d.offK = md->offK.as<float4>();
+    d.pos = (double4*)h->pos;
+    d.gid = h->gid;
     d.img_src = h->img_src.as<int>();
-    d.v = (float*)h->props[md->mp.vel_prop].d;
-    d.f = (float*)h->props[md->mp.force_prop].d;
+    d.img_shift = h->img_shift.as<unsigned char>();
+    d.v = (float*)h->props[sl.vp].d;
+    d.f = (float*)h->props[sl.fp].d;
     d.cap = h->cap;
     d.n_real = h->n_real;
-    d.n_img = h->n_img;
+    d.img_cap = sl.img_cap;
+    d.ncell = cl->ncells;
+    d.n_img = &h->ctrl->n_img;
+    for (int k = 0; k < 3; ++k) {
+        d.G.lo[k] = cl->box_lo[k];
+        d.G.sp[k] = cl->spacing[k];
+        d.G.gs[k] = cl->gs[k];
+        d.C.lo[k] = cl->box_lo[k];
+        d.C.sp[k] = cl->spacing[k];
+        d.C.gs[k] = cl->gs[k];
+    }
+    d.G.pad = cl->pad;
+    d.C.pad = cl->pad;
+    d.L = r->L;
     d.tg = md->tg;
     d.csR = md->csR.as<unsigned int>();
     d.csI = md->csI.as<unsigned int>();
     d.nbr = md->tnbr.as<unsigned int>();
     d.nn = md->tnn.as<int>();
     d.tstride = md->tstride;
-    d.tcap = md->tcap;
-    d.sx = (float)md->vl->cl->spacing[0];
-    d.sy = (float)md->vl->cl->spacing[1];
-    d.sz = (float)md->vl->cl->spacing[2];
+    d.max_nn = md->tmax_nn;
+    d.sx = (float)cl->spacing[0];
+    d.sy = (float)cl->spacing[1];
+    d.sz = (float)cl->spacing[2];
+    const double rl = md->vl->r_cut;
+    const double band = fp32_band(h, rl);
+    d.lo_thr = (float)(rl * rl - band);
+    d.hi_thr = (float)(rl * rl + band);
+    d.r2 = rl * rl;
+    d.boxes = h->boxes.as<BoxSet<double>>();
+    d.shifts = h->shifts.as<double>();
+    d.cntR = cl->cell_cnt.as<unsigned int>();
+    d.cntI = sl.cntI.as<unsigned int>();
+    d.cell_of = sl.cell_of.as<unsigned int>();
+    d.rank = sl.rank.as<unsigned int>();
+    d.img_cnt = h->img_cnt.as<unsigned int>();
+    d.img_start = h->img_start.as<unsigned int>();
+    d.spart = sl.spart.as<unsigned int>();
+    d.sorted = sl.sorted.as<int>();
+    d.sorted_tmp = sl.sorted_tmp.as<int>();
+    d.scr_pos = sl.scr_pos.as<double4>();
+    d.scr_gid = sl.scr_gid.as<int>();
+    d.scr_v = sl.scr_v.as<float>();
+    d.scr_src = sl.scr_src.as<int>();
+    d.scr_shf = sl.scr_shf.as<unsigned char>();
+    d.pos32 = md->pos32.as<float4>();
     d.ntiles = md->ntiles;
     d.nchunk = (h->n_real + CHUNK - 1) / CHUNK;
-    d.nimg_chunk = (h->n_img + CHUNK - 1) / CHUNK;
-    d.maxd2 = s->maxd2.as<unsigned long long>() + r->slot;
-    d.err = &h->ctrl->err;
-    d.E = r->Edev.as<double>();
-    d.step = r->step.as<int>();
+    d.nimg_chunk = (sl.img_cap + CHUNK - 1) / CHUNK;
+    const long n = h->n_real, nc = cl->ncells;
+    d.cnt[K_P] = (n + CHUNK - 1) / CHUNK;
+    d.cnt[K_C] = (nc + 1 + CHUNK - 1) / CHUNK;
+    d.cnt[K_Q] = (nc + 1 + SCH - 1) / SCH;
+    d.cnt[K_QP] = (n + SCH - 1) / SCH;
+    d.cnt[K_I] = (sl.img_cap + CHUNK - 1) / CHUNK;
+    d.cnt[K_A] = (n + sl.img_cap + CHUNK - 1) / CHUNK;
+    d.cnt[K_T] = md->ntiles;
+    d.cnt[K_W] = (nc + 7) / 8;
+    d.err = s->errs.as<unsigned int>() + r->slot;
+    d.E = sl.Edev.as<double>();
+    d.step = sl.step.as<int>();
     d.mass = md->mp.mass;
+    d.slot = r->slot;
 }
 
 // rebuild the descriptor table, prefixes and partial-buffer layout
@@ -331,9 +959,7 @@ static int upload_tables(pd_srv s) {
     long tb = 0, cb = 0, ib = 0, tp = 0, kp = 0;
     for (int k = 0; k < ns; ++k) {
         SysDesc& d = s->hdesc[k];
-        int skip = d.skip_replay;
         fill_desc(s, s->active[k], d);
-        d.skip_replay = skip;
         d.tile_base = tb;
         d.chunk_base = cb;
         d.img_base = ib;
@@ -361,7 +987,9 @@ static int upload_tables(pd_srv s) {
     return PD_OK;
 }
 
-static int capture_graphs(pd_srv s) {
+static constexpr int GRAPH_KERNELS = 30;  // kernel nodes of the step graph
+
+static int capture_graph(pd_srv s) {
     float half = (float)(0.5 * s->dt / 1.0), dt = (float)s->dt;
     LJP<float> P;
     P.eps24 = (float)(24.0 * s->lj.eps);
@@ -370,86 +998,190 @@ static int capture_graphs(pd_srv s) {
     float rc = (float)s->lj.r_cut;
     P.rc2 = rc * rc;
     PD_CUDA(cudaFuncSetAttribute(k_b_force, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
-    int sms = 148, dev = 0, per = 1;
+    PD_CUDA(cudaFuncSetAttribute(k_rb_build, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
+    int sms = 148, dev = 0, per = 1, perb = 1;
     PD_CUDA(cudaGetDevice(&dev));
     PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_force, FBLOCK_T, SRV_SMEM));
-    s->grid_force = sms * std::max(per, 1);
-    s->grid_chunks = sms * 8;
+    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_rb_build, TBLOCK, SRV_SMEM));
+    const int gf = sms * std::max(per, 1), gb = sms * std::max(perb, 1), gc = sms * 8;
     const SysDesc* D = s->desc.as<SysDesc>();
     BatchHdr* B = s->hdr.as<BatchHdr>();
+    RbWork* W = s->work.as<RbWork>();
+    unsigned long long* md2 = s->maxd2.as<unsigned long long>();
+    unsigned int* fl = s->flags.as<unsigned int>();
+    const double lim2 = 0.25 * s->skin * s->skin;
+    const int always = s->skin <= 0 ? 1 : 0;
+    const int M = s->max_slots;
     cudaGraph_t g = nullptr;
-    PD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    cudaMemsetAsync(s->maxd2.p, 0, sizeof(unsigned long long) * s->max_slots, s->st);
-    k_b_kick_drift<<<s->grid_chunks, CHUNK, 0, s->st>>>(D, B, half, dt);
-    PD_CUDA(cudaStreamEndCapture(s->st, &g));
-    PD_CUDA(cudaGraphInstantiate(&s->gA, g, 0));
+    cudaStream_t st = s->st;
+    PD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(md2, 0, sizeof(unsigned long long) * M, st);
+    cudaMemsetAsync(&B->tile_ctr, 0, sizeof(unsigned int), st);
+    unsigned int* ph = s->phase.as<unsigned int>();
+    k_b_kick_drift<<<gc, CHUNK, 0, st>>>(D, B, half, dt, md2, ph);
+    k_b_decide<<<1, 1024, 0, st>>>(D, B, md2, lim2, always, fl, ph, W);
+    // batched rebuild of the flagged systems
+    k_rb_zero<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_unpack<<<gc, CHUNK, 0, st>>>(D, W, ph);
+    k_rb_scan_sum<0><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_mid<0><<<M, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_apply<0><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scatter<0><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_stabilise<0><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_gather<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_put_count<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_sum<1><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_mid<1><<<M, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_apply<1><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_ghost_write<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_hash_img<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_sum<2><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_mid<2><<<M, CHUNK, 0, st>>>(D, W);
+    k_rb_scan_apply<2><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_scatter<1><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_stabilise<1><<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_gather_img<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_put_img<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_offsets<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_image_k<<<gc, CHUNK, 0, st>>>(D, W);
+    k_rb_build<<<gb, TBLOCK, SRV_SMEM, st>>>(D, W, s->nnmax.as<unsigned int>());
+    // step of every system
+    k_b_replay<<<gc, CHUNK, 0, st>>>(D, B, fl);
+    k_b_force<<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>());
+    k_b_kick<<<gc, CHUNK, 0, st>>>(D, B, half, s->kpart.as<double>(), ph);
+    k_b_energy<<<M, 256, 0, st>>>(D, B, s->tpart.as<double>(), s->kpart.as<double>(), fl, ph);
+    cudaMemcpyAsync(s->flags_h, fl, sizeof(unsigned int) * M, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(s->errs_h, s->errs.p, sizeof(unsigned int) * M, cudaMemcpyDeviceToHost, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (ce != cudaSuccess) {
+        set_error("serving: graph capture failed: %s", cudaGetErrorString(ce));
+        return PD_ECUDA;
+    }
+    ce = cudaGraphInstantiate(&s->gstep, g, 0);
     cudaGraphDestroy(g);
-    PD_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    cudaMemsetAsync(&B->tile_ctr, 0, sizeof(unsigned int), s->st);
-    k_b_replay<<<s->grid_chunks, CHUNK, 0, s->st>>>(D, B);
-    k_b_force<<<s->grid_force, FBLOCK_T, SRV_SMEM, s->st>>>(D, B, P, s->tpart.as<double>());
-    k_b_kick<<<s->grid_chunks, CHUNK, 0, s->st>>>(D, B, half, s->kpart.as<double>());
-    k_b_energy<<<s->max_slots, 256, 0, s->st>>>(D, B, s->tpart.as<double>(), s->kpart.as<double>());
-    PD_CUDA(cudaStreamEndCapture(s->st, &g));
-    PD_CUDA(cudaGraphInstantiate(&s->gB, g, 0));
-    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        set_error("serving: graph instantiation failed: %s", cudaGetErrorString(ce));
+        return PD_ECUDA;
+    }
     return PD_OK;
 }
 
-static int make_system(pd_srv s, SrvReq* r, pd_vd* hout, pd_md* mout) {
-    double lo[3] = {0, 0, 0}, hi[3] = {r->L, r->L, r->L};
-    int bc[3] = {PD_PERIODIC, PD_PERIODIC, PD_PERIODIC};
-    double rl = s->lj.r_cut + s->skin;
-    double g[3] = {rl, rl, rl};
-    pd_vd h = nullptr;
-    PD_TRY(pd_create(3, PD_F64, r->n, lo, hi, bc, g, 0, &h));
-    *hout = h;
-    int vp = -1, fp = -1;
-    PD_TRY(pd_add_prop(h, PD_F32, 3, &vp));
-    PD_TRY(pd_add_prop(h, PD_F32, 3, &fp));
-    PD_TRY(pd_h2d_pos(h, r->x.data(), 0, r->n, s->st));
+// (re)initialise a slot's containers for a system of n particles in a box of side L
+static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
+    const double rl = s->lj.r_cut + s->skin;
+    if (!sl.h) {
+        double lo[3] = {0, 0, 0}, hi[3] = {r->L, r->L, r->L};
+        int bc[3] = {PD_PERIODIC, PD_PERIODIC, PD_PERIODIC};
+        double g[3] = {rl, rl, rl};
+        PD_TRY(pd_create(3, PD_F64, 0, lo, hi, bc, g, 0, &sl.h));  // sized below, on the server's stream
+        PD_TRY(pd_add_prop(sl.h, PD_F32, 3, &sl.vp));
+        PD_TRY(pd_add_prop(sl.h, PD_F32, 3, &sl.fp));
+        pd_md_params_t mp;
+        memset(&mp, 0, sizeof(mp));
+        mp.dt = s->dt;
+        mp.mass = 1.0;
+        mp.skin = s->skin;
+        mp.vel_prop = sl.vp;
+        mp.force_prop = sl.fp;
+        mp.precision = PD_PREC_MIXED;
+        PD_TRY(pd_md_create(sl.h, &s->lj, &mp, &sl.md));
+    } else {
+        pd_vd h = sl.h;
+        pd_md md = sl.md;
+        for (int d = 0; d < 3; ++d) {
+            h->lo[d] = 0.0;
+            h->hi[d] = r->L;
+        }
+        h->nbox = 0;  // the ghost boxes of the new box are uploaded by the first build
+        h->n_img = 0;
+        PD_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), s->st));
+        memset(h->ctrl_h, 0, sizeof(Ctrl));
+        PD_TRY(cl_geometry(md->vl->cl, h, rl, 1.013, 1));
+        md->ready = false;
+        md->steps = 0;
+        md->builds = 0;
+        md->off_valid = false;
+        md->tiles_active = false;
+        md->tmax_nn = 0;
+        md->nblk = force_blocks(r->n);
+        PD_TRY(md->fpart.ensure(sizeof(double) * 2 * md->nblk));
+        PD_TRY(md->kpart.ensure(sizeof(double) * md->nblk));
+        PD_TRY(md->xb.ensure((size_t)r->n * h->pos_bytes));
+    }
+    sl.md->tile_tx = tx;
+    // capacities for the batched rebuilds, reserved before the first build so that
+    // the buffers it fills are not reallocated afterwards
+    sl.img_cap = (long)(1.3 * image_estimate(r->n, r->L, rl)) + 2048;
+    pd_vd h = sl.h;
+    pd_md md = sl.md;
+    PD_TRY(ensure_capacity(h, r->n + sl.img_cap + 1, s->st));
+    h->n_real = h->n_total = r->n;
+    h->img_valid = false;
+    h->epoch++;
+    pd::launch(k_srv_iota, grid_for(r->n, CHUNK), CHUNK, 0, s->st, h->gid, r->n);
+    PD_LAUNCH_CHECK();
+    PD_TRY(md->off.ensure(sizeof(float4) * (size_t)h->cap));
+    PD_TRY(md->offK.ensure(sizeof(float4) * (size_t)sl.img_cap));
+    PD_TRY(md->pos32.ensure(sizeof(float4) * (size_t)h->cap));
+    PD_TRY(h->img_src.ensure(sizeof(int) * (size_t)sl.img_cap));
+    PD_TRY(h->img_shift.ensure((size_t)sl.img_cap));
+    return PD_OK;
+}
+
+// scratch of the batched rebuild, from the slot's geometry after the first build
+static int slot_scratch(pd_srv s, SrvSlot& sl, SrvReq* r) {
+    pd_vd h = sl.h;
+    pd_md md = sl.md;
+    pd_cl cl = md->vl->cl;
+    const long n = r->n, nc = cl->ncells, m = std::max(n, sl.img_cap);
+    PD_TRY(cl->cell_cnt.ensure(sizeof(unsigned int) * (nc + 1)));
+    PD_TRY(sl.cntI.ensure(sizeof(unsigned int) * (nc + 1)));
+    PD_TRY(sl.cell_of.ensure(sizeof(unsigned int) * m));
+    PD_TRY(sl.rank.ensure(sizeof(unsigned int) * m));
+    PD_TRY(sl.sorted.ensure(sizeof(int) * m));
+    PD_TRY(sl.sorted_tmp.ensure(sizeof(int) * m));
+    PD_TRY(sl.spart.ensure(sizeof(unsigned int) * (std::max(nc + 1, n) / SCH + 2)));
+    PD_TRY(sl.scr_pos.ensure(sizeof(double4) * m));
+    PD_TRY(sl.scr_gid.ensure(sizeof(int) * m));
+    PD_TRY(sl.scr_v.ensure(sizeof(float) * 3 * n));
+    PD_TRY(sl.scr_src.ensure(sizeof(int) * sl.img_cap));
+    PD_TRY(sl.scr_shf.ensure((size_t)sl.img_cap));
+    PD_TRY(h->img_cnt.ensure(sizeof(unsigned int) * (n + 1)));
+    PD_TRY(h->img_start.ensure(sizeof(unsigned int) * (n + 1)));
+    PD_TRY(sl.Edev.ensure(sizeof(double) * 4 * (r->steps > 0 ? r->steps : 1)));
+    PD_TRY(sl.step.ensure(sizeof(int)));
+    PD_CUDA(cudaMemsetAsync(sl.step.p, 0, sizeof(int), s->st));
+    PD_CUDA(cudaMemsetAsync(s->errs.as<unsigned int>() + r->slot, 0, sizeof(unsigned int), s->st));
+    return PD_OK;
+}
+
+static int load_state(pd_srv s, SrvSlot& sl, SrvReq* r) {
+    PD_TRY(pd_h2d_pos(sl.h, r->x.data(), 0, r->n, s->st));
     std::vector<float> vc(3 * r->n);
     for (long i = 0; i < r->n; ++i)
         for (int d = 0; d < 3; ++d) vc[(size_t)d * r->n + i] = (float)r->v[3 * i + d];
-    PD_TRY(pd_h2d_prop(h, vp, vc.data(), 0, r->n, s->st));
-    PD_CUDA(cudaStreamSynchronize(s->st));  // vc is a local
-    pd_md_params_t mp;
-    memset(&mp, 0, sizeof(mp));
-    mp.dt = s->dt;
-    mp.mass = 1.0;
-    mp.skin = s->skin;
-    mp.vel_prop = vp;
-    mp.force_prop = fp;
-    mp.precision = PD_PREC_MIXED;
-    PD_TRY(pd_md_create(h, &s->lj, &mp, mout));
+    PD_TRY(pd_h2d_prop(sl.h, sl.vp, vc.data(), 0, r->n, s->st));
+    PD_CUDA(cudaStreamSynchronize(s->st));  // vc is a local (pageable copies may still be staged)
     return PD_OK;
 }
 
-static int autotune_tx_on(pd_srv s, SrvReq* r);
+static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r);
 
 // time the single-system force for candidate tile widths on a throw-away copy of
 // the system (so the admitted system starts from the submitted state); keep the fastest
 static int autotune_tx(pd_srv s, SrvReq* r) {
-    SrvReq tmp;
-    tmp.n = r->n;
-    tmp.L = r->L;
-    tmp.x = r->x;
-    tmp.v = r->v;
-    int rc = make_system(s, &tmp, &tmp.h, &tmp.md);
-    if (rc == PD_OK) {
-        std::swap(tmp.h, r->h);
-        std::swap(tmp.md, r->md);
-        rc = autotune_tx_on(s, r);
-        std::swap(tmp.h, r->h);
-        std::swap(tmp.md, r->md);
-    }
-    if (tmp.md) pd_md_destroy(tmp.md);
-    if (tmp.h) pd_destroy(tmp.h);
+    AllocScope scope(s->st, s->pool);
+    SrvSlot tmp;
+    int rc = slot_reset(s, tmp, r, 0);
+    if (rc == PD_OK) rc = load_state(s, tmp, r);
+    if (rc == PD_OK) rc = autotune_tx_on(s, tmp, r);
+    cudaStreamSynchronize(s->st);
+    tmp.release();
     return rc;
 }
 
-static int autotune_tx_on(pd_srv s, SrvReq* r) {
+static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
     static const int cand[] = {3, 5, 7, 9, 12};
     cudaEvent_t a, b;
     PD_CUDA(cudaEventCreate(&a));
@@ -458,12 +1190,12 @@ static int autotune_tx_on(pd_srv s, SrvReq* r) {
     float best_ms = 1e30f;
     double t0 = now_s(s);
     for (int tx : cand) {
-        r->md->tile_tx = tx;
-        int rc = md_rebuild(r->md, s->st);
-        if (rc != PD_OK || !r->md->tiles_active || r->md->tcap > SRV_CAP) continue;
-        PD_TRY(md_forces(r->md, s->st));  // warm
+        sl.md->tile_tx = tx;
+        int rc = md_rebuild(sl.md, s->st);
+        if (rc != PD_OK || !sl.md->tiles_active || sl.md->tcap > SRV_CAP) continue;
+        PD_TRY(md_forces(sl.md, s->st));  // warm
         PD_CUDA(cudaEventRecord(a, s->st));
-        for (int k = 0; k < 3; ++k) PD_TRY(md_forces(r->md, s->st));
+        for (int k = 0; k < 3; ++k) PD_TRY(md_forces(sl.md, s->st));
         PD_CUDA(cudaEventRecord(b, s->st));
         PD_CUDA(cudaEventSynchronize(b));
         float ms = 0;
@@ -484,55 +1216,69 @@ static int autotune_tx_on(pd_srv s, SrvReq* r) {
     return PD_OK;
 }
 
+// Admission is host-side setup only: geometry, tile plan and capacities of the
+// slot, the submitted state uploaded; the first build and forces run inside the
+// next step graph (phase 0), restating the single-system first build.
 static int admit_one(pd_srv s, SrvReq* r, int slot) {
     r->slot = slot;
     r->bucket = (int)std::floor(std::log2((double)std::max(r->n, 1L)));
     if (s->autotune && !s->tuned.count(r->bucket)) PD_TRY(autotune_tx(s, r));
-    PD_TRY(make_system(s, r, &r->h, &r->md));
-    r->md->tile_tx = s->autotune ? s->tuned[r->bucket] : s->fixed_tx;
-    PD_TRY(r->Edev.ensure(sizeof(double) * 4 * (r->steps > 0 ? r->steps : 1)));
-    PD_TRY(r->step.ensure(sizeof(int)));
-    PD_CUDA(cudaMemsetAsync(r->step.p, 0, sizeof(int), s->st));
-    PD_TRY(pd_md_run(r->md, 0, s->st, nullptr));  // first build + forces
-    if (!r->md->tiles_active || r->md->tcap > SRV_CAP) {
-        set_error("serving: system of %ld particles does not fit the batched tile kernel", r->n);
-        return PD_EOVERFLOW;
-    }
+    SrvSlot& sl = s->slots[slot];
+    const double t0 = now_s(s);
+    PD_TRY(slot_reset(s, sl, r, s->autotune ? s->tuned[r->bucket] : s->fixed_tx));
+    s->ms[1] += 1e3 * (now_s(s) - t0);
+    pd_vd h = sl.h;
+    pd_md md = sl.md;
+    pd_cl cl = md->vl->cl;
+    const long n = r->n;
+    PD_TRY(ghost_boxes_upload(h, s->st));
+    PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
+    // row capacity of the tiled build (tile_build's first estimate)
+    md->tstride = std::max(32L, ((n + 31) / 32) * 32);
+    const double rl = md->vl->r_cut;
+    const double vol = r->L * r->L * r->L;
+    md->tmax_nn = (((int)((double)n / vol * 4.18879 * rl * rl * rl * 1.5 + 32)) + 1) & ~1;
+    PD_TRY(md->tnbr.ensure(sizeof(unsigned short) * (size_t)md->tstride * md->tmax_nn));
+    PD_TRY(md->tnn.ensure(sizeof(int) * (size_t)md->tstride));
+    PD_TRY(md->csR.ensure(sizeof(unsigned int) * (cl->ncells + 1)));
+    PD_TRY(md->csI.ensure(sizeof(unsigned int) * (cl->ncells + 1)));
+    PD_TRY(md->offb.ensure(sizeof(float4) * (size_t)n));
+    md->tcap = SRV_CAP;
+    md->tiles_active = true;
+    md->off_valid = true;
+    md->ready = true;
+    PD_TRY(slot_scratch(s, sl, r));
+    PD_TRY(load_state(s, sl, r));
+    PD_CUDA(cudaMemsetAsync(s->phase.as<unsigned int>() + slot, 0, sizeof(unsigned int), s->st));
     r->x.clear();
     r->x.shrink_to_fit();
     r->v.clear();
     r->v.shrink_to_fit();
     r->state = 1;
+    r->done_steps = 0;
+    r->first = true;
     r->t_admit = now_s(s);
     return PD_OK;
 }
 
-static void free_system(SrvReq* r) {
-    if (r->md) pd_md_destroy(r->md);
-    if (r->h) pd_destroy(r->h);
-    r->md = nullptr;
-    r->h = nullptr;
-    r->Edev.release();
-    r->step.release();
-}
-
-static int retire(pd_srv s, SrvReq* r) {
-    pd_vd h = r->h;
-    PD_TRY(mixed_to_positions(h, r->md->vl->cl, r->md->off, s->st));
-    std::vector<double> xs(3 * r->n);
-    std::vector<long> gid(r->n);
-    PD_TRY(pd_d2h_pos(h, xs.data(), 0, r->n, s->st));
-    PD_TRY(pd_d2h_gid(h, gid.data(), 0, r->n, s->st));
-    r->xo.assign(3 * r->n, 0.0);
-    for (long i = 0; i < r->n; ++i)
-        for (int d = 0; d < 3; ++d) r->xo[3 * gid[i] + d] = xs[3 * i + d];
-    r->E.assign(4 * (size_t)r->steps, 0.0);
-    if (r->steps > 0)
-        PD_CUDA(cudaMemcpy(r->E.data(), r->Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost));
-    PD_TRY(read_ctrl(h, s->st));
-    const bool bad = (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW)) != 0;
-    free_system(r);
-    r->state = bad ? 3 : 2;
+static int retire(pd_srv s, SrvReq* r, bool failed) {
+    SrvSlot& sl = s->slots[r->slot];
+    pd_vd h = sl.h;
+    if (!failed) {
+        PD_TRY(mixed_to_positions(h, sl.md->vl->cl, sl.md->off, s->st));
+        std::vector<double> xs(3 * r->n);
+        std::vector<int> gid(r->n);
+        PD_TRY(pd_d2h_pos(h, xs.data(), 0, r->n, s->st));
+        PD_CUDA(cudaMemcpyAsync(gid.data(), h->gid, sizeof(int) * r->n, cudaMemcpyDeviceToHost, s->st));
+        r->E.assign(4 * (size_t)r->steps, 0.0);
+        PD_CUDA(cudaMemcpyAsync(r->E.data(), sl.Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost,
+                                s->st));
+        PD_CUDA(cudaStreamSynchronize(s->st));
+        r->xo.assign(3 * r->n, 0.0);
+        for (long i = 0; i < r->n; ++i)
+            for (int d = 0; d < 3; ++d) r->xo[3 * (size_t)gid[i] + d] = xs[3 * i + d];
+    }
+    r->state = failed ? 3 : 2;
     r->t_done = now_s(s);
     s->used -= r->bytes;
     s->systems_done++;
@@ -545,7 +1291,7 @@ extern "C" {
 
 int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj, double dt, double skin,
                   pd_srv* out) {
-    if (!out || !lj || max_slots < 1 || max_slots > 1024 || hbm_budget_bytes <= 0 || !(dt > 0) || skin < 0)
+    if (!out || !lj || max_slots < 1 || max_slots > MAXS || hbm_budget_bytes <= 0 || !(dt > 0) || skin < 0)
         return PD_EINVAL;
     pd_srv s = new pd_srv_s();
     s->budget = hbm_budget_bytes;
@@ -554,25 +1300,54 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
     s->dt = dt;
     s->skin = skin;
     s->t0 = std::chrono::steady_clock::now();
+    s->slots.resize(max_slots);
     memset(&s->hhdr, 0, sizeof(s->hhdr));
     int r = PD_OK;
     // partial buffers sized from the budget: at most budget/700 particles in flight
     long pmax = hbm_budget_bytes / 700 + 4096L * max_slots;
     s->kpart_cap = pmax / CHUNK + 2L * max_slots;
     s->tpart_cap = pmax / 4 + 4096L * max_slots;  // small boxes have about one tile per 7 particles
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaMemPoolProps pp;
+        memset(&pp, 0, sizeof(pp));
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = dev;
+        if (cudaMemPoolCreate(&s->pool, &pp) != cudaSuccess) {
+            cudaGetLastError();
+            s->pool = nullptr;
+            delete s;
+            set_error("pd_srv_create: memory pool creation failed");
+            return PD_ECUDA;
+        }
+        unsigned long long keep = ~0ull;  // freed slot memory stays in the pool for reuse
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
         (r = s->desc.ensure(sizeof(SysDesc) * max_slots)) != PD_OK || (r = s->hdr.ensure(sizeof(BatchHdr))) != PD_OK ||
         (r = s->maxd2.ensure(sizeof(unsigned long long) * max_slots)) != PD_OK ||
+        (r = s->errs.ensure(sizeof(unsigned int) * max_slots)) != PD_OK ||
+        (r = s->flags.ensure(sizeof(unsigned int) * max_slots)) != PD_OK ||
+        (r = s->phase.ensure(sizeof(unsigned int) * max_slots)) != PD_OK ||
+        (r = s->work.ensure(sizeof(RbWork))) != PD_OK || (r = s->nnmax.ensure(sizeof(unsigned int))) != PD_OK ||
         (r = s->tpart.ensure(sizeof(double) * 2 * s->tpart_cap)) != PD_OK ||
         (r = s->kpart.ensure(sizeof(double) * s->kpart_cap)) != PD_OK ||
-        cudaMallocHost(&s->maxd2_h, sizeof(unsigned long long) * max_slots) != cudaSuccess) {
+        cudaMallocHost(&s->flags_h, sizeof(unsigned int) * max_slots) != cudaSuccess ||
+        cudaMallocHost(&s->errs_h, sizeof(unsigned int) * max_slots) != cudaSuccess) {
         cudaGetLastError();
         pd_srv_destroy(s);
         set_error("pd_srv_create: allocation failed");
         return r != PD_OK ? r : PD_ENOMEM;
     }
     cudaMemset(s->hdr.p, 0, sizeof(BatchHdr));
-    if ((r = capture_graphs(s)) != PD_OK) {
+    cudaMemset(s->errs.p, 0, sizeof(unsigned int) * max_slots);
+    cudaMemset(s->flags.p, 0, sizeof(unsigned int) * max_slots);
+    cudaMemset(s->phase.p, 0, sizeof(unsigned int) * max_slots);
+    cudaMemset(s->work.p, 0, sizeof(RbWork));
+    cudaDeviceSynchronize();
+    if ((r = capture_graph(s)) != PD_OK) {
         pd_srv_destroy(s);
         return r;
     }
@@ -583,16 +1358,20 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
 int pd_srv_destroy(pd_srv s) {
     if (!s) return PD_EINVAL;
     if (s->st) cudaStreamSynchronize(s->st);
-    for (auto& kv : s->reqs) free_system(kv.second.get());
-    if (s->gA) cudaGraphExecDestroy(s->gA);
-    if (s->gB) cudaGraphExecDestroy(s->gB);
-    s->desc.release();
-    s->hdr.release();
-    s->maxd2.release();
-    s->tpart.release();
-    s->kpart.release();
-    if (s->maxd2_h) cudaFreeHost(s->maxd2_h);
+    if (s->pool) {
+        AllocScope scope(s->st, s->pool);
+        for (SrvSlot& sl : s->slots) sl.release();
+        cudaStreamSynchronize(s->st);
+    }
+    s->slots.clear();
+    if (s->gstep) cudaGraphExecDestroy(s->gstep);
+    Buf* bufs[] = {&s->desc, &s->hdr, &s->maxd2, &s->errs, &s->flags, &s->phase, &s->work, &s->nnmax, &s->tpart,
+                   &s->kpart};
+    for (Buf* b : bufs) b->release();
+    if (s->flags_h) cudaFreeHost(s->flags_h);
+    if (s->errs_h) cudaFreeHost(s->errs_h);
     if (s->st) cudaStreamDestroy(s->st);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return PD_OK;
 }
@@ -632,7 +1411,9 @@ int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const doub
 
 int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
     if (!s) return PD_EINVAL;
+    AllocScope scope(s->st, s->pool);  // slot memory: stream-ordered from the server's pool
     // admission (FIFO) by slot and memory
+    double ta = now_s(s);
     std::vector<char> used_slot(s->max_slots, 0);
     for (SrvReq* r : s->active) used_slot[r->slot] = 1;
     while (!s->queue.empty() && (int)s->active.size() < s->max_slots) {
@@ -646,7 +1427,6 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         s->used += r->bytes;
         int rc = admit_one(s, r, slot);
         if (rc != PD_OK) {
-            free_system(r);
             r->state = 3;
             s->used -= r->bytes;
             return rc;
@@ -655,61 +1435,50 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         s->active.push_back(r);
         s->dirty = true;
     }
+    s->ms[0] += 1e3 * (now_s(s) - ta);
     if (n_queued) *n_queued = (int)s->queue.size();
     if (s->active.empty()) {
         if (n_active) *n_active = 0;
         return PD_OK;
     }
     if (s->dirty) PD_TRY(upload_tables(s));
-    // kick-drift of every system, displacement per slot
-    PD_CUDA(cudaGraphLaunch(s->gA, s->st));
-    PD_CUDA(cudaMemcpyAsync(s->maxd2_h, s->maxd2.p, sizeof(unsigned long long) * s->max_slots,
-                            cudaMemcpyDeviceToHost, s->st));
+    // one velocity-Verlet step of every active system
+    double t_step = now_s(s);
+    PD_CUDA(cudaGraphLaunch(s->gstep, s->st));
     PD_CUDA(cudaStreamSynchronize(s->st));
-    double lim2 = 0.25 * s->skin * s->skin;
-    bool changed = false;
-    for (size_t k = 0; k < s->active.size(); ++k) {
-        SrvReq* r = s->active[k];
-        double d2;
-        memcpy(&d2, &s->maxd2_h[r->slot], sizeof(double));
-        int reb = (s->skin <= 0 || d2 > lim2) ? 1 : 0;
-        if (reb) {
-            PD_TRY(md_rebuild(r->md, s->st));
-            if (!r->md->tiles_active || r->md->tcap > SRV_CAP) {
-                set_error("serving: rebuilt system no longer fits the batched tile kernel");
-                return PD_EOVERFLOW;
-            }
-            s->rebuilds++;
-            changed = true;
-        }
-        if (s->hdesc[k].skip_replay != reb) changed = true;
-        s->hdesc[k].skip_replay = reb;
-    }
-    if (changed || s->dirty) PD_TRY(upload_tables(s));
-    PD_CUDA(cudaGraphLaunch(s->gB, s->st));
-    s->replays++;
-    __atomic_fetch_add(&g_launches, 5ull, __ATOMIC_RELAXED);  // kernels of the two graphs
-    PD_CUDA(cudaStreamSynchronize(s->st));
-    // retirement
+    s->steps_run++;
+    __atomic_fetch_add(&g_launches, (unsigned long long)GRAPH_KERNELS, __ATOMIC_RELAXED);
+    s->ms[2] += 1e3 * (now_s(s) - t_step);
+    // rebuild flags, errors and retirement
+    double t_ret = now_s(s);
     std::vector<SrvReq*> keep;
     for (SrvReq* r : s->active) {
-        r->md->steps++;
-        s->particle_steps += r->n;
-        if (r->md->steps >= r->steps) {
-            PD_TRY(retire(s, r));
+        SrvSlot& sl = s->slots[r->slot];
+        const unsigned int fl = s->flags_h[r->slot], er = s->errs_h[r->slot];
+        if (fl && !r->first) {
+            s->rebuilds++;
+            sl.md->builds++;
+        }
+        if (r->first) {
+            r->first = false;  // that graph ran the first build and forces only
+        } else {
+            r->done_steps++;
+            sl.md->steps++;
+            s->particle_steps += r->n;
+        }
+        if (er & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW | ERR_TILE_CAP | ERR_TIMEOUT | ERR_CELL_RANGE)) {
+            set_error("serving: system %ld failed in a batched step (err=0x%x)", r->ticket, er);
+            PD_TRY(retire(s, r, true));
+            s->dirty = true;
+        } else if (r->done_steps >= r->steps) {
+            PD_TRY(retire(s, r, false));
             s->dirty = true;
         } else {
             keep.push_back(r);
         }
     }
-    if (keep.size() != s->active.size()) {
-        // keep the replay flags aligned with the surviving systems
-        std::vector<SysDesc> nd;
-        for (size_t k = 0; k < s->active.size(); ++k)
-            if (s->active[k]->state == 1) nd.push_back(s->hdesc[k]);
-        s->hdesc = nd;
-    }
     s->active.swap(keep);
+    s->ms[3] += 1e3 * (now_s(s) - t_ret);
     if (n_active) *n_active = (int)s->active.size();
     return PD_OK;
 }
@@ -750,9 +1519,15 @@ int pd_srv_stats(pd_srv s, long* particle_steps, long* systems_done, long* ticks
     if (!s) return PD_EINVAL;
     if (particle_steps) *particle_steps = s->particle_steps;
     if (systems_done) *systems_done = s->systems_done;
-    if (ticks) *ticks = s->replays;
+    if (ticks) *ticks = s->steps_run;
     if (rebuilds) *rebuilds = s->rebuilds;
     if (tune_ms) *tune_ms = s->tune_ms;
+    return PD_OK;
+}
+
+int pd_srv_timers(pd_srv s, double ms[4]) {
+    if (!s || !ms) return PD_EINVAL;
+    for (int i = 0; i < 4; ++i) ms[i] = s->ms[i];
     return PD_OK;
 }
 

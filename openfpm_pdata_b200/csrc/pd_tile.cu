@@ -19,90 +19,11 @@
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
 #include "pd_tile.cuh"
+#include "pd_tile_dev.cuh"
 
 #include <cmath>
 
 namespace pd {
-
-// Rows hold two 16-bit entries per 32-bit word: entries 2w and 2w+1 of particle
-// i share word w*stride + i (column-major over words).
-__device__ __forceinline__ long pair_slot(int k, long stride, unsigned int i) {
-    return (((long)(k >> 1) * stride + i) << 1) | (k & 1);
-}
-
-struct TileSh {
-    unsigned int cR[9][TXMAX + 3];
-    unsigned int cI[9][TXMAX + 3];
-    unsigned int oR[9], oI[9];
-    unsigned int total;
-    int ncol;
-    unsigned long long bar;
-};
-
-__device__ __forceinline__ void tile_layout(const TileGeom& tg, long t, const unsigned int* __restrict__ csR,
-                                            const unsigned int* __restrict__ csI, TileSh& S) {
-    int tx = (int)(t % tg.ntx);
-    long rest = t / tg.ntx;
-    int y = (int)(rest % tg.ny) + tg.pad;
-    int z = (int)(rest / tg.ny) + tg.pad;
-    int x0 = tg.pad + tx * tg.TX;
-    int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
-    int ncol = x1 - x0 + 3;
-    for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
-        int img = e >= 9 * ncol;
-        int ee = img ? e - 9 * ncol : e;
-        int r = ee / ncol, j = ee % ncol;
-        int dz = r / 3 - 1, dy = r % 3 - 1;
-        long c = (long)(x0 - 1 + j) + (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
-        if (img) S.cI[r][j] = csI[c];
-        else S.cR[r][j] = csR[c];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int off = 0;
-        for (int r = 0; r < 9; ++r) {
-            S.oR[r] = off;
-            off += S.cR[r][ncol - 1] - S.cR[r][0];
-            S.oI[r] = off;
-            off += S.cI[r][ncol - 1] - S.cI[r][0];
-        }
-        S.total = off;
-        S.ncol = ncol;
-    }
-    __syncthreads();
-}
-
-// Stage the tile's 18 ranges; false (uniformly) if the tile does not fit or the
-// bounded wait gave up (error bit set).
-template <class T>
-__device__ __forceinline__ bool tile_stage(const typename V4<T>::type* __restrict__ preal,
-                                           const typename V4<T>::type* __restrict__ pimg, TileSh& S,
-                                           typename V4<T>::type* sm, unsigned int cap, unsigned int* err) {
-    typedef typename V4<T>::type T4;
-    if (S.total > cap) {
-        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
-        return false;
-    }
-    if (S.total == 0) return true;
-    if (threadIdx.x == 0) mbar_init(&S.bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(T4));
-        const int nc = S.ncol - 1;
-        for (int r = 0; r < 9; ++r) {
-            unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-            if (lr) bulk_g2s(sm + S.oR[r], preal + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
-            unsigned int li = S.cI[r][nc] - S.cI[r][0];
-            if (li) bulk_g2s(sm + S.oI[r], pimg + S.cI[r][0], li * (unsigned int)sizeof(T4), &S.bar);
-        }
-    }
-    bool ok = mbar_wait_bounded(&S.bar, 0, 1u << 24);
-    if (!ok) {
-        atomicOr(err, ERR_TIMEOUT);
-        mbar_wait_bounded(&S.bar, 0, 1u << 24);  // let copies in flight land before the CTA exits
-    }
-    return __syncthreads_and(ok ? 1 : 0) != 0;
-}
 
 // largest staged neighbourhood and largest centre count over the tiles
 __global__ void k_tile_sizes(TileGeom tg, long ntiles, const unsigned int* __restrict__ csR,
@@ -144,19 +65,7 @@ __global__ void k_pos32(const typename V4<T>::type* __restrict__ pos, long n, fl
     }
 }
 
-// exact predicate for the rare candidates inside the FP32 uncertainty band
-template <class T>
-__device__ __noinline__ bool exact_in(const typename V4<T>::type* __restrict__ pos, unsigned int i, int q, T r2) {
-    typename V4<T>::type a = ld4(pos, (long)i), b = ld4(pos, (long)q);
-    return dist2(a.x - b.x, a.y - b.y, a.z - b.z) < r2;
-}
-
-// List build.  The candidates are staged as FP32 copies; d2 in FP32 decides
-// every pair farther than `band` from r^2 (|d2_f32 - d2_exact| < band by the
-// error bound computed on the host), the few inside the band are decided
-// exactly in the position type T from global memory -- so the rows equal the
-// exact predicate d2 < r^2.  Entries are stored a 32-bit word (two entries) at
-// a time.
+// List build: one CTA per tile (rows: tile_rows in pd_tile_dev.cuh).
 template <class T>
 __global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::type* __restrict__ pos,
                                                         const float4* __restrict__ pos32, long n_real,
@@ -169,51 +78,13 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::ty
     extern __shared__ __align__(128) unsigned char tile_raw[];
     float4* sm = reinterpret_cast<float4*>(tile_raw);
     __shared__ TileSh S;
-    __shared__ unsigned int segb[18][TXMAX + 3];  // absolute staging index of every cell start, per segment
+    __shared__ unsigned int segb[18][TXMAX + 3];
     tile_layout(tg, blockIdx.x, csR, csI, S);
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     if (ib == ie) return;
-    const int ncol = S.ncol;
-    for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
-        int sg = e / ncol, j = e % ncol, r = sg >> 1;
-        segb[sg][j] = (sg & 1) ? S.oI[r] + (S.cI[r][j] - S.cI[r][0]) : S.oR[r] + (S.cR[r][j] - S.cR[r][0]);
-    }
+    tile_segb(S, segb);
     if (!tile_stage<float>(pos32, pos32 + n_real, S, sm, cap, err)) return;  // (its barrier also covers segb)
-    const unsigned int self_base = S.oR[4] - S.cR[4][0];
-    for (unsigned int i = ib + threadIdx.x; i < ie; i += blockDim.x) {
-        const float4 xi = sm[self_base + i];
-        int j = 1;
-        while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
-        int cnt = 0;
-        unsigned int pend = 0;
-        unsigned int* out = nbr + i;
-#pragma unroll 1
-        for (int sg = 0; sg < 18; ++sg) {
-            const unsigned int qe = segb[sg][j + 2];
-#pragma unroll 4
-            for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
-                const float4 xq = sm[q];
-                const float d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
-                if (d2 < hi_thr) {
-                    if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
-                        if (cnt < max_nn) {
-                            if (cnt & 1) out[(long)(cnt >> 1) * stride] = pend | (q << 16);
-                            else pend = q;
-                        }
-                        cnt++;
-                    }
-                }
-            }
-        }
-        // odd rows end with the particle itself, which the pair kernel skips
-        if ((cnt & 1) && cnt < max_nn) out[(long)(cnt >> 1) * stride] = pend | ((self_base + i) << 16);
-        if (cnt > max_nn) {
-            atomicOr(err, ERR_NN_OVERFLOW);
-            atomicMax(nn_max, (unsigned int)cnt);
-            cnt = max_nn;
-        }
-        nn[i] = cnt;
-    }
+    tile_rows<T>(S, segb, sm, pos, r2, lo_thr, hi_thr, nbr, nn, stride, max_nn, err, nn_max);
 }
 
 // P threads per domain particle split its row (words w = sub, sub+P, ...; two
@@ -386,7 +257,7 @@ bool tile_fits(pd_vd h, unsigned int tmax) {
 
 // |d2_f32 - d2| for pairs near r: coordinates rounded to FP32 (relative 2^-24)
 // at magnitude <= X, differences and the 3-term sum rounded once more each.
-static double fp32_band(pd_vd h, double r) {
+double fp32_band(pd_vd h, double r) {
     double X = 0;
     for (int d = 0; d < 3; ++d)
         X = std::max(X, std::max(std::fabs(h->lo[d] - 2 * h->g[d]), std::fabs(h->hi[d] + 2 * h->g[d])));

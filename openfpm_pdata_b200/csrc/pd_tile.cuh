@@ -16,7 +16,9 @@ struct TileGeom {
 int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles);
 int tile_sizes(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                unsigned int& tmax, unsigned int& cmax, cudaStream_t st);
-bool tile_fits(pd_vd h, unsigned int tmax);  // FP64/FP32 staging of the pair kernel fits
+bool tile_fits(pd_vd h, unsigned int tmax);
+// bound on |d2_f32 - d2| for pairs near r in the vector's box (FP32 prefilter band of the build)
+double fp32_band(pd_vd h, double r);  // FP64/FP32 staging of the pair kernel fits
 int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                unsigned int cap, double r_list, Buf& pos32, Buf& nbr, Buf& nn, long& stride, int& max_nn,
                cudaStream_t st);

@@ -142,6 +142,7 @@ def lib():
             "pd_srv_stats": ([vp, P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long),
                               P(ctypes.c_double)], ip),
             "pd_srv_tuned": ([vp, vp, vp, ip, P(ctypes.c_int)], ip),
+            "pd_srv_timers": ([vp, vp], ip),
             "pd_selftest_recip": ([ip, vp, vp, lp], ip),
             "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
@@ -521,6 +522,12 @@ class Server:
                                  ctypes.byref(tm)))
         return {"particle_steps": ps.value, "systems_done": sd.value, "ticks": tk.value, "rebuilds": rb.value,
                 "tune_ms": tm.value}
+
+    def timers(self):
+        """Host wall ms spent in admission (and its slot-reset part), batched steps and retirement."""
+        ms = np.zeros(4)
+        check(lib().pd_srv_timers(self.h, _ptr(ms)))
+        return dict(zip(("admit", "admit_reset", "step", "retire"), ms.tolist()))
 
     def tuned(self):
         b = np.zeros(64, np.int32)
