@@ -274,6 +274,7 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
     tm_cap = srv.timers()
     for t in tickets:
         srv.release(t)
+    srv.completed(1 << 20)  # drain: the Poisson phase polls its own tickets
     cap_ps = (st1["particle_steps"] - st0["particle_steps"]) / t_cap
     cap_sys = half / t_cap
     # (2) Poisson arrivals at 0.8 x capacity
@@ -296,7 +297,7 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
             continue
         srv.tick()
         now = time.perf_counter() - t0
-        for t in [t for t in live if srv.state(t) >= srv.DONE]:
+        for t in srv.completed():
             lat.append(now - live.pop(t))
             srv.release(t)
     t_run = time.perf_counter() - t0

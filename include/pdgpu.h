@@ -301,6 +301,9 @@ int pd_srv_release(pd_srv s, long ticket);
 int pd_srv_stats(pd_srv s, long* particle_steps, long* systems_done, long* ticks, long* rebuilds, double* tune_ms);
 /* autotuner table: size bucket (floor(log2 N)) -> tile width */
 int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int cap, int* n);
+/* tickets finished (done or failed) since the last call, oldest first, at most
+   `cap`; the rest stay for the next call */
+int pd_srv_completed(pd_srv s, long* tickets, int cap, int* n);
 /* host wall time (ms) spent in: admission, the slot reset part of admission, the
    batched step graphs (launch to completion), retirement */
 int pd_srv_timers(pd_srv s, double ms[4]);

@@ -204,6 +204,14 @@ int ghost_boxes_upload(pd_vd h, cudaStream_t st) {
     }
 }
 
+// domain ghost boxes and shift vectors of an FP64 vector into caller-owned host
+// memory (no copy); the caller uploads them to h->boxes / h->shifts
+int ghost_boxes_host(pd_vd h, BoxSet<double>* B, double* shifts27) {
+    if (h->dtype != PD_F64) return PD_EINVAL;
+    domain_boxes(h, *B, shifts27);
+    return PD_OK;
+}
+
 // count -> scan (total to the control block) -> write.  With sync_count the
 // total is read back and the capacity grown (the API path, like the reference's
 // D->H copy of the scan tail); without it `img_cap` bounds the write and an

@@ -20,4 +20,7 @@ template <class T> __device__ __forceinline__ bool inside_np(const BoxSet<T>& B,
              z >= B.hi[i][2]);
 }
 
+// host computation of the domain ghost boxes (pd_ghost.cu)
+int ghost_boxes_host(pd_vd h, BoxSet<double>* B, double* shifts27);
+
 }  // namespace pd

@@ -43,18 +43,22 @@ struct Kahan {
 };
 
 // One tile of the mixed-form LJ kernel, shared by the single-system kernel and
-// the batched persistent kernel of the serving loop.  The mbarrier `bar` is
+// the batched persistent kernels of the serving loop.  The mbarrier `bar` is
 // initialised by the caller; `uses` counts its completed phases (the parity of
-// the next wait).  Returns the thread's partial potential energy and virial.
+// the next wait).  Adds the thread's partial potential energy and virial to
+// pe / vir.  A tile whose staging exceeds `cap` sets ERR_TILE_CAP, or, with an
+// overflow list, is appended to it (item `ovf_item`) for a kernel with more
+// shared memory; the return value is then true (nothing computed).
 template <int P>
-__device__ __forceinline__ void mixed_tile(long tile, const float4* __restrict__ off, long n_real, const TileGeom& tg,
+__device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__ off, long n_real, const TileGeom& tg,
                                            const unsigned int* __restrict__ csR,
                                            const unsigned int* __restrict__ csI, unsigned int cap,
                                            const unsigned int* __restrict__ nbr, const int* __restrict__ nn,
                                            long stride, float sx, float sy, float sz, const LJP<float>& Pr,
                                            float* __restrict__ f, long fcap, unsigned int* __restrict__ err,
                                            float4* sm, TileShM& S, unsigned long long* bar, unsigned int& uses,
-                                           double& pe, double& vir) {
+                                           double& pe, double& vir, unsigned int* ovf_cnt = nullptr,
+                                           long* ovf_list = nullptr, long ovf_item = 0) {
     {
         long t = tile;
         int tx = (int)(t % tg.ntx);
@@ -90,7 +94,13 @@ __device__ __forceinline__ void mixed_tile(long tile, const float4* __restrict__
     const int ncol = S.ncol;
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][ncol - 2];
     bool ok = ib != ie && S.total <= cap;
-    if (ib != ie && S.total > cap && threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+    if (ib != ie && S.total > cap) {
+        if (ovf_cnt) {
+            if (threadIdx.x == 0) ovf_list[atomicAdd(ovf_cnt, 1u)] = ovf_item;
+            return true;
+        }
+        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+    }
     if (ok) {
         for (int e = threadIdx.x; e < 18 * ncol; e += blockDim.x) {
             int sg = e / ncol, j = e % ncol, r = sg >> 1;
@@ -192,6 +202,7 @@ __device__ __forceinline__ void mixed_tile(long tile, const float4* __restrict__
             }
         }
     }
+    return false;
 }
 
 }  // namespace pd

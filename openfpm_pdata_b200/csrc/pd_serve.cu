@@ -55,8 +55,12 @@
 namespace pd {
 
 static constexpr int SRV_P = 2;                       // lanes per particle in the batched force kernel
-static constexpr int SRV_SMEM = 96 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
+static constexpr int SRV_SMEM = 48 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
 static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged FP32 records per tile
+static constexpr int SRV_BSMEM = 32 * 1024;           // staging bytes per tile CTA of the batched list build
+static constexpr unsigned SRV_BCAP = SRV_BSMEM / 16;
+static constexpr int SRV_BIG = 192 * 1024;            // staging of the overflow kernels (tiles beyond SRV_CAP)
+static constexpr unsigned SRV_BIG_CAP = SRV_BIG / 16;
 static constexpr int CHUNK = 256;                     // threads per block of the chunked kernels
 static constexpr int SCH = 1024;                      // elements per scan chunk
 static constexpr int MAXS = 1024;                     // slots at most
@@ -130,7 +134,9 @@ struct BatchHdr {
     int nsys;
     int pad0;
     long tot_tiles, tot_chunks, tot_img;
-    unsigned int tile_ctr;
+    unsigned int tile_ctr;   // work queue of the force kernel
+    unsigned int ovf_force;  // tiles deferred to the large-staging kernels
+    unsigned int ovf_build;
     unsigned int pad1;
 };
 
@@ -313,7 +319,8 @@ __global__ void __launch_bounds__(CHUNK) k_b_replay(const SysDesc* __restrict__ 
 }
 
 __global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict__ D, BatchHdr* __restrict__ B,
-                                                      LJP<float> Pr, double* __restrict__ tpart) {
+                                                      LJP<float> Pr, double* __restrict__ tpart,
+                                                      long* __restrict__ ovf) {
     extern __shared__ __align__(128) unsigned char tile_raw[];
     float4* sm = reinterpret_cast<float4*>(tile_raw);
     __shared__ TileShM S;
@@ -335,8 +342,42 @@ __global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict_
         const int s = find_sys(D, nsys, g, 0);
         const SysDesc& d = D[s];
         double pe = 0, vir = 0;
-        mixed_tile<SRV_P>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_CAP, d.nbr, d.nn, d.tstride, d.sx,
-                          d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir);
+        if (mixed_tile<SRV_P>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_CAP, d.nbr, d.nn, d.tstride,
+                              d.sx, d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir, &B->ovf_force, ovf,
+                              g))
+            continue;  // deferred to k_b_force_ovf
+        pe = block_sum<double, FBLOCK_T>(pe);
+        vir = block_sum<double, FBLOCK_T>(vir);
+        if (threadIdx.x == 0) {
+            const long slot = d.tpart_base + (g - d.tile_base);
+            tpart[2 * slot] = pe;
+            tpart[2 * slot + 1] = vir;
+        }
+    }
+}
+
+// tiles whose staging exceeds SRV_CAP, with SRV_BIG of shared memory
+__global__ void __launch_bounds__(FBLOCK_T) k_b_force_ovf(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
+                                                          LJP<float> Pr, double* __restrict__ tpart,
+                                                          const long* __restrict__ ovf) {
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    float4* sm = reinterpret_cast<float4*>(tile_raw);
+    __shared__ TileShM S;
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    unsigned int uses = 0;
+    const int nsys = B->nsys;
+    const long tot = B->ovf_force;
+    for (long q = blockIdx.x; q < tot; q += gridDim.x) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        const long g = ovf[q];
+        const int s = find_sys(D, nsys, g, 0);
+        const SysDesc& d = D[s];
+        double pe = 0, vir = 0;
+        mixed_tile<SRV_P>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_BIG_CAP, d.nbr, d.nn, d.tstride,
+                          d.sx, d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir);
         pe = block_sum<double, FBLOCK_T>(pe);
         vir = block_sum<double, FBLOCK_T>(vir);
         if (threadIdx.x == 0) {
@@ -746,8 +787,12 @@ __global__ void __launch_bounds__(CHUNK) k_rb_image_k(const SysDesc* __restrict_
     RB_END
 }
 
-// tiled Verlet rows of the flagged systems (persistent CTAs, one mbarrier each)
+// tiled Verlet rows of the flagged systems (persistent CTAs, one mbarrier each).
+// BIG = 0: every flagged tile, those beyond SRV_BCAP appended to the overflow list;
+// BIG = 1: the overflow list, with SRV_BIG of shared memory.
+template <int BIG>
 __global__ void __launch_bounds__(TBLOCK) k_rb_build(const SysDesc* __restrict__ D, const RbWork* __restrict__ W,
+                                                     BatchHdr* __restrict__ B, long* __restrict__ ovf,
                                                      unsigned int* __restrict__ nn_max) {
     extern __shared__ __align__(128) unsigned char tile_raw[];
     float4* sm = reinterpret_cast<float4*>(tile_raw);
@@ -757,24 +802,35 @@ __global__ void __launch_bounds__(TBLOCK) k_rb_build(const SysDesc* __restrict__
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     unsigned int parity = 0;
-    RB_LOOP(K_T)
-    // generic-proxy reads of the previous tile are ordered before the next bulk copies
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    tile_layout(d.tg, c, d.csR, d.csI, S);
-    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
-    if (ib == ie) continue;
-    tile_segb(S, segb);
-    const int st = tile_stage_bar<float>(d.pos32, d.pos32 + d.n_real, S, sm, SRV_CAP, d.err, &bar, parity);
-    if (st > 0) parity ^= 1u;
-    if (st < 0) {
-        // the tile does not fit (error bit set; the next tile may), or the bounded
-        // wait gave up: its barrier phase cannot be tracked further, so stop
-        if (S.total <= SRV_CAP) break;
-        continue;
+    const unsigned int cap = BIG ? SRV_BIG_CAP : SRV_BCAP;
+    const long tot = BIG ? (long)B->ovf_build : W->tot[K_T];
+    for (long q = blockIdx.x; q < tot; q += gridDim.x) {
+        // generic-proxy reads of the previous tile are ordered before the next bulk copies
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        const long g = BIG ? ovf[q] : q;
+        const int k = find_flagged(W, K_T, g);
+        const SysDesc& d = D[W->sys[k]];
+        const long c = g - W->base[K_T][k];
+        tile_layout(d.tg, c, d.csR, d.csI, S);
+        const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+        if (ib == ie) continue;
+        if (!BIG && S.total > cap) {
+            if (threadIdx.x == 0) ovf[atomicAdd(&B->ovf_build, 1u)] = g;
+            continue;
+        }
+        tile_segb(S, segb);
+        const int st = tile_stage_bar<float>(d.pos32, d.pos32 + d.n_real, S, sm, cap, d.err, &bar, parity);
+        if (st > 0) parity ^= 1u;
+        if (st < 0) {
+            // the tile does not fit (error bit set; the next tile may), or the bounded
+            // wait gave up: its barrier phase cannot be tracked further, so stop
+            if (S.total <= cap) break;
+            continue;
+        }
+        tile_rows<double>(S, segb, sm, d.pos, d.r2, d.lo_thr, d.hi_thr, d.nbr, d.nn, d.tstride, d.max_nn, d.err,
+                          nn_max);
     }
-    tile_rows<double>(S, segb, sm, d.pos, d.r2, d.lo_thr, d.hi_thr, d.nbr, d.nn, d.tstride, d.max_nn, d.err, nn_max);
-    RB_END
 }
 
 __global__ void k_srv_iota(int* __restrict__ g, long n) {
@@ -829,18 +885,35 @@ struct pd_srv_s {
     std::map<long, std::unique_ptr<SrvReq>> reqs;
     std::deque<long> queue;
     std::vector<SrvReq*> active;
+    std::vector<std::pair<SrvReq*, bool>> finished;  // (system, failed), retired by the next tick
+    std::vector<long> completed;                      // tickets finished since the last poll
     std::vector<SrvSlot> slots;
     size_t used = 0;
     // device tables (fixed capacity: graph-invariant pointers)
-    Buf desc, hdr, maxd2, errs, flags, phase, work, nnmax, tpart, kpart;
+    Buf desc, hdr, maxd2, errs, flags, phase, work, nnmax, tpart, kpart, ovf_f, ovf_b;
     long tpart_cap = 0, kpart_cap = 0;
     std::vector<SysDesc> hdesc;
     BatchHdr hhdr;
     unsigned int* flags_h = nullptr;  // pinned: rebuild flag and error bits per slot after each step
     unsigned int* errs_h = nullptr;
-    cudaStream_t st = nullptr;
-    cudaMemPool_t pool = nullptr;  // device memory of the slots (stream-ordered on st)
-    cudaGraphExec_t gstep = nullptr;
+    cudaStream_t st = nullptr;     // step graphs
+    cudaStream_t as = nullptr;     // admission and retirement, overlapping the running step graph
+    cudaMemPool_t pool = nullptr;  // device memory of the slots (stream-ordered on `as`)
+    cudaEvent_t ev_adm = nullptr;  // end of the last admissions on `as`
+    // pinned staging: a ring for the admissions' uploads (a region is reused once
+    // the event recorded after its copies has completed) and a buffer for downloads
+    char* up = nullptr;
+    size_t up_bytes = 0, up_head = 0;
+    struct UpUse {
+        size_t lo, hi;
+        cudaEvent_t ev;
+    };
+    std::deque<UpUse> up_use;
+    std::vector<cudaEvent_t> ev_free;
+    char* down = nullptr;
+    size_t down_bytes = 0;
+    bool adm_pending = false;
+    cudaGraphExec_t gstep[4] = {nullptr, nullptr, nullptr, nullptr};  // 1, 2, 4, 8 steps per launch
     bool dirty = true;
     // autotuner: size bucket -> tile width
     bool autotune = true;
@@ -987,9 +1060,10 @@ static int upload_tables(pd_srv s) {
     return PD_OK;
 }
 
-static constexpr int GRAPH_KERNELS = 30;  // kernel nodes of the step graph
+static constexpr int GRAPH_KERNELS = 32;  // kernel nodes per step of the step graphs
 
-static int capture_graph(pd_srv s) {
+// the step graphs: 2^lk velocity-Verlet steps of every active system per launch
+static int capture_graph(pd_srv s, int lk) {
     float half = (float)(0.5 * s->dt / 1.0), dt = (float)s->dt;
     LJP<float> P;
     P.eps24 = (float)(24.0 * s->lj.eps);
@@ -998,12 +1072,14 @@ static int capture_graph(pd_srv s) {
     float rc = (float)s->lj.r_cut;
     P.rc2 = rc * rc;
     PD_CUDA(cudaFuncSetAttribute(k_b_force, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
-    PD_CUDA(cudaFuncSetAttribute(k_rb_build, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
+    PD_CUDA(cudaFuncSetAttribute(k_rb_build<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BSMEM));
+    PD_CUDA(cudaFuncSetAttribute(k_b_force_ovf, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
+    PD_CUDA(cudaFuncSetAttribute(k_rb_build<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
     int sms = 148, dev = 0, per = 1, perb = 1;
     PD_CUDA(cudaGetDevice(&dev));
     PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_force, FBLOCK_T, SRV_SMEM));
-    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_rb_build, TBLOCK, SRV_SMEM));
+    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_rb_build<0>, TBLOCK, SRV_BSMEM));
     const int gf = sms * std::max(per, 1), gb = sms * std::max(perb, 1), gc = sms * 8;
     const SysDesc* D = s->desc.as<SysDesc>();
     BatchHdr* B = s->hdr.as<BatchHdr>();
@@ -1016,8 +1092,9 @@ static int capture_graph(pd_srv s) {
     cudaGraph_t g = nullptr;
     cudaStream_t st = s->st;
     PD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int step = 0; step < (1 << lk); ++step) {
     cudaMemsetAsync(md2, 0, sizeof(unsigned long long) * M, st);
-    cudaMemsetAsync(&B->tile_ctr, 0, sizeof(unsigned int), st);
+    cudaMemsetAsync(&B->tile_ctr, 0, 3 * sizeof(unsigned int), st);  // tile_ctr, ovf_force, ovf_build
     unsigned int* ph = s->phase.as<unsigned int>();
     k_b_kick_drift<<<gc, CHUNK, 0, st>>>(D, B, half, dt, md2, ph);
     k_b_decide<<<1, 1024, 0, st>>>(D, B, md2, lim2, always, fl, ph, W);
@@ -1045,12 +1122,15 @@ static int capture_graph(pd_srv s) {
     k_rb_put_img<<<gc, CHUNK, 0, st>>>(D, W);
     k_rb_offsets<<<gc, CHUNK, 0, st>>>(D, W);
     k_rb_image_k<<<gc, CHUNK, 0, st>>>(D, W);
-    k_rb_build<<<gb, TBLOCK, SRV_SMEM, st>>>(D, W, s->nnmax.as<unsigned int>());
+    k_rb_build<0><<<gb, TBLOCK, SRV_BSMEM, st>>>(D, W, B, s->ovf_b.as<long>(), s->nnmax.as<unsigned int>());
+    k_rb_build<1><<<sms, TBLOCK, SRV_BIG, st>>>(D, W, B, s->ovf_b.as<long>(), s->nnmax.as<unsigned int>());
     // step of every system
     k_b_replay<<<gc, CHUNK, 0, st>>>(D, B, fl);
-    k_b_force<<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>());
+    k_b_force<<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force_ovf<<<sms, FBLOCK_T, SRV_BIG, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
     k_b_kick<<<gc, CHUNK, 0, st>>>(D, B, half, s->kpart.as<double>(), ph);
     k_b_energy<<<M, 256, 0, st>>>(D, B, s->tpart.as<double>(), s->kpart.as<double>(), fl, ph);
+    }
     cudaMemcpyAsync(s->flags_h, fl, sizeof(unsigned int) * M, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(s->errs_h, s->errs.p, sizeof(unsigned int) * M, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamEndCapture(st, &g);
@@ -1058,12 +1138,34 @@ static int capture_graph(pd_srv s) {
         set_error("serving: graph capture failed: %s", cudaGetErrorString(ce));
         return PD_ECUDA;
     }
-    ce = cudaGraphInstantiate(&s->gstep, g, 0);
+    ce = cudaGraphInstantiate(&s->gstep[lk], g, 0);
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) {
         set_error("serving: graph instantiation failed: %s", cudaGetErrorString(ce));
         return PD_ECUDA;
     }
+    return PD_OK;
+}
+
+// grow a slot vector's particle capacity without keeping its contents (a new
+// system is loaded next): stream-ordered frees and allocations, no host wait
+static int slot_capacity(pd_vd h, long need) {
+    if (need <= h->cap) return PD_OK;
+    long ncap = need + need / 4 + 1024;
+    dev_free(h->pos);
+    dev_free(h->gid);
+    h->pos = nullptr;
+    h->gid = nullptr;
+    for (Prop& P : h->props) {
+        dev_free(P.d);
+        P.d = nullptr;
+    }
+    h->cap = 0;
+    PD_CUDA(dev_alloc(&h->pos, (size_t)ncap * h->pos_bytes));
+    PD_CUDA(dev_alloc((void**)&h->gid, sizeof(int) * ncap));
+    for (Prop& P : h->props) PD_CUDA(dev_alloc((void**)&P.d, (size_t)P.esize * P.ncomp * ncap));
+    h->cap = ncap;
+    h->epoch++;
     return PD_OK;
 }
 
@@ -1095,7 +1197,7 @@ static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
         }
         h->nbox = 0;  // the ghost boxes of the new box are uploaded by the first build
         h->n_img = 0;
-        PD_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), s->st));
+        PD_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), s->as));
         memset(h->ctrl_h, 0, sizeof(Ctrl));
         PD_TRY(cl_geometry(md->vl->cl, h, rl, 1.013, 1));
         md->ready = false;
@@ -1115,11 +1217,11 @@ static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
     sl.img_cap = (long)(1.3 * image_estimate(r->n, r->L, rl)) + 2048;
     pd_vd h = sl.h;
     pd_md md = sl.md;
-    PD_TRY(ensure_capacity(h, r->n + sl.img_cap + 1, s->st));
+    PD_TRY(slot_capacity(h, r->n + sl.img_cap + 1));
     h->n_real = h->n_total = r->n;
     h->img_valid = false;
     h->epoch++;
-    pd::launch(k_srv_iota, grid_for(r->n, CHUNK), CHUNK, 0, s->st, h->gid, r->n);
+    pd::launch(k_srv_iota, grid_for(r->n, CHUNK), CHUNK, 0, s->as, h->gid, r->n);
     PD_LAUNCH_CHECK();
     PD_TRY(md->off.ensure(sizeof(float4) * (size_t)h->cap));
     PD_TRY(md->offK.ensure(sizeof(float4) * (size_t)sl.img_cap));
@@ -1151,18 +1253,84 @@ static int slot_scratch(pd_srv s, SrvSlot& sl, SrvReq* r) {
     PD_TRY(h->img_start.ensure(sizeof(unsigned int) * (n + 1)));
     PD_TRY(sl.Edev.ensure(sizeof(double) * 4 * (r->steps > 0 ? r->steps : 1)));
     PD_TRY(sl.step.ensure(sizeof(int)));
-    PD_CUDA(cudaMemsetAsync(sl.step.p, 0, sizeof(int), s->st));
-    PD_CUDA(cudaMemsetAsync(s->errs.as<unsigned int>() + r->slot, 0, sizeof(unsigned int), s->st));
+    PD_CUDA(cudaMemsetAsync(sl.step.p, 0, sizeof(int), s->as));
+    PD_CUDA(cudaMemsetAsync(s->errs.as<unsigned int>() + r->slot, 0, sizeof(unsigned int), s->as));
     return PD_OK;
 }
 
+// a region of `need` bytes of the upload ring, after the copies that last used it
+static char* ring_take(pd_srv s, size_t need, size_t& lo_out) {
+    need = (need + 255) & ~(size_t)255;
+    if (need > s->up_bytes) return nullptr;
+    if (s->up_head + need > s->up_bytes) s->up_head = 0;
+    const size_t lo = s->up_head, hi = lo + need;
+    for (auto it = s->up_use.begin(); it != s->up_use.end();) {
+        const bool overlap = it->lo < hi && lo < it->hi;
+        if (overlap || cudaEventQuery(it->ev) == cudaSuccess) {
+            if (overlap) cudaEventSynchronize(it->ev);
+            s->ev_free.push_back(it->ev);
+            it = s->up_use.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    cudaGetLastError();  // a query of an unfinished event reports cudaErrorNotReady
+    s->up_head = hi;
+    lo_out = lo;
+    return s->up + lo;
+}
+
+static int ring_mark(pd_srv s, size_t lo, size_t need) {
+    need = (need + 255) & ~(size_t)255;
+    cudaEvent_t ev = nullptr;
+    if (!s->ev_free.empty()) {
+        ev = s->ev_free.back();
+        s->ev_free.pop_back();
+    } else {
+        PD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    PD_CUDA(cudaEventRecord(ev, s->as));
+    s->up_use.push_back({lo, lo + need, ev});
+    return PD_OK;
+}
+
+// staging layout: ghost boxes, shift vectors, position records, velocities
+static size_t stage_off_shifts() { return (sizeof(BoxSet<double>) + 63) & ~(size_t)63; }
+static size_t stage_off_pos() { return (stage_off_shifts() + 81 * sizeof(double) + 63) & ~(size_t)63; }
+
+// upload the submitted state and the ghost boxes of the box, stream-ordered on the
+// admission stream from the pinned upload ring (the host does not wait)
 static int load_state(pd_srv s, SrvSlot& sl, SrvReq* r) {
-    PD_TRY(pd_h2d_pos(sl.h, r->x.data(), 0, r->n, s->st));
-    std::vector<float> vc(3 * r->n);
-    for (long i = 0; i < r->n; ++i)
-        for (int d = 0; d < 3; ++d) vc[(size_t)d * r->n + i] = (float)r->v[3 * i + d];
-    PD_TRY(pd_h2d_prop(sl.h, sl.vp, vc.data(), 0, r->n, s->st));
-    PD_CUDA(cudaStreamSynchronize(s->st));  // vc is a local (pageable copies may still be staged)
+    pd_vd h = sl.h;
+    const long n = r->n;
+    const size_t opos = stage_off_pos(), ov = opos + sizeof(double4) * n;
+    const size_t need = ov + sizeof(float) * 3 * n;
+    size_t lo = 0;
+    char* st = ring_take(s, need, lo);
+    std::vector<char> tmp;
+    if (!st) {  // larger than the ring: pageable staging, waited for below
+        tmp.resize(need);
+        st = tmp.data();
+    }
+    BoxSet<double>* B = reinterpret_cast<BoxSet<double>*>(st);
+    double* sh = reinterpret_cast<double*>(st + stage_off_shifts());
+    PD_TRY(ghost_boxes_host(h, B, sh));
+    PD_TRY(h->boxes.ensure(sizeof(BoxSet<double>)));
+    PD_TRY(h->shifts.ensure(sizeof(double) * 81));
+    PD_CUDA(cudaMemcpyAsync(h->boxes.p, B, sizeof(BoxSet<double>), cudaMemcpyHostToDevice, s->as));
+    PD_CUDA(cudaMemcpyAsync(h->shifts.p, sh, sizeof(double) * 81, cudaMemcpyHostToDevice, s->as));
+    h->nbox = B->nb;
+    double4* P = reinterpret_cast<double4*>(st + opos);
+    for (long i = 0; i < n; ++i) P[i] = make_double4(r->x[3 * i], r->x[3 * i + 1], r->x[3 * i + 2], 0.0);
+    PD_CUDA(cudaMemcpyAsync(h->pos, P, sizeof(double4) * n, cudaMemcpyHostToDevice, s->as));
+    float* V = reinterpret_cast<float*>(st + ov);
+    for (int d = 0; d < 3; ++d) {
+        for (long i = 0; i < n; ++i) V[(size_t)d * n + i] = (float)r->v[3 * i + d];
+        PD_CUDA(cudaMemcpyAsync(h->props[sl.vp].d + (size_t)d * h->cap * sizeof(float), V + (size_t)d * n,
+                                sizeof(float) * n, cudaMemcpyHostToDevice, s->as));
+    }
+    if (tmp.empty()) return ring_mark(s, lo, need);
+    PD_CUDA(cudaStreamSynchronize(s->as));
     return PD_OK;
 }
 
@@ -1171,18 +1339,18 @@ static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r);
 // time the single-system force for candidate tile widths on a throw-away copy of
 // the system (so the admitted system starts from the submitted state); keep the fastest
 static int autotune_tx(pd_srv s, SrvReq* r) {
-    AllocScope scope(s->st, s->pool);
+    AllocScope scope(s->as, s->pool);
     SrvSlot tmp;
     int rc = slot_reset(s, tmp, r, 0);
     if (rc == PD_OK) rc = load_state(s, tmp, r);
     if (rc == PD_OK) rc = autotune_tx_on(s, tmp, r);
-    cudaStreamSynchronize(s->st);
+    cudaStreamSynchronize(s->as);
     tmp.release();
     return rc;
 }
 
 static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
-    static const int cand[] = {3, 5, 7, 9, 12};
+    static const int cand[] = {5, 7, 9, 12};
     cudaEvent_t a, b;
     PD_CUDA(cudaEventCreate(&a));
     PD_CUDA(cudaEventCreate(&b));
@@ -1191,12 +1359,12 @@ static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
     double t0 = now_s(s);
     for (int tx : cand) {
         sl.md->tile_tx = tx;
-        int rc = md_rebuild(sl.md, s->st);
-        if (rc != PD_OK || !sl.md->tiles_active || sl.md->tcap > SRV_CAP) continue;
-        PD_TRY(md_forces(sl.md, s->st));  // warm
-        PD_CUDA(cudaEventRecord(a, s->st));
-        for (int k = 0; k < 3; ++k) PD_TRY(md_forces(sl.md, s->st));
-        PD_CUDA(cudaEventRecord(b, s->st));
+        int rc = md_rebuild(sl.md, s->as);
+        if (rc != PD_OK || !sl.md->tiles_active || sl.md->tcap > SRV_BIG_CAP) continue;
+        PD_TRY(md_forces(sl.md, s->as));  // warm
+        PD_CUDA(cudaEventRecord(a, s->as));
+        for (int k = 0; k < 3; ++k) PD_TRY(md_forces(sl.md, s->as));
+        PD_CUDA(cudaEventRecord(b, s->as));
         PD_CUDA(cudaEventSynchronize(b));
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
@@ -1227,11 +1395,9 @@ static int admit_one(pd_srv s, SrvReq* r, int slot) {
     const double t0 = now_s(s);
     PD_TRY(slot_reset(s, sl, r, s->autotune ? s->tuned[r->bucket] : s->fixed_tx));
     s->ms[1] += 1e3 * (now_s(s) - t0);
-    pd_vd h = sl.h;
     pd_md md = sl.md;
     pd_cl cl = md->vl->cl;
     const long n = r->n;
-    PD_TRY(ghost_boxes_upload(h, s->st));
     PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
     // row capacity of the tiled build (tile_build's first estimate)
     md->tstride = std::max(32L, ((n + 31) / 32) * 32);
@@ -1249,7 +1415,7 @@ static int admit_one(pd_srv s, SrvReq* r, int slot) {
     md->ready = true;
     PD_TRY(slot_scratch(s, sl, r));
     PD_TRY(load_state(s, sl, r));
-    PD_CUDA(cudaMemsetAsync(s->phase.as<unsigned int>() + slot, 0, sizeof(unsigned int), s->st));
+    PD_CUDA(cudaMemsetAsync(s->phase.as<unsigned int>() + slot, 0, sizeof(unsigned int), s->as));
     r->x.clear();
     r->x.shrink_to_fit();
     r->v.clear();
@@ -1261,27 +1427,74 @@ static int admit_one(pd_srv s, SrvReq* r, int slot) {
     return PD_OK;
 }
 
-static int retire(pd_srv s, SrvReq* r, bool failed) {
-    SrvSlot& sl = s->slots[r->slot];
-    pd_vd h = sl.h;
-    if (!failed) {
-        PD_TRY(mixed_to_positions(h, sl.md->vl->cl, sl.md->off, s->st));
-        std::vector<double> xs(3 * r->n);
-        std::vector<int> gid(r->n);
-        PD_TRY(pd_d2h_pos(h, xs.data(), 0, r->n, s->st));
-        PD_CUDA(cudaMemcpyAsync(gid.data(), h->gid, sizeof(int) * r->n, cudaMemcpyDeviceToHost, s->st));
-        r->E.assign(4 * (size_t)r->steps, 0.0);
-        PD_CUDA(cudaMemcpyAsync(r->E.data(), sl.Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost,
-                                s->st));
-        PD_CUDA(cudaStreamSynchronize(s->st));
-        r->xo.assign(3 * r->n, 0.0);
-        for (long i = 0; i < r->n; ++i)
-            for (int d = 0; d < 3; ++d) r->xo[3 * (size_t)gid[i] + d] = xs[3 * i + d];
+// retire the finished systems: final positions (offsets -> FP64), ids and
+// energies to the slots' pinned staging, one wait, results reordered by id
+static int retire_all(pd_srv s, std::vector<std::pair<SrvReq*, bool>>& fin) {
+    // download layout per system: position records, ids, energies (64-byte aligned)
+    std::vector<size_t> off(fin.size(), 0);
+    size_t need = 0;
+    for (size_t k = 0; k < fin.size(); ++k) {
+        if (fin[k].second) continue;
+        const long n = fin[k].first->n;
+        off[k] = need;
+        need += (sizeof(double4) * n + sizeof(int) * n + sizeof(double) * 4 * fin[k].first->steps + 192) &
+                ~(size_t)63;
     }
-    r->state = failed ? 3 : 2;
-    r->t_done = now_s(s);
-    s->used -= r->bytes;
-    s->systems_done++;
+    if (need > s->down_bytes) {
+        if (s->down) cudaFreeHost(s->down);
+        s->down = nullptr;
+        s->down_bytes = 0;
+        const size_t b = need + need / 2;
+        if (cudaMallocHost((void**)&s->down, b) != cudaSuccess) {
+            cudaGetLastError();
+            s->down = nullptr;
+            set_error("serving: pinned download buffer of %zu bytes failed", b);
+            return PD_ENOMEM;
+        }
+        s->down_bytes = b;
+    }
+    bool any = false;
+    for (size_t k = 0; k < fin.size(); ++k) {
+        if (fin[k].second) continue;
+        SrvReq* r = fin[k].first;
+        SrvSlot& sl = s->slots[r->slot];
+        pd_vd h = sl.h;
+        const long n = r->n;
+        PD_TRY(mixed_to_positions(h, sl.md->vl->cl, sl.md->off, s->as));
+        char* st = s->down + off[k];
+        const size_t og = sizeof(double4) * n, oe = (og + sizeof(int) * n + 63) & ~(size_t)63;
+        PD_CUDA(cudaMemcpyAsync(st, h->pos, og, cudaMemcpyDeviceToHost, s->as));
+        PD_CUDA(cudaMemcpyAsync(st + og, h->gid, sizeof(int) * n, cudaMemcpyDeviceToHost, s->as));
+        PD_CUDA(cudaMemcpyAsync(st + oe, sl.Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost, s->as));
+        any = true;
+    }
+    if (any) PD_CUDA(cudaStreamSynchronize(s->as));
+    for (size_t k = 0; k < fin.size(); ++k) {
+        SrvReq* r = fin[k].first;
+        if (!fin[k].second) {
+            const long n = r->n;
+            const char* st = s->down + off[k];
+            const size_t og = sizeof(double4) * n, oe = (og + sizeof(int) * n + 63) & ~(size_t)63;
+            const double4* P = reinterpret_cast<const double4*>(st);
+            const int* gid = reinterpret_cast<const int*>(st + og);
+            const double* E = reinterpret_cast<const double*>(st + oe);
+            r->xo.assign(3 * (size_t)n, 0.0);
+            for (long i = 0; i < n; ++i) {
+                const size_t g = (size_t)gid[i];
+                r->xo[3 * g] = P[i].x;
+                r->xo[3 * g + 1] = P[i].y;
+                r->xo[3 * g + 2] = P[i].z;
+            }
+            r->E.assign(E, E + 4 * (size_t)r->steps);
+            for (int k = 0; k < r->steps; ++k) s->rebuilds += E[4 * k + 3] != 0.0 ? 1 : 0;
+        }
+        r->state = fin[k].second ? 3 : 2;
+        r->t_done = now_s(s);
+        s->used -= r->bytes;
+        s->systems_done++;
+        s->completed.push_back(r->ticket);
+    }
+    fin.clear();
     return PD_OK;
 }
 
@@ -1326,6 +1539,8 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
         cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->as, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_adm, cudaEventDisableTiming) != cudaSuccess ||
         (r = s->desc.ensure(sizeof(SysDesc) * max_slots)) != PD_OK || (r = s->hdr.ensure(sizeof(BatchHdr))) != PD_OK ||
         (r = s->maxd2.ensure(sizeof(unsigned long long) * max_slots)) != PD_OK ||
         (r = s->errs.ensure(sizeof(unsigned int) * max_slots)) != PD_OK ||
@@ -1334,7 +1549,13 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
         (r = s->work.ensure(sizeof(RbWork))) != PD_OK || (r = s->nnmax.ensure(sizeof(unsigned int))) != PD_OK ||
         (r = s->tpart.ensure(sizeof(double) * 2 * s->tpart_cap)) != PD_OK ||
         (r = s->kpart.ensure(sizeof(double) * s->kpart_cap)) != PD_OK ||
+        (r = s->ovf_f.ensure(sizeof(long) * s->tpart_cap)) != PD_OK ||
+        (r = s->ovf_b.ensure(sizeof(long) * s->tpart_cap)) != PD_OK ||
         cudaMallocHost(&s->flags_h, sizeof(unsigned int) * max_slots) != cudaSuccess ||
+        cudaMallocHost((void**)&s->up, (s->up_bytes = std::min((size_t)256 << 20,
+                                                               std::max((size_t)32 << 20,
+                                                                        (size_t)hbm_budget_bytes / 64)))) !=
+            cudaSuccess ||
         cudaMallocHost(&s->errs_h, sizeof(unsigned int) * max_slots) != cudaSuccess) {
         cudaGetLastError();
         pd_srv_destroy(s);
@@ -1347,7 +1568,21 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
     cudaMemset(s->phase.p, 0, sizeof(unsigned int) * max_slots);
     cudaMemset(s->work.p, 0, sizeof(RbWork));
     cudaDeviceSynchronize();
-    if ((r = capture_graph(s)) != PD_OK) {
+    {
+        // reserve the budget in the pool once (one physical allocation instead of
+        // one per slot buffer; the pool keeps freed memory)
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        size_t want = std::min((size_t)hbm_budget_bytes, fr > ((size_t)2 << 30) ? fr - ((size_t)2 << 30) : 0);
+        void* p = nullptr;
+        if (want > 0 && cudaMallocFromPoolAsync(&p, want, s->pool, s->as) == cudaSuccess) {
+            cudaFreeAsync(p, s->as);
+            cudaStreamSynchronize(s->as);
+        }
+        cudaGetLastError();
+    }
+    for (int lk = 0; lk < 4 && r == PD_OK; ++lk) r = capture_graph(s, lk);
+    if (r != PD_OK) {
         pd_srv_destroy(s);
         return r;
     }
@@ -1358,19 +1593,27 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
 int pd_srv_destroy(pd_srv s) {
     if (!s) return PD_EINVAL;
     if (s->st) cudaStreamSynchronize(s->st);
-    if (s->pool) {
-        AllocScope scope(s->st, s->pool);
+    if (s->as) cudaStreamSynchronize(s->as);
+    if (s->pool && s->as) {
+        AllocScope scope(s->as, s->pool);
         for (SrvSlot& sl : s->slots) sl.release();
-        cudaStreamSynchronize(s->st);
+        cudaStreamSynchronize(s->as);
     }
+    for (auto& u : s->up_use) cudaEventDestroy(u.ev);
+    for (cudaEvent_t e : s->ev_free) cudaEventDestroy(e);
+    if (s->up) cudaFreeHost(s->up);
+    if (s->down) cudaFreeHost(s->down);
     s->slots.clear();
-    if (s->gstep) cudaGraphExecDestroy(s->gstep);
-    Buf* bufs[] = {&s->desc, &s->hdr, &s->maxd2, &s->errs, &s->flags, &s->phase, &s->work, &s->nnmax, &s->tpart,
-                   &s->kpart};
+    for (auto& ge : s->gstep)
+        if (ge) cudaGraphExecDestroy(ge);
+    Buf* bufs[] = {&s->desc, &s->hdr,   &s->maxd2, &s->errs, &s->flags, &s->phase,
+                   &s->work, &s->nnmax, &s->tpart, &s->kpart, &s->ovf_f, &s->ovf_b};
     for (Buf* b : bufs) b->release();
     if (s->flags_h) cudaFreeHost(s->flags_h);
     if (s->errs_h) cudaFreeHost(s->errs_h);
     if (s->st) cudaStreamDestroy(s->st);
+    if (s->as) cudaStreamDestroy(s->as);
+    if (s->ev_adm) cudaEventDestroy(s->ev_adm);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return PD_OK;
@@ -1411,15 +1654,37 @@ int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const doub
 
 int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
     if (!s) return PD_EINVAL;
-    AllocScope scope(s->st, s->pool);  // slot memory: stream-ordered from the server's pool
-    // admission (FIFO) by slot and memory
+    AllocScope scope(s->as, s->pool);  // slot memory: stream-ordered from the server's pool
+    // systems that finished in the previous step (the GPU is idle here)
+    double t_ret = now_s(s);
+    PD_TRY(retire_all(s, s->finished));
+    s->ms[3] += 1e3 * (now_s(s) - t_ret);
+    if (s->adm_pending) {
+        PD_CUDA(cudaStreamWaitEvent(s->st, s->ev_adm, 0));  // admissions before the step that builds them
+        s->adm_pending = false;
+    }
+    if (s->dirty && !s->active.empty()) PD_TRY(upload_tables(s));
+    // one velocity-Verlet step of every active system; admissions are prepared
+    // meanwhile on the admission stream (host work and asynchronous copies only)
+    const bool stepping = !s->active.empty();
+    // steps in this launch: up to 8, none past a system's last step, at most 2
+    // while requests wait for a slot (they are admitted between launches)
+    int K = 8;
+    for (SrvReq* r : s->active) K = std::min(K, r->steps - r->done_steps + (r->first ? 1 : 0));
+    if (!s->queue.empty()) K = std::min(K, 2);
+    int lk = 0;
+    while (lk < 3 && (2 << lk) <= K) ++lk;
+    K = 1 << lk;
+    double t_step = now_s(s);
+    if (stepping) PD_CUDA(cudaGraphLaunch(s->gstep[lk], s->st));
     double ta = now_s(s);
     std::vector<char> used_slot(s->max_slots, 0);
     for (SrvReq* r : s->active) used_slot[r->slot] = 1;
-    while (!s->queue.empty() && (int)s->active.size() < s->max_slots) {
+    std::vector<SrvReq*> admitted;
+    size_t fr = 0, tot = 0;
+    if (!s->queue.empty()) PD_CUDA(cudaMemGetInfo(&fr, &tot));
+    while (!s->queue.empty() && (int)(s->active.size() + admitted.size()) < s->max_slots) {
         SrvReq* r = s->reqs[s->queue.front()].get();
-        size_t fr = 0, tot = 0;
-        PD_CUDA(cudaMemGetInfo(&fr, &tot));
         if (s->used + r->bytes > (size_t)s->budget || r->bytes + (256ul << 20) > fr) break;
         int slot = 0;
         while (used_slot[slot]) ++slot;
@@ -1429,57 +1694,66 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         if (rc != PD_OK) {
             r->state = 3;
             s->used -= r->bytes;
+            cudaStreamSynchronize(s->st);
+            cudaStreamSynchronize(s->as);
             return rc;
         }
+        fr = fr > r->bytes ? fr - r->bytes : 0;
         used_slot[slot] = 1;
-        s->active.push_back(r);
-        s->dirty = true;
+        admitted.push_back(r);
+    }
+    if (!admitted.empty()) {
+        PD_CUDA(cudaEventRecord(s->ev_adm, s->as));
+        s->adm_pending = true;
     }
     s->ms[0] += 1e3 * (now_s(s) - ta);
-    if (n_queued) *n_queued = (int)s->queue.size();
-    if (s->active.empty()) {
-        if (n_active) *n_active = 0;
-        return PD_OK;
+    if (stepping) {
+        PD_CUDA(cudaStreamSynchronize(s->st));
+        s->steps_run += K;
+        __atomic_fetch_add(&g_launches, (unsigned long long)(GRAPH_KERNELS * K), __ATOMIC_RELAXED);
+        s->ms[2] += 1e3 * (now_s(s) - t_step);
     }
-    if (s->dirty) PD_TRY(upload_tables(s));
-    // one velocity-Verlet step of every active system
-    double t_step = now_s(s);
-    PD_CUDA(cudaGraphLaunch(s->gstep, s->st));
-    PD_CUDA(cudaStreamSynchronize(s->st));
-    s->steps_run++;
-    __atomic_fetch_add(&g_launches, (unsigned long long)GRAPH_KERNELS, __ATOMIC_RELAXED);
-    s->ms[2] += 1e3 * (now_s(s) - t_step);
-    // rebuild flags, errors and retirement
-    double t_ret = now_s(s);
+    // rebuild flags and errors of the step; finished systems are retired by the next tick
     std::vector<SrvReq*> keep;
     for (SrvReq* r : s->active) {
         SrvSlot& sl = s->slots[r->slot];
-        const unsigned int fl = s->flags_h[r->slot], er = s->errs_h[r->slot];
-        if (fl && !r->first) {
-            s->rebuilds++;
-            sl.md->builds++;
-        }
-        if (r->first) {
-            r->first = false;  // that graph ran the first build and forces only
-        } else {
-            r->done_steps++;
-            sl.md->steps++;
-            s->particle_steps += r->n;
-        }
+        const unsigned int er = s->errs_h[r->slot];
+        // the first launch of a system spends its first step on the first build and forces
+        const int done = stepping ? K - (r->first ? 1 : 0) : 0;
+        r->first = false;
+        r->done_steps += done;
+        sl.md->steps += done;
+        s->particle_steps += r->n * (long)done;
         if (er & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW | ERR_TILE_CAP | ERR_TIMEOUT | ERR_CELL_RANGE)) {
             set_error("serving: system %ld failed in a batched step (err=0x%x)", r->ticket, er);
-            PD_TRY(retire(s, r, true));
-            s->dirty = true;
+            s->finished.push_back({r, true});
         } else if (r->done_steps >= r->steps) {
-            PD_TRY(retire(s, r, false));
-            s->dirty = true;
+            s->finished.push_back({r, false});
         } else {
             keep.push_back(r);
         }
     }
+    if (keep.size() != s->active.size() || !admitted.empty()) s->dirty = true;
+    for (SrvReq* r : admitted) keep.push_back(r);
     s->active.swap(keep);
-    s->ms[3] += 1e3 * (now_s(s) - t_ret);
+    if (s->active.empty() && !s->finished.empty()) {
+        // nothing left to step: retire now rather than at the next tick
+        PD_TRY(retire_all(s, s->finished));
+    }
+    if (n_queued) *n_queued = (int)s->queue.size();
     if (n_active) *n_active = (int)s->active.size();
+    return PD_OK;
+}
+
+int pd_srv_completed(pd_srv s, long* tickets, int cap, int* n) {
+    if (!s || !n || (cap > 0 && !tickets)) return PD_EINVAL;
+    int k = 0;
+    while (k < cap && k < (int)s->completed.size()) {
+        tickets[k] = s->completed[k];
+        ++k;
+    }
+    s->completed.erase(s->completed.begin(), s->completed.begin() + k);
+    *n = k;
     return PD_OK;
 }
 

@@ -143,6 +143,7 @@ def lib():
                               P(ctypes.c_double)], ip),
             "pd_srv_tuned": ([vp, vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_srv_timers": ([vp, vp], ip),
+            "pd_srv_completed": ([vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_selftest_recip": ([ip, vp, vp, lp], ip),
             "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
@@ -528,6 +529,13 @@ class Server:
         ms = np.zeros(4)
         check(lib().pd_srv_timers(self.h, _ptr(ms)))
         return dict(zip(("admit", "admit_reset", "step", "retire"), ms.tolist()))
+
+    def completed(self, cap=4096):
+        """Tickets finished (done or failed) since the last call."""
+        out = np.zeros(cap, np.int64)
+        n = ctypes.c_int(0)
+        check(lib().pd_srv_completed(self.h, _ptr(out), int(cap), ctypes.byref(n)))
+        return out[: n.value].tolist()
 
     def tuned(self):
         b = np.zeros(64, np.int32)
