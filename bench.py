@@ -188,13 +188,74 @@ def form_precision(pd, torch, x, v, L, steps, warmup, fp64_value):
     f64 = vd64.deviceToHostProp(0, with_ghost=False)  # same order as xf (map on one domain keeps it)
     frms = np.sqrt((f64 ** 2).sum(axis=1).mean())
     err = np.sqrt(((f32 - f64) ** 2).sum(axis=1)) / frms
+    gerr = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
     TUNE["precision"] = "fp64"
     return {"workload": workload_name(N_SIDE, True), "value": val, "unit": METRIC, "steps": steps,
             "ms_per_step": ms / steps, "vs_fp64_path": val / fp64_value,
             "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in t.items()},
             "list_rebuilds": int(E[:, 3].sum()),
-            "force_error_vs_fp64": {"mean": float(err.mean()), "max": float(err.max()),
-                                    "norm": "|F32 - F64| / F_rms(F64), per particle, final positions"}}
+            "force_error_vs_fp64": {"mean": float(err.mean()), "max": float(err.max()), "global": gerr,
+                                    "norm": "per particle |F32 - F64| / F_rms(F64) at the final positions; "
+                                            "global = ||F32 - F64|| / ||F64||"}}
+
+
+def fp64_forces(pd, x, L):
+    """LJ forces of the FP64 GPU cell-list path (the path the parity tests hold to
+    the FP64 oracle) at positions x, in the order of x."""
+    n = x.shape[0]
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(n, lo, hi, bc, R_CUT, dtype=np.float64, props=[(pd.PD_F64, 3)])
+    vd.hostToDevicePos(x)
+    vd.map()
+    vd.ghost_get()
+    cl = vd.getCellListGPU(R_CUT)
+    vd.updateCellListGPU(cl)
+    vd.lj_forces(0, cl=cl, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+    f = vd.deviceToHostProp(0, with_ghost=False)
+    del cl, vd
+    return f
+
+
+def form_clustered(pd, torch, steps=200, check_every=20, warmup=3):
+    """Precision form on the clustered layout: 4,096,000 particles in 64 Gaussian
+    clusters (sigma_c 8) at uniform centres in a 176 periodic box, minimum distance
+    0.8 (redraws, then centre moves); force error against the FP64 path every
+    `check_every` steps."""
+    from openfpm_pdata_b200 import workloads
+    t0 = time.perf_counter()
+    x, v, L, redraws = workloads.lj_clustered_lib(4096000, 176.0, seed=4)
+    t_gen = time.perf_counter() - t0
+    n = x.shape[0]
+    TUNE["precision"] = "mixed"
+    vd, md = build_system(pd, x, v, L)
+    TUNE["precision"] = "fp64"
+    md.run(warmup, energies=False)
+    errs, ms_tot, done, rebuilds = [], 0.0, 0, 0
+    while done < steps:
+        k = min(check_every, steps - done)
+        ms, E = _timed(md, k, torch)
+        ms_tot += ms
+        done += k
+        rebuilds += int(E[:, 3].sum())
+        xf = vd.deviceToHostPos(with_ghost=False)
+        f32 = vd.deviceToHostProp(1, with_ghost=False).astype(np.float64)
+        f64 = fp64_forces(pd, xf, L)
+        frms = np.sqrt((f64 ** 2).sum(axis=1).mean())
+        e = np.sqrt(((f32 - f64) ** 2).sum(axis=1)) / frms
+        g = np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum())
+        errs.append((done, float(e.mean()), float(e.max()), float(g)))
+    cnt = np.bincount((np.floor(x / (L / 62)).astype(int) % 62) @ np.array([1, 62, 62 * 62]), minlength=62 ** 3)
+    del md, vd
+    return {"workload": "LJ MD mixed-precision, N=4,096,000 in 64 Gaussian clusters (sigma_c 8) at uniform "
+                        "centres, periodic box 176, minimum distance 0.8, r_cut 2.5, skin 0.3, dt 0.005",
+            "value": n * steps / (ms_tot / 1e3), "unit": METRIC, "steps": steps, "ms_per_step": ms_tot / steps,
+            "list_rebuilds": rebuilds, "generator_s": t_gen, "centre_redraws": redraws,
+            "layout": {"cell_occupancy_max": int(cnt.max()), "cell_occupancy_p99": float(np.percentile(cnt, 99)),
+                       "cell_occupancy_mean": float(cnt.mean()), "cell_side": L / 62},
+            "force_error_vs_fp64": {"steps_checked": [e[0] for e in errs],
+                                    "mean": [e[1] for e in errs], "max": [e[2] for e in errs],
+                                    "global": [e[3] for e in errs],
+                                    "norm": "per particle |F32 - F64| / F_rms(F64); global = ||F32 - F64|| / ||F64||"}}
 
 
 def form_cell_list_every_step(pd, torch, steps=100, warmup=5):
@@ -367,7 +428,8 @@ def main():
                     help="fp64: plain FP64 path; mixed: FP32 cell-local positions, Kahan sums, FP64 wrap/energies")
     ap.add_argument("--forms", default="all",
                     help="other workloads reported beside the main line: all, none, or a comma list of "
-                         "precision,c1,sph,serving")
+                         "precision,clustered,c1,sph,serving")
+    ap.add_argument("--clustered-steps", type=int, default=200, help="steps of the clustered precision form")
     ap.add_argument("--serve-systems", type=int, default=400, help="systems in the serving sample")
     a = ap.parse_args()
     TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp, precision=a.precision)
@@ -496,10 +558,12 @@ def main():
         assert np.isfinite(E2).all()
 
     if rank == 0 and world == 1 and a.forms != "none":
-        want = a.forms.split(",") if a.forms != "all" else ["precision", "c1", "sph", "serving"]
+        want = a.forms.split(",") if a.forms != "all" else ["precision", "clustered", "c1", "sph", "serving"]
         forms = {}
         if "precision" in want and not mixed:
             forms["precision"] = form_precision(pd, torch, x, v, L, a.steps, a.warmup, value)
+        if "clustered" in want:
+            forms["clustered"] = form_clustered(pd, torch, steps=a.clustered_steps)
         if "c1" in want:
             forms["cell_list_every_step"] = form_cell_list_every_step(pd, torch)
         if "sph" in want:

@@ -144,6 +144,8 @@ def lib():
             "pd_srv_tuned": ([vp, vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_srv_timers": ([vp, vp], ip),
             "pd_srv_completed": ([vp, vp, ip, P(ctypes.c_int)], ip),
+            "pd_gen_clustered": ([lp, ctypes.c_double, ip, ctypes.c_double, ctypes.c_double, ctypes.c_ulong, ip, vp,
+                                  P(ctypes.c_long)], ip),
             "pd_selftest_recip": ([ip, vp, vp, lp], ip),
             "pd_md_verlet_get": ([vp, vp, vp, lp, P(ctypes.c_int)], ip),
         }
