@@ -330,6 +330,21 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
         if (md->tg.TX <= 1) return PD_OK;  // stays on global rows
         PD_TRY(tile_plan(cl, n, md->tg.TX / 2, md->tg, md->ntiles));
     }
+    if (md->tile_tx == 0 && md->physics == 1 && md->tg.TX > 1) {
+        // automatic width for SPH: the densest tile's two staged records within about
+        // 48 KB (several CTAs per SM); the mean occupancy counts the empty part of
+        // the tank, so the width is rescaled from the measured largest tile
+        const long target = 48L * 1024 / (2L * h->pos_bytes);
+        if ((long)tmax > target) {
+            int tx = (int)((double)(md->tg.TX + 2) * (double)target / (double)tmax) - 2;
+            if (tx < 1) tx = 1;
+            if (tx < md->tg.TX) {
+                PD_TRY(tile_plan(cl, n, tx, md->tg, md->ntiles));
+                PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax,
+                                  cmax, st));
+            }
+        }
+    }
     md->tcap = tmax;
     PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                       md->vl->r_cut, md->pos32, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
@@ -535,6 +550,7 @@ int pd_sph_create(pd_vd h, const pd_sph_params_t* sp, const pd_md_params_t* mp, 
     md->mp = *mp;
     md->sp = *sp;
     md->physics = 1;
+    md->tile_p = 4;  // narrow SPH tiles: four lanes per particle keep the CTA busy
     md->lj.eps = md->lj.sigma = 1.0;
     md->lj.r_cut = 2.0 * sp->h;
     double rlist = 2.0 * sp->h + (mp->skin > 0 ? mp->skin : 0);

@@ -18,13 +18,14 @@
 // from a packed auxiliary array written by the integrator.
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
+#include "pd_lj.cuh"
 #include "pd_sph.cuh"
 #include "pd_tile.cuh"
 
 namespace pd {
 
 template <class T> struct SphK {
-    T h, m, c0, rho0, B, alpha, gz, eta2, dw3, r2c;
+    T h, m, c0, rho0, B, alpha, gz, eta2, dw3, r2c, inv_h, visc;  // visc = -alpha c0 h
 };
 
 template <class T> __device__ __forceinline__ T eos(const SphK<T>& P, T rho) {
@@ -34,24 +35,30 @@ template <class T> __device__ __forceinline__ T eos(const SphK<T>& P, T rho) {
     return P.B * (x7 - T(1));
 }
 
-// (dW/dr)/r of the cubic spline, q = r/h
-template <class T> __device__ __forceinline__ T dwdr_over_r(const SphK<T>& P, T r) {
-    T q = r / P.h;
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
+// (dW/dr)/r of the cubic spline from r and 1/r, q = r/h
+template <class T> __device__ __forceinline__ T dwdr_over_r(const SphK<T>& P, T r, T inv_r) {
+    T q = r * P.inv_h;
     T d;
     if (q < T(1)) d = (T(-3) * q + T(2.25) * q * q);
     else if (q < T(2)) d = T(-0.75) * (T(2) - q) * (T(2) - q);
     else d = T(0);
-    return P.dw3 * d / r;
+    return P.dw3 * d * inv_r;
 }
 
-// pressure into the position record, (v, rho) into the auxiliary record
+// the staged pressure term p / rho^2 (the same operations as p_b / (rho_b rho_b) per pair)
+template <class T> __device__ __forceinline__ T p_over_rho2(const SphK<T>& P, T rho) { return eos(P, rho) / (rho * rho); }
+
+// p / rho^2 into the position record, (v, rho) into the auxiliary record
 template <class T>
 __global__ void k_sph_pack(typename V4<T>::type* __restrict__ pos, typename V4<T>::type* __restrict__ aux,
                            const T* __restrict__ v, const T* __restrict__ rho, long cap, long n, SphK<T> P) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         typename V4<T>::type x = ld4(pos, i);
         T r = rho[i];
-        x.w = eos(P, r);
+        x.w = p_over_rho2(P, r);
         st4(pos, i, x);
         typename V4<T>::type a;
         a.x = v[i];
@@ -90,7 +97,7 @@ __global__ void __launch_bounds__(256) k_sph_kick_drift(typename V4<T>::type* __
         }
         T r = rho[i] + half * drho[i];
         rho[i] = r;
-        x.w = eos(P, r);
+        x.w = p_over_rho2(P, r);
         st4(pos, i, x);
         typename V4<T>::type au;
         au.x = vx;
@@ -219,7 +226,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
         const unsigned int li = base + i;
         const T4 xi = sp[active ? li : 0];
         const T4 ai = sa[active ? li : 0];
-        const T pa_r = active ? xi.w / (ai.w * ai.w) : T(0);
+        const T pa_r = xi.w;
         const int words = active ? (nn[i] + 1) >> 1 : 0;
         T ax = 0, ay = 0, az = 0, dr = 0;
         const unsigned int* row = nbr + i;
@@ -233,18 +240,16 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
                 const T r2 = dist2(dx, dy, dz);
                 if (r2 < K.r2c && l != li) {
                     const T4 aq = sa[l];
-                    const T r = sqrt(r2);
-                    const T dwr = dwdr_over_r(K, r);
+                    const T inv_r = rsqrt_t(r2);
+                    const T dwr = dwdr_over_r(K, r2 * inv_r, inv_r);
                     const T vx = ai.x - aq.x, vy = ai.y - aq.y, vz = ai.z - aq.z;
                     const T vr = vx * dx + vy * dy + vz * dz;
-                    const T pb = xq.w;
                     T pi_ab = 0;
                     if (vr < T(0)) {
-                        const T mu = K.h * vr / (r2 + K.eta2);
-                        const T rbar = T(0.5) * (ai.w + aq.w);
-                        pi_ab = -K.alpha * K.c0 * mu / rbar;
+                        // -alpha c0 mu / rho_bar, mu = h vr / (r^2 + eta^2): one reciprocal
+                        pi_ab = K.visc * vr * recip((r2 + K.eta2) * (T(0.5) * (ai.w + aq.w)));
                     }
-                    const T coef = -K.m * (pa_r + pb / (aq.w * aq.w) + pi_ab) * dwr;
+                    const T coef = -K.m * (pa_r + xq.w + pi_ab) * dwr;
                     ax += coef * dx;
                     ay += coef * dy;
                     az += coef * dz;
@@ -285,6 +290,8 @@ template <class T> static SphK<T> sphk(const pd_sph_params_t& sp) {
     K.dw3 = w3 / K.h;
     T two_h = T(2) * K.h;
     K.r2c = two_h * two_h;
+    K.inv_h = T(1) / K.h;
+    K.visc = -K.alpha * K.c0 * K.h;
     return K;
 }
 
