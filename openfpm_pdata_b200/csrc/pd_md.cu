@@ -116,6 +116,22 @@ __global__ void k_gather_cs2(const typename V4<T>::type* __restrict__ pos, const
     }
 }
 
+// the same gather bounded by the device count of real particles + images
+template <class T>
+__global__ void k_gather_cs2_dev(const typename V4<T>::type* __restrict__ pos, const int* __restrict__ sorted,
+                                 long bound, const unsigned int* __restrict__ n_img, long n_real,
+                                 typename V4<T>::type* __restrict__ out) {
+    long n = n_real + (long)*n_img;
+    if (n > bound) n = bound;
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        int i = sorted[k];
+        typename V4<T>::type r = ld4(pos, i);
+        if (sizeof(T) == 8) r.w = __longlong_as_double((long long)i);
+        else r.w = __int_as_float(i);
+        st4(out, k, r);
+    }
+}
+
 // v += h f ; x += dt v ; largest |x - xb|^2
 template <class T>
 __global__ void __launch_bounds__(FBLOCK) k_kick_drift(typename V4<T>::type* __restrict__ pos,
@@ -219,6 +235,36 @@ __global__ void k_energy(const double* __restrict__ fpart, int nbf, const double
         E[1] = sh[1][0];
         E[2] = sh[2][0];
         E[3] = rebuilt ? (double)*rebuilt : 0.0;
+    }
+}
+
+// k_energy writing the row of a device step counter, which it advances (captured
+// steps: the same graph writes successive rows)
+__global__ void k_energy_idx(const double* __restrict__ fpart, int nbf, const double* __restrict__ kpart, int nbk,
+                             double rebuilt, double* __restrict__ E, int* __restrict__ idx) {
+    __shared__ double sh[3][256];
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < nbk; i += 256) a += kpart[i];
+    for (int i = threadIdx.x; i < nbf; i += 256) {
+        b += fpart[2 * i];
+        c += fpart[2 * i + 1];
+    }
+    sh[0][threadIdx.x] = a;
+    sh[1][threadIdx.x] = b;
+    sh[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double* e = E + 4 * (long)*idx;
+        e[0] = sh[0][0];
+        e[1] = sh[1][0];
+        e[2] = sh[2][0];
+        e[3] = rebuilt;
+        *idx += 1;
     }
 }
 
@@ -418,6 +464,116 @@ int md_forces(pd_md md, cudaStream_t st) {
 
 using namespace pd;
 
+namespace pd {
+
+// One velocity-Verlet step of the LJ driver in cell-list mode (cell list rebuilt
+// every step) with no host synchronisation: the image count stays on the device
+// (ghost_generate without the read-back, capacity img_cap) and bounds the image
+// cell sort and the gather.  The same operations as the synchronous step.
+template <class T>
+static int md_step_cl(pd_md md, cudaStream_t st, long img_cap) {
+    typedef typename V4<T>::type T4;
+    pd_vd h = md->h;
+    pd_cl cl = md->cl;
+    const long n = h->n_real;
+    Prop& V = h->props[md->mp.vel_prop];
+    Prop& F = h->props[md->mp.force_prop];
+    const T half = (T)(0.5 * md->mp.dt / md->mp.mass);
+    PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
+    pd::launch(k_kick_drift<T>, md->nblk, FBLOCK, 0, st, (T4*)h->pos, md->xb.as<T4>(), (T*)V.d, (const T*)F.d, h->cap,
+               n, half, (T)md->mp.dt, &h->ctrl->maxdisp2);
+    PD_LAUNCH_CHECK();
+    h->n_total = n;
+    h->img_valid = false;
+    PD_TRY(wrap_positions(h, n, st));
+    PD_TRY(cl_build(h, cl, n, nullptr, st));
+    PD_TRY(cl_reorder(h, cl, n, 1ul << md->mp.vel_prop, true, true, st));
+    PD_TRY(ghost_generate(h, img_cap, false, st));
+    PD_TRY(cl_build(h, cl, n + img_cap, &h->ctrl->n_img, st));
+    const long bound = n + img_cap;
+    PD_TRY(h->tmp.ensure((size_t)bound * h->pos_bytes));
+    pd::launch(k_gather_cs2_dev<T>, grid_for(bound, 256), 256, 0, st, (const T4*)h->pos, cl->sorted.as<int>(), bound,
+               (const unsigned int*)&h->ctrl->n_img, n, h->tmp.as<T4>());
+    pd::launch(k_lj_cell<T>, md->nblk, FBLOCK, 0, st, (const T4*)h->pos, n, h->tmp.as<T4>(),
+               cl->cell_start.as<unsigned int>(), grid_of<T>(cl), ljp<T>(md->lj), (T*)F.d, h->cap,
+               md->fpart.as<double>());
+    pd::launch(k_kick<T>, md->nblk, FBLOCK, 0, st, (T*)V.d, (const T*)F.d, h->cap, n, half, md->mp.mass,
+               md->kpart.as<double>());
+    pd::launch(k_energy_idx, 1, 256, 0, st, (const double*)md->fpart.as<double>(), md->nblk,
+               (const double*)md->kpart.as<double>(), md->nblk, 1.0, md->E.as<double>(), md->eidx.as<int>());
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+static int md_step_cl_any(pd_md md, cudaStream_t st, long img_cap) {
+    return md->h->dtype == PD_F64 ? md_step_cl<double>(md, st, img_cap) : md_step_cl<float>(md, st, img_cap);
+}
+
+// cell-list mode: the first step of a run sizes every buffer, the step is
+// captured once as a CUDA graph (on a private stream: the legacy stream cannot
+// capture) and the remaining steps are graph launches on the caller's stream
+static int md_run_cl_graph(pd_md md, int steps, cudaStream_t st, double* E) {
+    pd_vd h = md->h;
+    if (!md->ready) {
+        PD_TRY(md_rebuild(md, st));
+        PD_TRY(md_forces(md, st));
+        md->ready = true;
+        md->gcl_img_cap = 0;
+    }
+    PD_TRY(md->E.ensure(sizeof(double) * 4 * (steps + 1)));
+    PD_TRY(md->eidx.ensure(sizeof(int)));
+    PD_CUDA(cudaMemsetAsync(md->eidx.p, 0, sizeof(int), st));
+    int s0 = 0;
+    if (!md->gcl) {
+        PD_TRY(read_ctrl(h, st));
+        const long m = h->ctrl_h->n_img;
+        md->gcl_img_cap = m + m / 2 + 1024;
+        PD_TRY(ensure_capacity(h, h->n_real + md->gcl_img_cap + 1, st));
+        if (steps > 0) {
+            PD_TRY(md_step_cl_any(md, st, md->gcl_img_cap));  // also sizes the buffers the graph uses
+            s0 = 1;
+        }
+        PD_CUDA(cudaStreamSynchronize(st));
+        if (!md->gst) PD_CUDA(cudaStreamCreateWithFlags(&md->gst, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        const unsigned long long l0 = pd_launch_count();
+        PD_CUDA(cudaStreamBeginCapture(md->gst, cudaStreamCaptureModeThreadLocal));
+        int rc = md_step_cl_any(md, md->gst, md->gcl_img_cap);
+        cudaError_t ce = cudaStreamEndCapture(md->gst, &g);
+        md->gcl_kernels = pd_launch_count() - l0;
+        __atomic_fetch_sub(&g_launches, md->gcl_kernels, __ATOMIC_RELAXED);  // captured, not launched
+        if (rc != PD_OK || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_error("cell-list step capture failed: %s", cudaGetErrorString(ce));
+            return rc != PD_OK ? rc : PD_ECUDA;
+        }
+        ce = cudaGraphInstantiate(&md->gcl, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            md->gcl = nullptr;
+            set_error("cell-list step graph: %s", cudaGetErrorString(ce));
+            return PD_ECUDA;
+        }
+    }
+    for (int s = s0; s < steps; ++s) PD_CUDA(cudaGraphLaunch(md->gcl, st));
+    __atomic_fetch_add(&g_launches, (unsigned long long)(steps - s0) * md->gcl_kernels, __ATOMIC_RELAXED);
+    md->steps += steps;
+    md->builds += steps;
+    if (E && steps > 0) PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));
+    PD_CUDA(cudaStreamSynchronize(st));
+    PD_TRY(read_ctrl(h, st));
+    h->n_img = h->ctrl_h->n_img;
+    h->n_total = h->n_real + h->n_img;
+    h->img_valid = true;
+    if (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW | ERR_CAP_OVERFLOW)) {
+        set_error("pd_md_run: device capacity overflow (err=0x%x)", h->ctrl_h->err);
+        return PD_EOVERFLOW;
+    }
+    return PD_OK;
+}
+
+}  // namespace pd
+
 extern "C" {
 
 int pd_selftest_recip(int dtype, const void* x_host, void* out_host, long n) {
@@ -590,6 +746,9 @@ int pd_md_destroy(pd_md md) {
     md->offK.release();
     md->aux.release();
     md->rpart.release();
+    md->eidx.release();
+    if (md->gcl) cudaGraphExecDestroy(md->gcl);
+    if (md->gst) cudaStreamDestroy(md->gst);
     for (int i = 0; i < 8; ++i)
         if (md->ev[i]) cudaEventDestroy(md->ev[i]);
     delete md;
@@ -598,6 +757,8 @@ int pd_md_destroy(pd_md md) {
 
 int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     if (!md || steps < 0) return PD_EINVAL;
+    if (md->mp.use_cell_list && md->physics == 0 && !md->mixed && !md->timing)
+        return md_run_cl_graph(md, steps, S(stream), E);
     pd_vd h = md->h;
     cudaStream_t st = S(stream);
     long n = h->n_real;

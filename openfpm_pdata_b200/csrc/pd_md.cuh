@@ -33,6 +33,12 @@ struct pd_md_s {
     bool off_valid = false;  // `off` holds the authoritative state (after the first build)
     pd::Buf off, offb, offK;
     long builds = 0, steps = 0;
+    // cell-list mode: the captured step graph, its image capacity, the step counter
+    cudaGraphExec_t gcl = nullptr;
+    cudaStream_t gst = nullptr;
+    long gcl_img_cap = 0;
+    unsigned long long gcl_kernels = 0;
+    pd::Buf eidx;
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
     cudaEvent_t ev[8] = {};
