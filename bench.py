@@ -392,7 +392,10 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
                         f"first {half} submitted at once (capacity), last {n_systems - half} Poisson at 0.8 x capacity",
             "max_slots": slots, "mean_particles": float(sizes.mean()),
             "capacity": {"value": cap_ps, "unit": METRIC, "systems_per_s": cap_sys},
-            "poisson_0.8": {"value": srv_ps, "unit": METRIC, "vs_capacity": srv_ps / cap_ps,
+            "poisson_0.8": {"value": srv_ps, "unit": METRIC, "offered_vs_capacity": 0.8,
+                            "vs_capacity": srv_ps / cap_ps,
+                            "note": "value = all particle-steps of the Poisson systems / (last completion - first "
+                                    "arrival), ramp-up and drain included",
                             "p50_ms": float(np.percentile(lat, 50) * 1e3),
                             "p99_ms": float(np.percentile(lat, 99) * 1e3),
                             "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50))},

@@ -378,9 +378,10 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     }
     if (md->tile_tx == 0 && md->physics == 1 && md->tg.TX > 1) {
         // automatic width for SPH: the densest tile's two staged records within about
-        // 48 KB (several CTAs per SM); the mean occupancy counts the empty part of
-        // the tank, so the width is rescaled from the measured largest tile
-        const long target = 48L * 1024 / (2L * h->pos_bytes);
+        // 60 KB in FP64 (tiles of two or more cells, three CTAs per SM) or 48 KB in
+        // FP32; the mean occupancy counts the empty part of the tank, so the width
+        // is rescaled from the measured largest tile
+        const long target = (h->dtype == PD_F64 ? 60L : 48L) * 1024 / (2L * h->pos_bytes);
         if ((long)tmax > target) {
             int tx = (int)((double)(md->tg.TX + 2) * (double)target / (double)tmax) - 2;
             if (tx < 1) tx = 1;

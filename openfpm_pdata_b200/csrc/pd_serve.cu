@@ -57,7 +57,7 @@ namespace pd {
 static constexpr int SRV_P = 2;                       // lanes per particle in the batched force kernel
 static constexpr int SRV_SMEM = 48 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
 static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged FP32 records per tile
-static constexpr int SRV_BSMEM = 32 * 1024;           // staging bytes per tile CTA of the batched list build
+static constexpr int SRV_BSMEM = 48 * 1024;           // staging bytes per tile CTA of the batched list build
 static constexpr unsigned SRV_BCAP = SRV_BSMEM / 16;
 static constexpr int SRV_BIG = 192 * 1024;            // staging of the overflow kernels (tiles beyond SRV_CAP)
 static constexpr unsigned SRV_BIG_CAP = SRV_BIG / 16;
