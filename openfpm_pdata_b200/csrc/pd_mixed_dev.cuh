@@ -153,11 +153,18 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             Kahan kx = {0.f, 0.f}, ky = {0.f, 0.f}, kz = {0.f, 0.f}, ke = {0.f, 0.f}, kw = {0.f, 0.f};
             const unsigned int* row = nbr + i;
-            unsigned int nxt = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+            // row words read four iterations ahead (register shift ring) to cover the memory latency
+            unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+            unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
+            unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
+            unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
 #pragma unroll 2
             for (int k = sub; k < words; k += P) {
-                const unsigned int pair = nxt;
-                if (k + P < words) nxt = __ldg(row + (long)(k + P) * stride);
+                const unsigned int pair = q0;
+                q0 = q1;
+                q1 = q2;
+                q2 = q3;
+                q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
                 float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {

@@ -230,8 +230,17 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
         const int words = active ? (nn[i] + 1) >> 1 : 0;
         T ax = 0, ay = 0, az = 0, dr = 0;
         const unsigned int* row = nbr + i;
+        // row words read four iterations ahead (register shift ring)
+        unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+        unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
+        unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
+        unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
         for (int k = sub; k < words; k += P) {
-            const unsigned int pair = __ldg(row + (long)k * stride);
+            const unsigned int pair = q0;
+            q0 = q1;
+            q1 = q2;
+            q2 = q3;
+            q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
 #pragma unroll
             for (int hh = 0; hh < 2; ++hh) {
                 const unsigned int l = hh ? (pair >> 16) : (pair & 0xffffu);

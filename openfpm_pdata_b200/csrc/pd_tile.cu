@@ -119,11 +119,18 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             const unsigned int* row = nbr + i;
-            unsigned int nxt = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+            // row words read four iterations ahead (register shift ring) to cover the memory latency
+            unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+            unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
+            unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
+            unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
 #pragma unroll 2
             for (int k = sub; k < words; k += P) {
-                const unsigned int pair = nxt;
-                if (k + P < words) nxt = __ldg(row + (long)(k + P) * stride);
+                const unsigned int pair = q0;
+                q0 = q1;
+                q1 = q2;
+                q2 = q3;
+                q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
