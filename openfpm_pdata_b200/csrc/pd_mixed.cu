@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) k_kick32(float* __restrict__ v, const flo
 }
 
 template <int P>
-__global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj_mixed(const float4* __restrict__ off, long n_real,
+__global__ void __launch_bounds__(FBLOCK_T, 5) k_vtile_lj_mixed(const float4* __restrict__ off, long n_real,
                                                              TileGeom tg, const unsigned int* __restrict__ csR,
                                                              const unsigned int* __restrict__ csI, unsigned int cap,
                                                              const unsigned int* __restrict__ nbr,
