@@ -407,6 +407,22 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
                         "rebuilds": st1["rebuilds"]}}
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (every rank gets it): the replicas' timed regions
+    are bracketed by barriers, so the job takes as long as its slowest GPU."""
+    import torch
+    if dist is None:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, n_local, steps, ms_max):
+    """Whole-job particle-steps/s of `world` replicas of n_local particles each."""
+    return world * n_local * steps / (ms_max / 1000.0)
+
+
 def dist_setup(n_gpus):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -433,7 +449,7 @@ def main():
                     help="other workloads reported beside the main line: all, none, or a comma list of "
                          "precision,clustered,c1,sph,serving")
     ap.add_argument("--clustered-steps", type=int, default=200, help="steps of the clustered precision form")
-    ap.add_argument("--serve-systems", type=int, default=400, help="systems in the serving sample")
+    ap.add_argument("--serve-systems", type=int, default=600, help="systems in the serving sample")
     a = ap.parse_args()
     TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp, precision=a.precision)
     mixed = a.precision == "mixed"
@@ -495,15 +511,12 @@ def main():
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
     barrier()
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, pg, "cuda")
     timers = md.timers()
     n_dom, mean_nn, max_nn = md.list_stats()
     builds = int(E[:, 3].sum())
 
-    value = world * n * a.steps / (ms / 1000.0)
+    value = replica_value(world, n, a.steps, ms)
     # roofline of the dominant kernel (Verlet-list LJ force): algorithmic bytes per launch
     # = N * (32 B position record + 4 B row length + 4 B * mean row + 24 B force)
     f_ms, f_cnt = timers["force"]
