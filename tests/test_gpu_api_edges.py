@@ -1,0 +1,120 @@
+"""Edge cases and the remaining reference-API rows through the C ABI.
+
+reduce_local (vector_dist_cuda_funcs.cuh:247-270), getDomainIteratorGPU and
+toKernel (vector_dist.hpp:1958-1979, 2961-2966), resize, an empty vector, a
+single particle, and ghost_get with periodic and non-periodic directions mixed
+(vector_dist_unit_test.cpp:631-735 checks periodic ghosts; bc per direction is
+the reference's `const size_t (&bc)[dim]`).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+F32, F64 = np.float32, np.float64
+
+
+@pytest.fixture(scope="module")
+def pd():
+    from openfpm_pdata_b200 import pd as _pd
+    _pd.lib()
+    return _pd
+
+
+def test_reduce_local_sum_and_max(pd):
+    rng = np.random.default_rng(3)
+    n = 100003  # ragged: not a multiple of any block size
+    vd = pd.VectorDist(n, np.zeros(3), np.ones(3), np.ones(3, np.int32), 0.1, dtype=F64,
+                       props=[(pd.PD_F64, 2), (pd.PD_F32, 1), (pd.PD_I32, 1)])
+    vd.hostToDevicePos(rng.random((n, 3)))
+    a = rng.normal(size=(n, 2))
+    b = rng.normal(size=n).astype(np.float32)
+    c = rng.integers(-1000, 1000, size=n).astype(np.int32)
+    vd.hostToDeviceProp(0, a)
+    vd.hostToDeviceProp(1, b)
+    vd.hostToDeviceProp(2, c)
+    for comp in range(2):
+        assert vd.reduce_local(0, comp, pd.RED_ADD) == pytest.approx(a[:, comp].sum(), rel=1e-12, abs=1e-9)
+        assert vd.reduce_local(0, comp, pd.RED_MAX) == a[:, comp].max()
+    assert vd.reduce_local(1, 0, pd.RED_ADD) == pytest.approx(b.astype(np.float64).sum(), rel=1e-12, abs=1e-9)
+    assert vd.reduce_local(1, 0, pd.RED_MAX) == float(b.max())
+    assert vd.reduce_local(2, 0, pd.RED_ADD) == float(c.astype(np.int64).sum())
+    assert vd.reduce_local(2, 0, pd.RED_MAX) == float(c.max())
+    # deterministic: the same bits twice
+    assert vd.reduce_local(0, 1, pd.RED_ADD) == vd.reduce_local(0, 1, pd.RED_ADD)
+
+
+def test_domain_iterator_and_view(pd):
+    n = 1000
+    rng = np.random.default_rng(4)
+    vd = pd.VectorDist(n, np.zeros(3), np.ones(3), np.ones(3, np.int32), 0.1, dtype=F64, props=[(pd.PD_F64, 3)])
+    vd.hostToDevicePos(rng.random((n, 3)))
+    it = vd.getDomainIteratorGPU(128)
+    assert tuple(it.thr) == (128, 1, 1) and tuple(it.wthr) == (8, 1, 1)
+    v0 = vd.toKernel()
+    assert v0.size_local == n and v0.size == n and v0.n_prop == 1 and v0.stride >= n
+    vd.map()
+    vd.ghost_get()
+    v1 = vd.toKernel()
+    m = vd.size_local_with_ghost()
+    assert v1.size_local == n and v1.size == m > n and v1.epoch > v0.epoch
+    itg = vd.getDomainIteratorGPU(256, with_ghost=True)
+    assert itg.wthr[0] * itg.thr[0] >= m and (itg.wthr[0] - 1) * itg.thr[0] < m
+
+
+def test_resize_keeps_leading_particles(pd):
+    rng = np.random.default_rng(5)
+    x = rng.random((5000, 3))
+    vd = pd.VectorDist(5000, np.zeros(3), np.ones(3), np.ones(3, np.int32), 0.1, dtype=F64, props=[(pd.PD_F64, 1)])
+    vd.hostToDevicePos(x)
+    vd.resize(20000)
+    assert vd.size_local() == 20000
+    assert np.array_equal(vd.deviceToHostPos(count=5000, with_ghost=False), x)
+    vd.resize(1000)
+    assert vd.size_local() == 1000
+    assert np.array_equal(vd.deviceToHostPos(with_ghost=False), x[:1000])
+
+
+def test_empty_vector(pd):
+    vd = pd.VectorDist(0, np.zeros(3), np.ones(3), np.ones(3, np.int32), 0.1, dtype=F64, props=[(pd.PD_F64, 3)])
+    vd.map()
+    vd.ghost_get()
+    assert vd.size_local() == 0 and vd.size_local_with_ghost() == 0
+    cl = vd.getCellListGPU(0.1)
+    vd.updateCellListGPU(cl)
+    start, ids = cl.get()[:2]
+    assert np.all(np.asarray(start) == 0) and len(ids) == 0
+    vl = vd.getVerlet(0.1)
+    off, idx = vl.get()
+    assert len(idx) == 0
+    assert vd.reduce_local(0, 0, pd.RED_ADD) == 0.0
+
+
+def test_single_particle_corner_images(pd, orc):
+    """One particle near a corner of a periodic box has 7 images (every shift
+    that reaches it), in shift order."""
+    lo, hi, bc = np.zeros(3), np.ones(3), np.ones(3, np.int32)
+    x = np.array([[0.01, 0.02, 0.97]])
+    vd = pd.VectorDist(1, lo, hi, bc, 0.1, dtype=F64)
+    vd.hostToDevicePos(x)
+    vd.ghost_get()
+    got = vd.deviceToHostPos()[1:]
+    img, src, shf = orc.ghost_get(x, lo, hi, bc, 0.1)
+    assert got.shape[0] == 7
+    assert np.array_equal(got, img)
+
+
+@pytest.mark.parametrize("bc", [[1, 0, 1], [0, 1, 0], [0, 0, 0]])
+def test_ghost_get_mixed_boundaries(pd, orc, bc):
+    rng = np.random.default_rng(6)
+    lo, hi = np.zeros(3), np.ones(3)
+    bc = np.array(bc, np.int32)
+    pos = rng.random((20000, 3))
+    vd = pd.VectorDist(pos.shape[0], lo, hi, bc, 0.2, dtype=F64)
+    vd.hostToDevicePos(pos)
+    vd.ghost_get()
+    img, src, shf = orc.ghost_get(pos, lo, hi, bc, 0.2)
+    got = vd.deviceToHostPos()[pos.shape[0]:]
+    assert np.array_equal(got, img)
+    gsrc, gshf = vd.ghost_records()
+    assert np.array_equal(gsrc, src) and np.array_equal(gshf, shf)
