@@ -529,6 +529,14 @@ def main():
         alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
+    # secondary roofline of the FP64 pair kernel (its arithmetic, not HBM, is the
+    # nearer ceiling): flops counted as executed -- distance 8 per row entry; inside
+    # r_cut another 29 (reciprocal seed + two Newton steps 9, s2 1, s6 2, force
+    # factor 5, three force FMAs 6, energy 4, virial 2); pairs inside r_cut
+    # estimated from the density (4/3 pi r_cut^3 rho)
+    rho = n / (L * L * L)
+    in_cut = 4.18879 * R_CUT ** 3 * rho
+    flops = n * (8 * mean_nn + 29 * in_cut)
     kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_f64" if a.tiles else "k_lj_verlet_f64")
     traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
 
@@ -546,7 +554,11 @@ def main():
                      "kernel": "k_vtile_lj_mixed" if mixed else ("k_vtile_lj<double>" if a.tiles else
                                                                   "k_lj_verlet<double>"),
                      "peak_kind": peak_kind,
-                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0},
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0,
+                     "arith": {"unit": "TFLOP/s", "dtype": "f32" if mixed else "f64",
+                               "achieved": flops / f_avg_s / 1e12, "flops_per_launch": flops,
+                               "nominal_peak": 75.0 if mixed else 37.0,
+                               "peak_kind": "nominal per-GPU vector FP32/FP64 figure, not measured on this pool"}},
         "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in timers.items()},
         "gpu_launches": int(launches),
         "clocks": ck,
