@@ -28,8 +28,8 @@ namespace pd {
 // largest staged neighbourhood and largest centre count over the tiles
 __global__ void k_tile_sizes(TileGeom tg, long ntiles, const unsigned int* __restrict__ csR,
                              const unsigned int* __restrict__ csI, unsigned int* __restrict__ tmax,
-                             unsigned int* __restrict__ cmax) {
-    unsigned int mt = 0, mc = 0;
+                             unsigned int* __restrict__ cmax, unsigned int* __restrict__ pmax) {
+    unsigned int mt = 0, mc = 0, mp = 0;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ntiles; t += (long)gridDim.x * blockDim.x) {
         int tx = (int)(t % tg.ntx);
         long rest = t / tg.ntx;
@@ -37,21 +37,28 @@ __global__ void k_tile_sizes(TileGeom tg, long ntiles, const unsigned int* __res
         int z = (int)(rest / tg.ny) + tg.pad;
         int x0 = tg.pad + tx * tg.TX;
         int x1 = min(x0 + tg.TX, tg.gs0 - tg.pad);
-        unsigned int tot = 0;
+        unsigned int tot = 0, pass = 0;
         for (int r = 0; r < 9; ++r) {
             int dz = r / 3 - 1, dy = r % 3 - 1;
             long rb = (long)tg.gs0 * ((y + dy) + (long)tg.gs1 * (z + dz));
-            tot += csR[rb + x1 + 1] - csR[rb + x0 - 1];
-            tot += csI[rb + x1 + 1] - csI[rb + x0 - 1];
+            const unsigned int rt = (csR[rb + x1 + 1] - csR[rb + x0 - 1]) + (csI[rb + x1 + 1] - csI[rb + x0 - 1]);
+            tot += rt;
+            pass += rt;
+            if (r % 3 == 2) {
+                mp = max(mp, pass);
+                pass = 0;
+            }
             if (r == 4) mc = max(mc, csR[rb + x1] - csR[rb + x0]);
         }
         mt = max(mt, tot);
     }
     mt = warp_max(mt);
     mc = warp_max(mc);
+    mp = warp_max(mp);
     if ((threadIdx.x & 31) == 0) {
         atomicMax(tmax, mt);
         atomicMax(cmax, mc);
+        atomicMax(pmax, mp);
     }
 }
 
@@ -85,6 +92,127 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::ty
     tile_segb(S, segb);
     if (!tile_stage<float>(pos32, pos32 + n_real, S, sm, cap, err)) return;  // (its barrier also covers segb)
     tile_rows<T>(S, segb, sm, pos, r2, lo_thr, hi_thr, nbr, nn, stride, max_nn, err, nn_max);
+}
+
+// List build in three passes of one z-layer each (rows 0-2, 3-5, 6-8 of the tile:
+// segments 0-5, 6-11, 12-17), staged one after the other into the same shared
+// memory with a third of the full staging (more resident CTAs).  A particle's
+// entry count and pending half-word carry over the passes, so its row holds the
+// entries in the same order as the single-pass walk; entries are indices into
+// the full staging layout, which the pair kernels stage.
+template <class T>
+__global__ void __launch_bounds__(TBLOCK) k_vtile_build3(const typename V4<T>::type* __restrict__ pos,
+                                                         const float4* __restrict__ pos32, long n_real,
+                                                         TileGeom tg, const unsigned int* __restrict__ csR,
+                                                         const unsigned int* __restrict__ csI, unsigned int pcap,
+                                                         T r2, float lo_thr, float hi_thr,
+                                                         unsigned int* __restrict__ nbr, int* __restrict__ nn,
+                                                         long stride, int max_nn, unsigned int* __restrict__ err,
+                                                         unsigned int* __restrict__ nn_max) {
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    float4* sm = reinterpret_cast<float4*>(tile_raw);
+    __shared__ TileSh S;
+    __shared__ unsigned int segb[18][TXMAX + 3];
+    tile_layout(tg, blockIdx.x, csR, csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    if (ib == ie) return;
+    tile_segb(S, segb);
+    const int ncol = S.ncol, nc = ncol - 1;
+    if (threadIdx.x == 0) mbar_init(&S.bar, 1);
+    __syncthreads();
+    const unsigned int self_base = S.oR[4] - S.cR[4][0];
+    const float4* pimg = pos32 + n_real;
+    // each thread: one domain particle per 128 (the tile's particles in order)
+    constexpr int MAXI = 2;  // domain particles per thread (tiles of up to 256)
+    float4 xi[MAXI];
+    unsigned int ph = 0;  // completed phases of the barrier (layers with records)
+    int jcol[MAXI], cnt[MAXI];
+    unsigned int pend[MAXI];
+    int nmine = 0;
+    for (unsigned int i = ib + threadIdx.x; i < ie && nmine < MAXI; i += blockDim.x, ++nmine) {
+        xi[nmine] = pos32[i];
+        int j = 1;
+        while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
+        jcol[nmine] = j;
+        cnt[nmine] = 0;
+        pend[nmine] = 0;
+    }
+    if (ie - ib > (unsigned int)(MAXI * blockDim.x)) {
+        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+        return;
+    }
+    for (int pass = 0; pass < 3; ++pass) {
+        const unsigned int base = S.oR[3 * pass];
+        const unsigned int end = pass < 2 ? S.oR[3 * pass + 3] : S.total;
+        const unsigned int tot = end - base;
+        if (tot > pcap) {
+            if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+            return;
+        }
+        bool ok = true;
+        if (tot > 0) {
+            if (threadIdx.x == 0) {
+                mbar_arrive_expect_tx(&S.bar, tot * (unsigned int)sizeof(float4));
+                for (int r = 3 * pass; r < 3 * pass + 3; ++r) {
+                    unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+                    if (lr) bulk_g2s(sm + (S.oR[r] - base), pos32 + S.cR[r][0], lr * (unsigned int)sizeof(float4), &S.bar);
+                    unsigned int li = S.cI[r][nc] - S.cI[r][0];
+                    if (li) bulk_g2s(sm + (S.oI[r] - base), pimg + S.cI[r][0], li * (unsigned int)sizeof(float4), &S.bar);
+                }
+            }
+            ok = mbar_wait_bounded(&S.bar, ph & 1u, 1u << 24);
+            if (!ok) {
+                atomicOr(err, ERR_TIMEOUT);
+                mbar_wait_bounded(&S.bar, ph & 1u, 1u << 24);
+            }
+            ++ph;
+        }
+        if (!__syncthreads_and(ok ? 1 : 0)) return;
+        for (int m = 0; m < nmine; ++m) {
+            const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
+            const int j = jcol[m];
+            const float4 x = xi[m];
+            int c = cnt[m];
+            unsigned int pd_ = pend[m];
+            unsigned int* out = nbr + i;
+#pragma unroll 1
+            for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg) {
+                const unsigned int qe = segb[sg][j + 2];
+#pragma unroll 4
+                for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
+                    const float4 xq = sm[q - base];
+                    const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
+                    if (d2 < hi_thr) {
+                        if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
+                            if (c < max_nn) {
+                                if (c & 1) out[(long)(c >> 1) * stride] = pd_ | (q << 16);
+                                else pd_ = q;
+                            }
+                            c++;
+                        }
+                    }
+                }
+            }
+            cnt[m] = c;
+            pend[m] = pd_;
+        }
+        // every thread is done with this layer before the next one is copied over it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+    }
+    for (int m = 0; m < nmine; ++m) {
+        const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
+        int c = cnt[m];
+        unsigned int* out = nbr + i;
+        // odd rows end with the particle itself, which the pair kernel skips
+        if ((c & 1) && c < max_nn) out[(long)(c >> 1) * stride] = pend[m] | ((self_base + i) << 16);
+        if (c > max_nn) {
+            atomicOr(err, ERR_NN_OVERFLOW);
+            atomicMax(nn_max, (unsigned int)c);
+            c = max_nn;
+        }
+        nn[i] = c;
+    }
 }
 
 // P threads per domain particle split its row (words w = sub, sub+P, ...; two
@@ -243,9 +371,9 @@ int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles) {
 
 int tile_sizes(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                unsigned int& tmax, unsigned int& cmax, cudaStream_t st) {
-    PD_CUDA(cudaMemsetAsync(&h->ctrl->tile_max, 0, 2 * sizeof(unsigned int), st));
+    PD_CUDA(cudaMemsetAsync(&h->ctrl->tile_max, 0, 3 * sizeof(unsigned int), st));
     pd::launch(k_tile_sizes, grid_for(ntiles, 256), 256, 0, st, tg, ntiles, csR, csI, &h->ctrl->tile_max,
-               &h->ctrl->tile_center_max);
+               &h->ctrl->tile_center_max, &h->ctrl->tile_pass_max);
     PD_LAUNCH_CHECK();
     PD_TRY(read_ctrl(h, st));
     tmax = h->ctrl_h->tile_max;
@@ -295,13 +423,29 @@ int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR
         max_nn = (int)(mean * 1.5 + 32);
     }
     max_nn = (max_nn + 1) & ~1;  // whole 32-bit words
+    // three z-layer passes with a third of the staging (more resident CTAs) when
+    // the largest layer is well below the whole tile and the tile's domain
+    // particles fit two per thread (the sizes of the tile_sizes call before)
+    const unsigned int pcap = h->ctrl_h->tile_pass_max, cmax = h->ctrl_h->tile_center_max;
+    const bool layers = pcap > 0 && 2 * pcap < cap && cmax <= 2u * TBLOCK;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        int smem = (int)(cap * sizeof(float4));
+        int smem = (int)((layers ? pcap : cap) * sizeof(float4));
         if (smem < 16) smem = 16;
         PD_TRY(nbr.ensure(sizeof(unsigned short) * (size_t)stride * max_nn));
         PD_TRY(nn.ensure(sizeof(int) * (size_t)stride));
         PD_CUDA(cudaMemsetAsync(nn.p, 0, sizeof(int) * (size_t)stride, st));
-        if (h->dtype == PD_F64) {
+        if (layers && h->dtype == PD_F64) {
+            PD_TRY(allow_smem(k_vtile_build3<double>, smem));
+            pd::launch(k_vtile_build3<double>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const double4*)h->pos,
+                       (const float4*)pos32.as<float4>(), n, tg, csR, csI, pcap, r_list * r_list, lo_thr, hi_thr,
+                       nbr.as<unsigned int>(), nn.as<int>(), stride, max_nn, &h->ctrl->err, &h->ctrl->nn_max);
+        } else if (layers) {
+            float rl = (float)r_list;
+            PD_TRY(allow_smem(k_vtile_build3<float>, smem));
+            pd::launch(k_vtile_build3<float>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const float4*)h->pos,
+                       (const float4*)pos32.as<float4>(), n, tg, csR, csI, pcap, rl * rl, lo_thr, hi_thr,
+                       nbr.as<unsigned int>(), nn.as<int>(), stride, max_nn, &h->ctrl->err, &h->ctrl->nn_max);
+        } else if (h->dtype == PD_F64) {
             PD_TRY(allow_smem(k_vtile_build<double>, smem));
             pd::launch(k_vtile_build<double>, (unsigned)ntiles, TBLOCK, (size_t)smem, st, (const double4*)h->pos,
                        (const float4*)pos32.as<float4>(), n, tg, csR, csI, cap, r_list * r_list, lo_thr, hi_thr,
