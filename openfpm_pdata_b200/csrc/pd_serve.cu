@@ -57,7 +57,7 @@ namespace pd {
 static constexpr int SRV_P = 2;                       // lanes per particle in the batched force kernel
 static constexpr int SRV_SMEM = 48 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
 static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged FP32 records per tile
-static constexpr int SRV_BSMEM = 48 * 1024;           // staging bytes per tile CTA of the batched list build
+static constexpr int SRV_BSMEM = 24 * 1024;           // staging bytes per CTA of the batched list build (one z-layer)
 static constexpr unsigned SRV_BCAP = SRV_BSMEM / 16;
 static constexpr int SRV_BIG = 192 * 1024;            // staging of the overflow kernels (tiles beyond SRV_CAP)
 static constexpr unsigned SRV_BIG_CAP = SRV_BIG / 16;
@@ -788,8 +788,9 @@ __global__ void __launch_bounds__(CHUNK) k_rb_image_k(const SysDesc* __restrict_
 }
 
 // tiled Verlet rows of the flagged systems (persistent CTAs, one mbarrier each).
-// BIG = 0: every flagged tile, those beyond SRV_BCAP appended to the overflow list;
-// BIG = 1: the overflow list, with SRV_BIG of shared memory.
+// BIG = 0: every flagged tile, built one z-layer at a time in SRV_BSMEM; tiles
+// with a layer beyond it (or more than 2 x TBLOCK domain particles) are appended
+// to the overflow list; BIG = 1: the overflow list, whole tiles in SRV_BIG.
 template <int BIG>
 __global__ void __launch_bounds__(TBLOCK) k_rb_build(const SysDesc* __restrict__ D, const RbWork* __restrict__ W,
                                                      BatchHdr* __restrict__ B, long* __restrict__ ovf,
@@ -815,11 +816,20 @@ __global__ void __launch_bounds__(TBLOCK) k_rb_build(const SysDesc* __restrict__
         tile_layout(d.tg, c, d.csR, d.csI, S);
         const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
         if (ib == ie) continue;
-        if (!BIG && S.total > cap) {
-            if (threadIdx.x == 0) ovf[atomicAdd(&B->ovf_build, 1u)] = g;
+        tile_segb(S, segb);
+        if (!BIG) {
+            unsigned int lmax = S.total - S.oR[6];
+            lmax = max(lmax, S.oR[3] - S.oR[0]);
+            lmax = max(lmax, S.oR[6] - S.oR[3]);
+            if (lmax > cap || ie - ib > 2u * TBLOCK) {
+                if (threadIdx.x == 0) ovf[atomicAdd(&B->ovf_build, 1u)] = g;
+                continue;
+            }
+            if (!tile_rows_layers<double>(S, segb, d.pos32, d.pos32 + d.n_real, sm, cap, d.pos, d.r2, d.lo_thr,
+                                          d.hi_thr, d.nbr, d.nn, d.tstride, d.max_nn, d.err, nn_max, &bar, parity))
+                break;  // a bounded wait gave up (error bit set): the barrier phase is unknown
             continue;
         }
-        tile_segb(S, segb);
         const int st = tile_stage_bar<float>(d.pos32, d.pos32 + d.n_real, S, sm, cap, d.err, &bar, parity);
         if (st > 0) parity ^= 1u;
         if (st < 0) {
@@ -1664,6 +1674,10 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         s->adm_pending = false;
     }
     if (s->dirty && !s->active.empty()) PD_TRY(upload_tables(s));
+    // free device memory for the admission check, queried while the GPU is idle
+    // (the query waits for running work)
+    size_t fr = 0, tot = 0;
+    if (!s->queue.empty()) PD_CUDA(cudaMemGetInfo(&fr, &tot));
     // one velocity-Verlet step of every active system; admissions are prepared
     // meanwhile on the admission stream (host work and asynchronous copies only)
     const bool stepping = !s->active.empty();
@@ -1681,8 +1695,6 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
     std::vector<char> used_slot(s->max_slots, 0);
     for (SrvReq* r : s->active) used_slot[r->slot] = 1;
     std::vector<SrvReq*> admitted;
-    size_t fr = 0, tot = 0;
-    if (!s->queue.empty()) PD_CUDA(cudaMemGetInfo(&fr, &tot));
     while (!s->queue.empty() && (int)(s->active.size() + admitted.size()) < s->max_slots) {
         SrvReq* r = s->reqs[s->queue.front()].get();
         if (s->used + r->bytes > (size_t)s->budget || r->bytes + (256ul << 20) > fr) break;

@@ -94,12 +94,8 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::ty
     tile_rows<T>(S, segb, sm, pos, r2, lo_thr, hi_thr, nbr, nn, stride, max_nn, err, nn_max);
 }
 
-// List build in three passes of one z-layer each (rows 0-2, 3-5, 6-8 of the tile:
-// segments 0-5, 6-11, 12-17), staged one after the other into the same shared
-// memory with a third of the full staging (more resident CTAs).  A particle's
-// entry count and pending half-word carry over the passes, so its row holds the
-// entries in the same order as the single-pass walk; entries are indices into
-// the full staging layout, which the pair kernels stage.
+// List build in three passes of one z-layer each (tile_rows_layers in
+// pd_tile_dev.cuh): a third of the full staging, more resident CTAs.
 template <class T>
 __global__ void __launch_bounds__(TBLOCK) k_vtile_build3(const typename V4<T>::type* __restrict__ pos,
                                                          const float4* __restrict__ pos32, long n_real,
@@ -117,102 +113,11 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build3(const typename V4<T>::t
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     if (ib == ie) return;
     tile_segb(S, segb);
-    const int ncol = S.ncol, nc = ncol - 1;
     if (threadIdx.x == 0) mbar_init(&S.bar, 1);
     __syncthreads();
-    const unsigned int self_base = S.oR[4] - S.cR[4][0];
-    const float4* pimg = pos32 + n_real;
-    // each thread: one domain particle per 128 (the tile's particles in order)
-    constexpr int MAXI = 2;  // domain particles per thread (tiles of up to 256)
-    float4 xi[MAXI];
-    unsigned int ph = 0;  // completed phases of the barrier (layers with records)
-    int jcol[MAXI], cnt[MAXI];
-    unsigned int pend[MAXI];
-    int nmine = 0;
-    for (unsigned int i = ib + threadIdx.x; i < ie && nmine < MAXI; i += blockDim.x, ++nmine) {
-        xi[nmine] = pos32[i];
-        int j = 1;
-        while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
-        jcol[nmine] = j;
-        cnt[nmine] = 0;
-        pend[nmine] = 0;
-    }
-    if (ie - ib > (unsigned int)(MAXI * blockDim.x)) {
-        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
-        return;
-    }
-    for (int pass = 0; pass < 3; ++pass) {
-        const unsigned int base = S.oR[3 * pass];
-        const unsigned int end = pass < 2 ? S.oR[3 * pass + 3] : S.total;
-        const unsigned int tot = end - base;
-        if (tot > pcap) {
-            if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
-            return;
-        }
-        bool ok = true;
-        if (tot > 0) {
-            if (threadIdx.x == 0) {
-                mbar_arrive_expect_tx(&S.bar, tot * (unsigned int)sizeof(float4));
-                for (int r = 3 * pass; r < 3 * pass + 3; ++r) {
-                    unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-                    if (lr) bulk_g2s(sm + (S.oR[r] - base), pos32 + S.cR[r][0], lr * (unsigned int)sizeof(float4), &S.bar);
-                    unsigned int li = S.cI[r][nc] - S.cI[r][0];
-                    if (li) bulk_g2s(sm + (S.oI[r] - base), pimg + S.cI[r][0], li * (unsigned int)sizeof(float4), &S.bar);
-                }
-            }
-            ok = mbar_wait_bounded(&S.bar, ph & 1u, 1u << 24);
-            if (!ok) {
-                atomicOr(err, ERR_TIMEOUT);
-                mbar_wait_bounded(&S.bar, ph & 1u, 1u << 24);
-            }
-            ++ph;
-        }
-        if (!__syncthreads_and(ok ? 1 : 0)) return;
-        for (int m = 0; m < nmine; ++m) {
-            const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
-            const int j = jcol[m];
-            const float4 x = xi[m];
-            int c = cnt[m];
-            unsigned int pd_ = pend[m];
-            unsigned int* out = nbr + i;
-#pragma unroll 1
-            for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg) {
-                const unsigned int qe = segb[sg][j + 2];
-#pragma unroll 4
-                for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
-                    const float4 xq = sm[q - base];
-                    const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
-                    if (d2 < hi_thr) {
-                        if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
-                            if (c < max_nn) {
-                                if (c & 1) out[(long)(c >> 1) * stride] = pd_ | (q << 16);
-                                else pd_ = q;
-                            }
-                            c++;
-                        }
-                    }
-                }
-            }
-            cnt[m] = c;
-            pend[m] = pd_;
-        }
-        // every thread is done with this layer before the next one is copied over it
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-    }
-    for (int m = 0; m < nmine; ++m) {
-        const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
-        int c = cnt[m];
-        unsigned int* out = nbr + i;
-        // odd rows end with the particle itself, which the pair kernel skips
-        if ((c & 1) && c < max_nn) out[(long)(c >> 1) * stride] = pend[m] | ((self_base + i) << 16);
-        if (c > max_nn) {
-            atomicOr(err, ERR_NN_OVERFLOW);
-            atomicMax(nn_max, (unsigned int)c);
-            c = max_nn;
-        }
-        nn[i] = c;
-    }
+    unsigned int ph = 0;
+    tile_rows_layers<T>(S, segb, pos32, pos32 + n_real, sm, pcap, pos, r2, lo_thr, hi_thr, nbr, nn, stride, max_nn,
+                        err, nn_max, &S.bar, ph);
 }
 
 // P threads per domain particle split its row (words w = sub, sub+P, ...; two
