@@ -55,6 +55,11 @@ extern "C" {
 #define PD_CL_GPU_REORDER_PROPERTY 128
 #define PD_CL_GPU_REORDER (PD_CL_GPU_REORDER_POSITION | PD_CL_GPU_REORDER_PROPERTY)
 
+/* ghost_put merge operations (add_, max_, replace_ of the reference) */
+#define PD_PUT_ADD 1
+#define PD_PUT_MAX 2
+#define PD_PUT_REPLACE 3
+
 /* reductions (reduce_local<prp,_add_/_max_>) */
 #define PD_RED_ADD 1
 #define PD_RED_MAX 2
@@ -169,6 +174,12 @@ int pd_map(pd_vd h, int opt, void* stream);
 int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream);
 /* the (source, shift id) record of every ghost (o_part_loc) */
 int pd_ghost_records(pd_vd h, int* src, int* shift_id, long cap, long* n_img);
+/* ghost_put<op, prp...>(opt) on one process -- vector_dist.hpp:2304-2310 ->
+ * vector_dist_comm.hpp:2086-2182 (local part merge_prp_v): the values of every
+ * ghost are merged onto its source with op (PD_PUT_ADD / _MAX / _REPLACE), the
+ * ghosts of a source in image order.  Needs the images of the last ghost_get
+ * (PD_ESTATE otherwise).  prop_mask: bit p = property p. */
+int pd_ghost_put(pd_vd h, unsigned long prop_mask, int op, void* stream);
 /* explicit box-list image kernels, the reference's num_shift_ghost_each_part +
  * scan + shift_ghost_each_part (vector_dist_cuda_funcs.cuh:157-233) on caller
  * data: boxes [nb][2][3] (lo, hi), sv[nb] shift ids sorted ascending, shifts[..][3].
@@ -226,6 +237,12 @@ int pd_celllist_build_static(int dtype, const void* pos_xyz, long n, const doubl
  * over domain + ghost within r_cut (self included), built from a cell list of
  * side r_cut on the domain enlarged by the ghost magnified 1.013. */
 int pd_verlet_create(pd_vd h, double r_cut, pd_vl* out);
+/* getVerletSym(r_cut) -- vector_dist.hpp:1412-1416: symmetric (half) list, each
+ * interacting pair once: a domain partner q of p iff q > p, a ghost iff it lies
+ * after p in (x, y, z) lexicographic order (the mirror pair across the periodic
+ * boundary is then kept by the other particle).  Forces from it (pd_lj_forces)
+ * land on ghosts too; pd_ghost_put(PD_PUT_ADD) folds them onto their sources. */
+int pd_verlet_create_sym(pd_vd h, double r_cut, pd_vl* out);
 int pd_verlet_destroy(pd_vl vl);
 /* updateVerlet(vl, r_cut) -- vector_dist.hpp:1556-1620 */
 int pd_verlet_update(pd_vd h, pd_vl vl, void* stream);

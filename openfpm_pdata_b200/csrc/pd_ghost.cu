@@ -123,6 +123,29 @@ __global__ void k_ghost_replay(typename V4<T>::type* __restrict__ pos, long n, c
     }
 }
 
+// ghost_put<op, prp...> on one process (vector_dist_comm.hpp:2086-2182, the local
+// part merge_prp_v): every image's value is merged onto its source in image
+// order -- the images of a source are consecutive (generation order), so one
+// thread per source applies them in that order and the result is deterministic.
+template <class E>
+__global__ void k_ghost_put(E* __restrict__ a, long cap, int ncomp, long n, const unsigned int* __restrict__ start,
+                            const unsigned int* __restrict__ cnt, int op) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+        const unsigned int m = cnt[p];
+        if (m == 0) continue;
+        const long base = n + (long)start[p];
+        for (int c = 0; c < ncomp; ++c) {
+            E* col = a + (long)c * cap;
+            E acc = col[p];
+            for (unsigned int j = 0; j < m; ++j) {
+                const E v = col[base + j];
+                acc = op == PD_PUT_ADD ? acc + v : (op == PD_PUT_MAX ? (v > acc ? v : acc) : v);
+            }
+            col[p] = acc;
+        }
+    }
+}
+
 static PropCopy make_copy(pd_vd h, unsigned long mask) {
     PropCopy pc;
     memset(&pc, 0, sizeof(pc));
@@ -260,6 +283,7 @@ int ghost_generate(pd_vd h, long img_cap, bool sync_count, cudaStream_t st) {
         h->n_img = h->ctrl_h->n_img;
         h->n_total = n + h->n_img;
         h->img_valid = true;
+        h->img_gen_order = true;
     }
     return PD_OK;
 }
@@ -325,6 +349,33 @@ int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream) {
         return PD_EOVERFLOW;
     }
     h->epoch++;
+    return PD_OK;
+}
+
+int pd_ghost_put(pd_vd h, unsigned long prop_mask, int op, void* stream) {
+    if (!h || (op != PD_PUT_ADD && op != PD_PUT_MAX && op != PD_PUT_REPLACE)) return PD_EINVAL;
+    if (!h->img_valid || !h->img_gen_order) {
+        set_error("ghost_put: no ghost_get images in generation order (call ghost_get first)");
+        return PD_ESTATE;
+    }
+    cudaStream_t st = S(stream);
+    const long n = h->n_real;
+    if (n == 0 || h->n_img == 0) return PD_OK;
+    const unsigned g = grid_for(n, 256);
+    const unsigned int* start = h->img_start.as<unsigned int>();
+    const unsigned int* cnt = h->img_cnt.as<unsigned int>();
+    for (size_t p = 0; p < h->props.size(); ++p) {
+        if (!(prop_mask & (1ul << p))) continue;
+        Prop& P = h->props[p];
+        switch (P.type) {
+            case PD_F64: pd::launch(k_ghost_put<double>, g, 256, 0, st, (double*)P.d, h->cap, P.ncomp, n, start, cnt, op); break;
+            case PD_F32: pd::launch(k_ghost_put<float>, g, 256, 0, st, (float*)P.d, h->cap, P.ncomp, n, start, cnt, op); break;
+            case PD_I32: pd::launch(k_ghost_put<int>, g, 256, 0, st, (int*)P.d, h->cap, P.ncomp, n, start, cnt, op); break;
+            case PD_U32: pd::launch(k_ghost_put<unsigned int>, g, 256, 0, st, (unsigned int*)P.d, h->cap, P.ncomp, n, start, cnt, op); break;
+            case PD_I64: pd::launch(k_ghost_put<long long>, g, 256, 0, st, (long long*)P.d, h->cap, P.ncomp, n, start, cnt, op); break;
+        }
+        PD_LAUNCH_CHECK();
+    }
     return PD_OK;
 }
 

@@ -140,6 +140,7 @@ struct pd_vd_s {
     int nbox = 0;
     long n_img = 0;
     bool img_valid = false;
+    bool img_gen_order = false;  // images in generation order (ghost_put can fold them)
     pd::Ctrl* ctrl = nullptr;    // device
     pd::Ctrl* ctrl_h = nullptr;  // pinned host mirror
     pd::Buf scan_scratch, tmp, tmp2, red;
@@ -173,6 +174,7 @@ struct pd_vl_s {
     int max_nn = 0;
     long n_dom = 0;
     long epoch = -1;
+    bool sym = false;  // half list (VL_SYMMETRIC): each pair once, see verlet_build
 };
 
 // ---------------------------------------------------------------------------

@@ -54,6 +54,51 @@ __global__ void __launch_bounds__(FBLOCK) k_lj_verlet(const typename V4<T>::type
     }
 }
 
+// LJ from a symmetric (half) Verlet list: each pair once, the reaction added to
+// the partner (a domain particle or a periodic image) with atomics; image forces
+// are folded onto their sources by ghost_put<add_>.  Energies count each pair
+// once.  The forces must be zero on entry (domain and images).
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_lj_verlet_sym(const typename V4<T>::type* __restrict__ pos, long n,
+                                                          const int* __restrict__ nbr, const int* __restrict__ nn,
+                                                          long stride, LJP<T> P, T* __restrict__ f, long fcap,
+                                                          double* __restrict__ part) {
+    double pe = 0, vir = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        typename V4<T>::type xi = ld4(pos, i);
+        int m = nn[i];
+        T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
+        const int* row = nbr + i;
+        for (int k = 0; k < m; ++k) {
+            int q = __ldg(row + (long)k * stride);
+            typename V4<T>::type xq = ld4(pos, q);
+            T dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
+            T r2 = dist2(dx, dy, dz);
+            if (r2 < P.rc2 && q != (int)i) {
+                T gx = 0, gy = 0, gz = 0;
+                lj_acc(P, r2, dx, dy, dz, gx, gy, gz, e, w);
+                fx += gx;
+                fy += gy;
+                fz += gz;
+                atomicAdd(f + q, -gx);
+                atomicAdd(f + fcap + q, -gy);
+                atomicAdd(f + 2 * fcap + q, -gz);
+            }
+        }
+        atomicAdd(f + i, fx);
+        atomicAdd(f + fcap + i, fy);
+        atomicAdd(f + 2 * fcap + i, fz);
+        pe += (double)e;
+        vir += (double)w;
+    }
+    pe = block_sum<double, FBLOCK>(pe);
+    vir = block_sum<double, FBLOCK>(vir);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = pe;
+        part[2 * blockIdx.x + 1] = vir;
+    }
+}
+
 // LJ through the cell list (27-cell walk over the cell-ordered positions pcs,
 // whose 4th word holds the original index)
 template <class T> struct IdxDec;
@@ -300,7 +345,19 @@ static int lj_launch(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t& lj, int 
     Prop& F = h->props[force_prop];
     long n = h->n_real;
     if (vl) {
-        if (h->dtype == PD_F64)
+        if (vl->sym) {
+            // forces of domain particles and images start at zero (the images receive reactions)
+            for (int c = 0; c < 3; ++c)
+                PD_CUDA(cudaMemsetAsync(F.d + (size_t)c * h->cap * F.esize, 0, (size_t)h->n_total * F.esize, st));
+            if (h->dtype == PD_F64)
+                pd::launch(k_lj_verlet_sym<double>, nblk, FBLOCK, 0, st, (const double4*)h->pos, n,
+                           (const int*)vl->nbr.as<int>(), (const int*)vl->nn.as<int>(), vl->stride, ljp<double>(lj),
+                           (double*)F.d, h->cap, part);
+            else
+                pd::launch(k_lj_verlet_sym<float>, nblk, FBLOCK, 0, st, (const float4*)h->pos, n,
+                           (const int*)vl->nbr.as<int>(), (const int*)vl->nn.as<int>(), vl->stride, ljp<float>(lj),
+                           (float*)F.d, h->cap, part);
+        } else if (h->dtype == PD_F64)
             pd::launch(k_lj_verlet<double>, nblk, FBLOCK, 0, st, (const double4*)h->pos, n, vl->nbr.as<int>(),
                                                          vl->nn.as<int>(), vl->stride, ljp<double>(lj), (double*)F.d,
                                                          h->cap, part);
@@ -352,6 +409,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     long m = h->n_img, n = h->n_real;
     PD_TRY(cl_build(h, cl, m, nullptr, st, n));
     PD_CUDA(cudaMemcpyAsync(md->csI.p, cl->cell_start.p, sizeof(unsigned int) * nc1, cudaMemcpyDeviceToDevice, st));
+    h->img_gen_order = false;  // the images are sorted into cell order below
     if (m > 0) {
         const int* ids = cl->sorted.as<int>();
         size_t need = std::max((size_t)m * h->pos_bytes, (size_t)m * sizeof(int));
@@ -566,6 +624,7 @@ static int md_run_cl_graph(pd_md md, int steps, cudaStream_t st, double* E) {
     h->n_img = h->ctrl_h->n_img;
     h->n_total = h->n_real + h->n_img;
     h->img_valid = true;
+    h->img_gen_order = false;  // the step may leave the images in cell order
     if (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW | ERR_CAP_OVERFLOW)) {
         set_error("pd_md_run: device capacity overflow (err=0x%x)", h->ctrl_h->err);
         return PD_EOVERFLOW;

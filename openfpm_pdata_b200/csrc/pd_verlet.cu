@@ -14,6 +14,15 @@
 //      order), writing column-major rows nbr[k*stride + i].
 // Rows longer than the capacity set ERR_NN_OVERFLOW and record the longest row;
 // the host grows the capacity and rebuilds.
+//
+// Symmetric (half) list, getVerletSym (vector_dist.hpp:1412-1416): each
+// interacting pair once.  A domain partner q is kept by p iff q > p; a periodic
+// image is kept iff it lies after p in the lexicographic (x, y, z) order.  The
+// mirror of a pair (p, image of r) is (r, image of p), shifted by the opposite
+// vector, so exactly one of the two is kept; forces or counts accumulated on an
+// image are folded onto its source by ghost_put<add_> (vector_dist.hpp:2304).
+// The criterion is geometric, not cell-based, so it does not depend on the box
+// being a whole number of cells.
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
 
@@ -44,11 +53,16 @@ __global__ void k_gather_cs(const typename V4<T>::type* __restrict__ pos, const 
     }
 }
 
+template <class T4> __device__ __forceinline__ bool lex_after(const T4& a, const T4& b) {
+    return a.x > b.x || (a.x == b.x && (a.y > b.y || (a.y == b.y && a.z > b.z)));
+}
+
 template <class T>
 __global__ void __launch_bounds__(128) k_verlet_tile(const typename V4<T>::type* __restrict__ pcs, Grid<T> G, int TX,
                                                      int ntx, const unsigned int* __restrict__ cs, long n_dom, T r2,
                                                      int* __restrict__ nbr, int* __restrict__ nn, long stride,
-                                                     int max_nn, int smem_cap, unsigned int* __restrict__ ctrl_err,
+                                                     int max_nn, int smem_cap, int sym,
+                                                     unsigned int* __restrict__ ctrl_err,
                                                      unsigned int* __restrict__ ctrl_nnmax) {
     typedef typename V4<T>::type T4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -113,7 +127,9 @@ __global__ void __launch_bounds__(128) k_verlet_tile(const typename V4<T>::type*
                 T4 xq = base[q];
                 T d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
                 if (d2 < r2) {
-                    if (cnt < max_nn) nbr[(long)cnt * stride + i] = IdxBits<T>::dec(xq.w);
+                    const int qi = IdxBits<T>::dec(xq.w);
+                    if (sym && !(qi < n_dom ? qi > i : lex_after(xq, xi))) continue;
+                    if (cnt < max_nn) nbr[(long)cnt * stride + i] = qi;
                     cnt++;
                 }
             }
@@ -198,8 +214,8 @@ int verlet_build(pd_vd h, pd_vl vl, long n_dom, const unsigned int* n_img_dev, c
                         return G;
                     }(),
                     TX, ntx, cl->cell_start.as<unsigned int>(), n_dom, (double)(vl->r_cut * vl->r_cut),
-                    vl->nbr.as<int>(), vl->nn.as<int>(), stride, vl->max_nn, smem_cap, &h->ctrl->err,
-                    &h->ctrl->nn_max);
+                    vl->nbr.as<int>(), vl->nn.as<int>(), stride, vl->max_nn, smem_cap, vl->sym ? 1 : 0,
+                    &h->ctrl->err, &h->ctrl->nn_max);
             } else {
                 static bool attr = false;
                 if (!attr) {
@@ -219,7 +235,7 @@ int verlet_build(pd_vd h, pd_vl vl, long n_dom, const unsigned int* n_img_dev, c
                         return G;
                     }(),
                     TX, ntx, cl->cell_start.as<unsigned int>(), n_dom, rc * rc, vl->nbr.as<int>(), vl->nn.as<int>(),
-                    stride, vl->max_nn, smem_cap, &h->ctrl->err, &h->ctrl->nn_max);
+                    stride, vl->max_nn, smem_cap, vl->sym ? 1 : 0, &h->ctrl->err, &h->ctrl->nn_max);
             }
             PD_LAUNCH_CHECK();
         }
@@ -256,6 +272,12 @@ int pd_verlet_create(pd_vd h, double r_cut, pd_vl* out) {
     }
     *out = vl;
     return PD_OK;
+}
+
+int pd_verlet_create_sym(pd_vd h, double r_cut, pd_vl* out) {
+    int r = pd_verlet_create(h, r_cut, out);
+    if (r == PD_OK) (*out)->sym = true;
+    return r;
 }
 
 int pd_verlet_destroy(pd_vl vl) {

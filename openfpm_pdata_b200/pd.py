@@ -25,6 +25,7 @@ CL_NON_SYMMETRIC = 2
 CL_GPU_REORDER_POSITION, CL_GPU_REORDER_PROPERTY = 64, 128
 CL_GPU_REORDER = CL_GPU_REORDER_POSITION | CL_GPU_REORDER_PROPERTY
 RED_ADD, RED_MAX = 1, 2
+PUT_ADD, PUT_MAX, PUT_REPLACE = 1, 2, 3
 
 _NP = {PD_F32: np.float32, PD_F64: np.float64, PD_I32: np.int32, PD_U32: np.uint32, PD_I64: np.int64}
 _CODES = {-1: "PD_EINVAL", -2: "PD_ENOMEM", -3: "PD_ECUDA", -4: "PD_ESTALE", -5: "PD_ETIMEOUT",
@@ -116,6 +117,8 @@ def lib():
             "pd_celllist_get": ([vp, vp, vp, vp], ip),
             "pd_test_force": ([vp, vp, ip, ip, ip, vp], ip),
             "pd_verlet_create": ([vp, ctypes.c_double, P(vp)], ip),
+            "pd_verlet_create_sym": ([vp, ctypes.c_double, P(vp)], ip),
+            "pd_ghost_put": ([vp, ctypes.c_ulong, ip, vp], ip),
             "pd_verlet_destroy": ([vp], ip),
             "pd_verlet_update": ([vp, vp, vp], ip),
             "pd_verlet_get": ([vp, vp, vp, lp, vp], ip),
@@ -224,10 +227,12 @@ class CellList:
 class VerletList:
     """VerletList handle (getVerlet / updateVerlet)."""
 
-    def __init__(self, vd, r_cut):
+    def __init__(self, vd, r_cut, sym=False):
         self.vd = vd
+        self.sym = bool(sym)
         h = ctypes.c_void_p()
-        check(lib().pd_verlet_create(vd.h, float(r_cut), ctypes.byref(h)))
+        create = lib().pd_verlet_create_sym if sym else lib().pd_verlet_create
+        check(create(vd.h, float(r_cut), ctypes.byref(h)))
         self.h = h
 
     def get(self):
@@ -329,6 +334,11 @@ class VectorDist:
         mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
         check(lib().pd_ghost_get(self.h, ctypes.c_ulong(mask), int(opt), None))
 
+    def ghost_put(self, props=None, op=PUT_ADD):
+        """ghost_put<op_, prp...>(): merge every ghost's values onto its source."""
+        mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
+        check(lib().pd_ghost_put(self.h, ctypes.c_ulong(mask), int(op), None))
+
     def ghost_records(self):
         n = ctypes.c_long(0)
         check(lib().pd_ghost_records(self.h, None, None, 0, ctypes.byref(n)))
@@ -383,6 +393,11 @@ class VectorDist:
 
     def getVerlet(self, r_cut):
         vl = VerletList(self, r_cut)
+        check(lib().pd_verlet_update(self.h, vl.h, None))
+        return vl
+
+    def getVerletSym(self, r_cut):
+        vl = VerletList(self, r_cut, sym=True)
         check(lib().pd_verlet_update(self.h, vl.h, None))
         return vl
 
