@@ -49,7 +49,11 @@ extern "C" {
 #define PD_KEEP_PROPERTIES 512
 #define PD_RUN_ON_DEVICE 1024
 
-/* cell-list options (CL_* of openfpm_data; values are this library's own) */
+/* cell-list options (CL_* of openfpm_data; values are this library's own).
+ * PD_CL_SYMMETRIC: getCellListSym (vector_dist.hpp:1062-1066) -- pair kernels
+ * through it visit each pair once and put the reaction on the partner, ghosts
+ * included; pd_ghost_put(PD_PUT_ADD) folds the ghosts' share onto the sources. */
+#define PD_CL_SYMMETRIC 1
 #define PD_CL_NON_SYMMETRIC 2
 #define PD_CL_GPU_REORDER_POSITION 64
 #define PD_CL_GPU_REORDER_PROPERTY 128
@@ -59,6 +63,14 @@ extern "C" {
 #define PD_PUT_ADD 1
 #define PD_PUT_MAX 2
 #define PD_PUT_REPLACE 3
+
+/* comparisons of pd_get_indexes_by_type (the functor::check of the reference) */
+#define PD_CMP_EQ 0
+#define PD_CMP_NE 1
+#define PD_CMP_LT 2
+#define PD_CMP_LE 3
+#define PD_CMP_GT 4
+#define PD_CMP_GE 5
 
 /* reductions (reduce_local<prp,_add_/_max_>) */
 #define PD_RED_ADD 1
@@ -194,6 +206,19 @@ int pd_view(pd_vd h, pd_view_t* out);
 int pd_domain_iterator(pd_vd h, int n_thr, int with_ghost, pd_launch_t* out);
 /* reduce_local<prp,_add_/_max_> -- vector_dist_cuda_funcs.cuh:247-270 (component `comp`) */
 int pd_reduce(pd_vd h, int prop, int comp, int op, void* stream, double* out);
+/* remove_marked<prp>(vd) -- vector_dist_cuda_funcs.cuh:333-412: removes the
+ * domain particles whose property `prop` (component 0; int, unsigned, float,
+ * double or int64) is non-zero, keeping the order of the others, and drops the
+ * ghosts.  Destructive on `prop` like the reference: it holds 1 on the kept
+ * particles afterwards (and on every particle when none was marked). */
+int pd_remove_marked(pd_vd h, int prop, void* stream);
+/* get_indexes_by_type<prp, functor>(vd, ids, end, ctx) -- vector_dist_cuda_funcs.cuh:449-481:
+ * the ascending indexes p < end (end < 0: the domain size) whose property `prop`
+ * (component 0) compares `cmp` (PD_CMP_*) to `value` -- the functor::check of the
+ * reference as a comparison.  `ids` (device or host memory, room for `cap`)
+ * receives them; *n_out their count (PD_EOVERFLOW if above cap). */
+int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end, unsigned int* ids, long cap,
+                           long* n_out, void* stream);
 /* the original index of every particle in its current storage slot */
 int pd_d2h_gid(pd_vd h, long* host, long offset, long count, void* stream);
 

@@ -1,0 +1,208 @@
+// Stream compaction of the domain particles: remove_marked and get_indexes_by_type
+// (Vector/cuda/vector_dist_cuda_funcs.cuh:313-481).
+//
+// remove_marked<prp>: the mark property is flipped in place (x -> x == 0, the
+// reference's destructive step, flip_one_to_zero :313-321), the flipped flags are
+// scanned, and every kept particle (mark 0 before the flip) is scattered, in
+// order, with its position, global id and all properties (copy_new_to_old_by_scan
+// :295-311).  The ghosts are dropped: the vector then holds the kept particles
+// only (setGhostMarker(kept), :406).  When nothing is marked the vector keeps its
+// particles and the flipped mark (:366-372).
+//
+// The scatter writes all columns of one particle in one thread (a column table
+// passed by value), into one scratch block; one device-to-device copy per column
+// then brings the compacted columns back, so the arrays keep their addresses.
+//
+// get_indexes_by_type<prp, functor>: flag p < end whose property satisfies the
+// comparison (mark_indexes :414-423), scan, and write p at its scan offset
+// (fill_indexes :425-438): the indexes come out ascending.
+#include "pd_device.cuh"
+#include "pd_internal.cuh"
+
+namespace pd {
+
+static constexpr int CMAXC = 24;  // columns per scatter launch
+
+struct ColSet {
+    int nc;
+    const unsigned char* src[CMAXC];
+    unsigned char* dst[CMAXC];
+    int wsize[CMAXC];  // bytes per element: 4, 8, 16 or 32
+};
+
+template <class E>
+__global__ void k_flip_mark(E* __restrict__ m, long n, unsigned int* __restrict__ keep) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const bool k = (m[i] == E(0));
+        m[i] = k ? E(1) : E(0);
+        keep[i] = k ? 1u : 0u;
+    }
+}
+
+__global__ void k_compact_scatter(ColSet C, long n, const unsigned int* __restrict__ keep,
+                                  const unsigned int* __restrict__ off) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (!keep[i]) continue;
+        const long d = off[i];
+        for (int c = 0; c < C.nc; ++c) {
+            switch (C.wsize[c]) {
+                case 4: ((unsigned int*)C.dst[c])[d] = ((const unsigned int*)C.src[c])[i]; break;
+                case 8: ((unsigned long long*)C.dst[c])[d] = ((const unsigned long long*)C.src[c])[i]; break;
+                case 16: ((uint4*)C.dst[c])[d] = ((const uint4*)C.src[c])[i]; break;
+                default: {
+                    const uint4* s = (const uint4*)C.src[c] + 2 * i;
+                    uint4* t = (uint4*)C.dst[c] + 2 * d;
+                    t[0] = s[0];
+                    t[1] = s[1];
+                }
+            }
+        }
+    }
+}
+
+template <class E>
+__device__ __forceinline__ bool cmp_ok(E v, E ref, int cmp) {
+    switch (cmp) {
+        case PD_CMP_EQ: return v == ref;
+        case PD_CMP_NE: return v != ref;
+        case PD_CMP_LT: return v < ref;
+        case PD_CMP_LE: return v <= ref;
+        case PD_CMP_GT: return v > ref;
+        default: return v >= ref;
+    }
+}
+
+template <class E>
+__global__ void k_mark_indexes(const E* __restrict__ a, long n, E ref, int cmp, unsigned int* __restrict__ flag) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        flag[i] = cmp_ok(a[i], ref, cmp) ? 1u : 0u;
+}
+
+__global__ void k_fill_indexes(const unsigned int* __restrict__ flag, const unsigned int* __restrict__ off, long n,
+                               unsigned int* __restrict__ ids) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        if (flag[i]) ids[off[i]] = (unsigned int)i;
+}
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace pd
+
+using namespace pd;
+
+extern "C" {
+
+int pd_remove_marked(pd_vd h, int prop, void* stream) {
+    if (!h || prop < 0 || prop >= (int)h->props.size()) return PD_EINVAL;
+    const Prop& M = h->props[prop];
+    cudaStream_t st = S(stream);
+    const long n = h->n_real;
+    if (n == 0) return PD_OK;
+    if (n >= (1L << 32)) return PD_EINVAL;
+    // flags and offsets
+    PD_TRY(h->tmp2.ensure(sizeof(unsigned int) * 2 * (size_t)n));
+    unsigned int* keep = h->tmp2.as<unsigned int>();
+    unsigned int* off = keep + n;
+    const unsigned g = grid_for(n, 256);
+    switch (M.type) {
+        case PD_F64: pd::launch(k_flip_mark<double>, g, 256, 0, st, (double*)M.d, n, keep); break;
+        case PD_F32: pd::launch(k_flip_mark<float>, g, 256, 0, st, (float*)M.d, n, keep); break;
+        case PD_I32: pd::launch(k_flip_mark<int>, g, 256, 0, st, (int*)M.d, n, keep); break;
+        case PD_U32: pd::launch(k_flip_mark<unsigned int>, g, 256, 0, st, (unsigned int*)M.d, n, keep); break;
+        case PD_I64: pd::launch(k_flip_mark<long long>, g, 256, 0, st, (long long*)M.d, n, keep); break;
+        default: return PD_EINVAL;
+    }
+    PD_LAUNCH_CHECK();
+    PD_TRY(scan_u32(keep, off, n, &h->ctrl->n_keep, h->scan_scratch, st));
+    PD_CUDA(cudaMemcpyAsync(&h->ctrl_h->n_keep, &h->ctrl->n_keep, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    PD_CUDA(cudaStreamSynchronize(st));
+    const long k = h->ctrl_h->n_keep;
+    if (k == n) return PD_OK;  // nothing marked: the particles stay, the mark stays flipped
+    if (k > 0) {
+        // columns: positions, global ids, every component of every property
+        struct Col {
+            unsigned char* a;
+            int w;
+        };
+        std::vector<Col> cols;
+        cols.push_back({(unsigned char*)h->pos, h->pos_bytes});
+        cols.push_back({(unsigned char*)h->gid, (int)sizeof(int)});
+        for (auto& P : h->props)
+            for (int c = 0; c < P.ncomp; ++c) cols.push_back({(unsigned char*)P.d + (size_t)c * h->cap * P.esize, P.esize});
+        for (size_t c0 = 0; c0 < cols.size(); c0 += CMAXC) {
+            const size_t c1 = std::min(cols.size(), c0 + (size_t)CMAXC);
+            size_t bytes = 0;
+            for (size_t c = c0; c < c1; ++c) bytes += align_up((size_t)k * cols[c].w);
+            PD_TRY(h->tmp.ensure(bytes));
+            ColSet C;
+            memset(&C, 0, sizeof(C));
+            C.nc = (int)(c1 - c0);
+            size_t o = 0;
+            for (size_t c = c0; c < c1; ++c) {
+                C.src[c - c0] = cols[c].a;
+                C.dst[c - c0] = h->tmp.as<unsigned char>() + o;
+                C.wsize[c - c0] = cols[c].w;
+                o += align_up((size_t)k * cols[c].w);
+            }
+            pd::launch(k_compact_scatter, g, 256, 0, st, C, n, (const unsigned int*)keep, (const unsigned int*)off);
+            PD_LAUNCH_CHECK();
+            for (int c = 0; c < C.nc; ++c)
+                PD_CUDA(cudaMemcpyAsync((void*)C.src[c], C.dst[c], (size_t)k * C.wsize[c], cudaMemcpyDeviceToDevice,
+                                        st));
+        }
+    }
+    h->n_real = h->n_total = k;
+    h->n_img = 0;
+    h->img_valid = false;
+    h->epoch++;
+    return PD_OK;
+}
+
+int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end, unsigned int* ids, long cap,
+                           long* n_out, void* stream) {
+    if (!h || !n_out || prop < 0 || prop >= (int)h->props.size() || cmp < PD_CMP_EQ || cmp > PD_CMP_GE || cap < 0)
+        return PD_EINVAL;
+    const Prop& P = h->props[prop];
+    cudaStream_t st = S(stream);
+    long n = end < 0 ? h->n_real : std::min(end, h->n_total);
+    *n_out = 0;
+    if (n <= 0) return PD_OK;
+    if (n >= (1L << 32)) return PD_EINVAL;
+    PD_TRY(h->tmp2.ensure(sizeof(unsigned int) * 3 * (size_t)n));
+    unsigned int* flag = h->tmp2.as<unsigned int>();
+    unsigned int* off = flag + n;
+    unsigned int* out = off + n;
+    const unsigned g = grid_for(n, 256);
+    switch (P.type) {
+        case PD_F64: pd::launch(k_mark_indexes<double>, g, 256, 0, st, (const double*)P.d, n, (double)value, cmp, flag); break;
+        case PD_F32: pd::launch(k_mark_indexes<float>, g, 256, 0, st, (const float*)P.d, n, (float)value, cmp, flag); break;
+        case PD_I32: pd::launch(k_mark_indexes<int>, g, 256, 0, st, (const int*)P.d, n, (int)value, cmp, flag); break;
+        case PD_U32:
+            pd::launch(k_mark_indexes<unsigned int>, g, 256, 0, st, (const unsigned int*)P.d, n, (unsigned int)value,
+                       cmp, flag);
+            break;
+        case PD_I64: pd::launch(k_mark_indexes<long long>, g, 256, 0, st, (const long long*)P.d, n, value, cmp, flag); break;
+        default: return PD_EINVAL;
+    }
+    PD_LAUNCH_CHECK();
+    PD_TRY(scan_u32(flag, off, n, &h->ctrl->n_keep, h->scan_scratch, st));
+    pd::launch(k_fill_indexes, g, 256, 0, st, (const unsigned int*)flag, (const unsigned int*)off, n, out);
+    PD_LAUNCH_CHECK();
+    PD_CUDA(cudaMemcpyAsync(&h->ctrl_h->n_keep, &h->ctrl->n_keep, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    PD_CUDA(cudaStreamSynchronize(st));
+    const long m = h->ctrl_h->n_keep;
+    *n_out = m;
+    if (m > cap) {
+        set_error("get_indexes_by_type: %ld indexes, room for %ld", m, cap);
+        return PD_EOVERFLOW;
+    }
+    if (m > 0) {
+        if (!ids) return PD_EINVAL;
+        // ids may be device or host memory (unified addressing)
+        PD_CUDA(cudaMemcpyAsync(ids, out, sizeof(unsigned int) * m, cudaMemcpyDefault, st));
+        PD_CUDA(cudaStreamSynchronize(st));
+    }
+    return PD_OK;
+}
+
+}  // extern "C"

@@ -55,6 +55,7 @@ struct Ctrl {
     unsigned int tile_max;         // largest staged neighbourhood of a tile (records)
     unsigned int tile_center_max;  // largest number of domain particles of a tile
     unsigned int tile_pass_max;    // largest staged z-layer (3 rows) of a tile (records)
+    unsigned int n_keep;           // count of the last compaction / index selection
 };
 
 // Allocation context: inside an AllocScope, device allocations of the library are

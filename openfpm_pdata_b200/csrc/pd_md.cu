@@ -54,6 +54,11 @@ __global__ void __launch_bounds__(FBLOCK) k_lj_verlet(const typename V4<T>::type
     }
 }
 
+// the half-list pair rule: an image is kept iff it lies after p in (x, y, z) order
+template <class T4> __device__ __forceinline__ bool lex_after(const T4& a, const T4& b) {
+    return a.x > b.x || (a.x == b.x && (a.y > b.y || (a.y == b.y && a.z > b.z)));
+}
+
 // LJ from a symmetric (half) Verlet list: each pair once, the reaction added to
 // the partner (a domain particle or a periodic image) with atomics; image forces
 // are folded onto their sources by ghost_put<add_>.  Energies count each pair
@@ -113,8 +118,10 @@ template <class T>
 __global__ void __launch_bounds__(FBLOCK) k_lj_cell(const typename V4<T>::type* __restrict__ pos, long n,
                                                     const typename V4<T>::type* __restrict__ pcs,
                                                     const unsigned int* __restrict__ cs, Grid<T> G, LJP<T> P,
-                                                    T* __restrict__ f, long fcap, double* __restrict__ part) {
+                                                    T* __restrict__ f, long fcap, int sym,
+                                                    double* __restrict__ part) {
     double pe = 0, vir = 0;
+    const T half = sym ? T(1) : T(0.5);
     for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
         typename V4<T>::type xi = ld4(pos, i);
         unsigned int bad = 0;
@@ -129,17 +136,39 @@ __global__ void __launch_bounds__(FBLOCK) k_lj_cell(const typename V4<T>::type* 
                 unsigned int a = cs[rb + xa], b = cs[rb + xb + 1];
                 for (unsigned int k = a; k < b; ++k) {
                     typename V4<T>::type xq = ld4(pcs, k);
-                    if (IdxDec<T>::dec(xq.w) == (int)i) continue;
+                    const int qi = IdxDec<T>::dec(xq.w);
+                    if (qi == (int)i) continue;
+                    // symmetric cell list: each pair once (the half-list rule of pd_verlet.cu)
+                    if (sym && !(qi < n ? qi > (int)i : lex_after(xq, xi))) continue;
                     T dx = xi.x - xq.x, dy2 = xi.y - xq.y, dz2 = xi.z - xq.z;
                     T r2 = dist2(dx, dy2, dz2);
-                    if (r2 < P.rc2) lj_acc(P, r2, dx, dy2, dz2, fx, fy, fz, e, w);
+                    if (r2 < P.rc2) {
+                        if (sym) {
+                            T gx = 0, gy = 0, gz = 0;
+                            lj_acc(P, r2, dx, dy2, dz2, gx, gy, gz, e, w);
+                            fx += gx;
+                            fy += gy;
+                            fz += gz;
+                            atomicAdd(f + qi, -gx);
+                            atomicAdd(f + fcap + qi, -gy);
+                            atomicAdd(f + 2 * fcap + qi, -gz);
+                        } else {
+                            lj_acc(P, r2, dx, dy2, dz2, fx, fy, fz, e, w);
+                        }
+                    }
                 }
             }
-        f[i] = fx;
-        f[fcap + i] = fy;
-        f[2 * fcap + i] = fz;
-        pe += 0.5 * (double)e;
-        vir += 0.5 * (double)w;
+        if (sym) {
+            atomicAdd(f + i, fx);
+            atomicAdd(f + fcap + i, fy);
+            atomicAdd(f + 2 * fcap + i, fz);
+        } else {
+            f[i] = fx;
+            f[fcap + i] = fy;
+            f[2 * fcap + i] = fz;
+        }
+        pe += (double)(half * e);
+        vir += (double)(half * w);
     }
     pe = block_sum<double, FBLOCK>(pe);
     vir = block_sum<double, FBLOCK>(vir);
@@ -367,6 +396,10 @@ static int lj_launch(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t& lj, int 
     } else {
         // cell-ordered copy of all positions for the walk
         long nt = h->n_total;
+        const int sym = (cl->opt & PD_CL_SYMMETRIC) ? 1 : 0;
+        if (sym)  // the images receive reactions: domain and image forces start at zero
+            for (int c = 0; c < 3; ++c)
+                PD_CUDA(cudaMemsetAsync(F.d + (size_t)c * h->cap * F.esize, 0, (size_t)nt * F.esize, st));
         PD_TRY(h->tmp.ensure((size_t)(nt > 0 ? nt : 1) * h->pos_bytes));
         unsigned g = grid_for(nt, 256);
         if (h->dtype == PD_F64) {
@@ -374,13 +407,13 @@ static int lj_launch(pd_vd h, pd_vl vl, pd_cl cl, const pd_lj_params_t& lj, int 
                                                     h->tmp.as<double4>());
             pd::launch(k_lj_cell<double>, nblk, FBLOCK, 0, st, (const double4*)h->pos, n, h->tmp.as<double4>(),
                                                        cl->cell_start.as<unsigned int>(), grid_of<double>(cl),
-                                                       ljp<double>(lj), (double*)F.d, h->cap, part);
+                                                       ljp<double>(lj), (double*)F.d, h->cap, sym, part);
         } else {
             pd::launch(k_gather_cs2<float>, g, 256, 0, st, (const float4*)h->pos, cl->sorted.as<int>(), nt,
                                                    h->tmp.as<float4>());
             pd::launch(k_lj_cell<float>, nblk, FBLOCK, 0, st, (const float4*)h->pos, n, h->tmp.as<float4>(),
                                                       cl->cell_start.as<unsigned int>(), grid_of<float>(cl),
-                                                      ljp<float>(lj), (float*)F.d, h->cap, part);
+                                                      ljp<float>(lj), (float*)F.d, h->cap, sym, part);
         }
     }
     PD_LAUNCH_CHECK();
@@ -554,7 +587,7 @@ static int md_step_cl(pd_md md, cudaStream_t st, long img_cap) {
     pd::launch(k_gather_cs2_dev<T>, grid_for(bound, 256), 256, 0, st, (const T4*)h->pos, cl->sorted.as<int>(), bound,
                (const unsigned int*)&h->ctrl->n_img, n, h->tmp.as<T4>());
     pd::launch(k_lj_cell<T>, md->nblk, FBLOCK, 0, st, (const T4*)h->pos, n, h->tmp.as<T4>(),
-               cl->cell_start.as<unsigned int>(), grid_of<T>(cl), ljp<T>(md->lj), (T*)F.d, h->cap,
+               cl->cell_start.as<unsigned int>(), grid_of<T>(cl), ljp<T>(md->lj), (T*)F.d, h->cap, 0,
                md->fpart.as<double>());
     pd::launch(k_kick<T>, md->nblk, FBLOCK, 0, st, (T*)V.d, (const T*)F.d, h->cap, n, half, md->mp.mass,
                md->kpart.as<double>());

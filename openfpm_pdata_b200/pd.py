@@ -21,11 +21,12 @@ NON_PERIODIC, PERIODIC = 0, 1
 NO_POSITION, WITH_POSITION, NO_CHANGE_ELEMENTS = 1, 2, 4
 SKIP_LABELLING = KEEP_PROPERTIES = 512
 RUN_ON_DEVICE = 1024
-CL_NON_SYMMETRIC = 2
+CL_SYMMETRIC, CL_NON_SYMMETRIC = 1, 2
 CL_GPU_REORDER_POSITION, CL_GPU_REORDER_PROPERTY = 64, 128
 CL_GPU_REORDER = CL_GPU_REORDER_POSITION | CL_GPU_REORDER_PROPERTY
 RED_ADD, RED_MAX = 1, 2
 PUT_ADD, PUT_MAX, PUT_REPLACE = 1, 2, 3
+CMP_EQ, CMP_NE, CMP_LT, CMP_LE, CMP_GT, CMP_GE = range(6)
 
 _NP = {PD_F32: np.float32, PD_F64: np.float64, PD_I32: np.int32, PD_U32: np.uint32, PD_I64: np.int64}
 _CODES = {-1: "PD_EINVAL", -2: "PD_ENOMEM", -3: "PD_ECUDA", -4: "PD_ESTALE", -5: "PD_ETIMEOUT",
@@ -119,6 +120,9 @@ def lib():
             "pd_verlet_create": ([vp, ctypes.c_double, P(vp)], ip),
             "pd_verlet_create_sym": ([vp, ctypes.c_double, P(vp)], ip),
             "pd_ghost_put": ([vp, ctypes.c_ulong, ip, vp], ip),
+            "pd_remove_marked": ([vp, ip, vp], ip),
+            "pd_get_indexes_by_type": ([vp, ip, ip, ctypes.c_longlong, ctypes.c_long, vp, ctypes.c_long,
+                                        P(ctypes.c_long), vp], ip),
             "pd_verlet_destroy": ([vp], ip),
             "pd_verlet_update": ([vp, vp, vp], ip),
             "pd_verlet_get": ([vp, vp, vp, lp, vp], ip),
@@ -375,6 +379,20 @@ class VectorDist:
         check(lib().pd_domain_iterator(self.h, int(n_thr), int(with_ghost), ctypes.byref(it)))
         return it
 
+    def remove_marked(self, p):
+        """remove_marked<p>(): drop the domain particles whose property p is non-zero."""
+        check(lib().pd_remove_marked(self.h, int(p), None))
+
+    def get_indexes_by_type(self, p, value, cmp=CMP_EQ, end=None):
+        """get_indexes_by_type<p, functor>(): ascending indexes i < end with prop p `cmp` value."""
+        n = ctypes.c_long(0)
+        e = -1 if end is None else int(end)
+        cap = self.size_local_with_ghost()
+        ids = np.zeros(max(cap, 1), np.uint32)
+        check(lib().pd_get_indexes_by_type(self.h, int(p), int(cmp), int(value), e, _ptr(ids), cap,
+                                           ctypes.byref(n), None))
+        return ids[: n.value]
+
     def reduce_local(self, p, comp=0, op=RED_ADD):
         out = ctypes.c_double(0)
         check(lib().pd_reduce(self.h, int(p), int(comp), int(op), None, ctypes.byref(out)))
@@ -382,6 +400,9 @@ class VectorDist:
 
     def getCellListGPU(self, r_cut, opt=CL_NON_SYMMETRIC, NNIteratorBox=1, ghostEnlargeFactor=None):
         return CellList(self, r_cut, opt, NNIteratorBox, ghostEnlargeFactor)
+
+    def getCellListSym(self, r_cut):
+        return CellList(self, r_cut, CL_SYMMETRIC)
 
     def updateCellListGPU(self, cl, props=None):
         mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)

@@ -281,3 +281,66 @@ def md_lj(x, v, lo, hi, bc, ghost, rc, skin, eps, sigma, dt, mass, steps, timing
                            _a(g, np.float64), rc, skin, eps, sigma, dt, mass, steps, E, ctypes.byref(t))
     assert rc_ == 0
     return (x, v, E, t.value) if timing else (x, v, E)
+
+
+# ---------------------------------------------------------------------------
+# index / merge restatements in numpy (small, sequential: the order is the spec)
+
+def ghost_put(a, n, src, op):
+    """ghost_put<op_> on one process (vector_dist_comm.hpp:2086-2182, merge_prp_v):
+    the value of every ghost j (slot n + j) is merged onto its source src[j]; the
+    ghosts of one source in ghost order.  op: 1 add_, 2 max_, 3 replace_."""
+    out = np.array(a[:n], copy=True)
+    for j in np.argsort(np.asarray(src), kind="stable"):
+        p = src[j]
+        v = a[n + j]
+        if op == 1:
+            out[p] = out[p] + v
+        elif op == 2:
+            out[p] = np.maximum(out[p], v)
+        else:
+            out[p] = v
+    return out
+
+
+def _lex_after(a, b):
+    return a[0] > b[0] or (a[0] == b[0] and (a[1] > b[1] or (a[1] == b[1] and a[2] > b[2])))
+
+
+def verlet_sym(pos, n_dom, off, idx):
+    """Symmetric (half) list from the full list (getVerletSym, vector_dist.hpp:1412-1416):
+    row p keeps a domain partner q iff q > p and a ghost iff it lies after p in
+    (x, y, z) lexicographic order, so each pair -- and each periodic mirror pair --
+    appears once.  Rows keep the full list's order.  Returns CSR (offsets, idx)."""
+    hoff = np.zeros(n_dom + 1, np.int64)
+    rows = []
+    for i in range(n_dom):
+        row = idx[off[i]:off[i + 1]]
+        keep = [q for q in row if (q > i if q < n_dom else _lex_after(pos[q], pos[i]))]
+        rows.append(np.asarray(keep, np.int32))
+        hoff[i + 1] = hoff[i] + len(keep)
+    return hoff, (np.concatenate(rows) if hoff[-1] else np.zeros(0, np.int32))
+
+
+def remove_marked(mark, *cols):
+    """remove_marked<prp> (vector_dist_cuda_funcs.cuh:333-412): the mark is flipped
+    (flip_one_to_zero :313-321, x -> x == 0), the particles with a flipped mark of
+    1 are kept in order (copy_new_to_old_by_scan :295-311).  Returns (flipped mark
+    of all particles, kept flipped mark, kept columns...); when nothing is marked
+    the columns come back whole."""
+    mark = np.asarray(mark)
+    flipped = (mark == 0).astype(mark.dtype)
+    keep = flipped != 0
+    if keep.all():
+        return (flipped, flipped) + tuple(np.asarray(c) for c in cols)
+    return (flipped, flipped[keep]) + tuple(np.asarray(c)[keep] for c in cols)
+
+
+def indexes_by_type(vals, end, cmp, value):
+    """get_indexes_by_type<prp, functor> (vector_dist_cuda_funcs.cuh:414-481): the
+    ascending indexes p < end with functor::check(vals[p]); here the check is a
+    comparison (0 ==, 1 !=, 2 <, 3 <=, 4 >, 5 >=) with `value`."""
+    v = np.asarray(vals)[:end]
+    ref = np.asarray(value).astype(v.dtype)
+    f = [v == ref, v != ref, v < ref, v <= ref, v > ref, v >= ref][cmp]
+    return np.nonzero(f)[0].astype(np.uint32)

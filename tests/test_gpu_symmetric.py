@@ -26,10 +26,6 @@ def pd():
     return _pd
 
 
-def _lex_after(a, b):
-    return a[0] > b[0] or (a[0] == b[0] and (a[1] > b[1] or (a[1] == b[1] and a[2] > b[2])))
-
-
 def _system(pd, orc, n, L, ghost, dtype, seed, props, bc=(1, 1, 1)):
     rng = np.random.default_rng(seed)
     lo, hi, bcv = np.zeros(3), np.full(3, L), np.asarray(bc, np.int32)
@@ -39,21 +35,6 @@ def _system(pd, orc, n, L, ghost, dtype, seed, props, bc=(1, 1, 1)):
     vd.map()
     vd.ghost_get()
     return vd
-
-
-def _put_expected(a, n, src, op):
-    out = a[:n].copy()
-    order = np.argsort(src, kind="stable")  # images of one source, in image order
-    for j in order:
-        p = src[j]
-        v = a[n + j]
-        if op == 1:
-            out[p] = out[p] + v
-        elif op == 2:
-            out[p] = np.maximum(out[p], v)
-        else:
-            out[p] = v
-    return out
 
 
 @pytest.mark.parametrize("op", [1, 2, 3])
@@ -75,7 +56,7 @@ def test_ghost_put_bit_exact(pd, orc, op, ptype):
     vd.hostToDeviceProp(1, b)
     vd.ghost_put([0], op=op)
     got = vd.deviceToHostProp(0)
-    assert np.array_equal(got[:n], _put_expected(a, n, src, op))
+    assert np.array_equal(got[:n], orc.ghost_put(a, n, src, op))
     assert np.array_equal(got[n:], a[n:])                      # ghosts keep their values
     assert np.array_equal(vd.deviceToHostProp(1), b)           # props outside the mask untouched
 
@@ -105,15 +86,9 @@ def test_verlet_sym_rows_are_filtered_full_rows(pd, orc, dtype, bc):
     off, idx = full.get()
     hoff, hidx = half.get()
     allp = vd.deviceToHostPos()
-    eo = np.zeros(n + 1, np.int64)
-    rows = []
-    for i in range(n):
-        row = idx[off[i]:off[i + 1]]
-        keep = [q for q in row if (q > i if q < n else _lex_after(allp[q], allp[i]))]
-        rows.append(np.asarray(keep, np.int32))
-        eo[i + 1] = eo[i] + len(keep)
-    assert np.array_equal(hoff, eo)
-    assert np.array_equal(hidx, np.concatenate(rows) if eo[-1] else hidx[:0])
+    eoff, eidx = orc.verlet_sym(allp, n, off, idx)
+    assert np.array_equal(hoff, eoff)
+    assert np.array_equal(hidx, eidx)
     # the full list holds each pair from both sides, plus p itself on row p
     assert off[-1] == 2 * hoff[-1] + n
 
@@ -199,3 +174,32 @@ def test_lj_sym_narrow_box_two_images(pd):
     frms = np.sqrt((ef ** 2).sum(axis=1).mean())
     assert np.all(np.abs(f - ef) <= 1e-10 * (np.abs(ef) + frms))
     assert abs(pe_s - pe) <= 1e-11 * abs(pe) and abs(vir_s - vir) <= 1e-11 * abs(vir)
+
+
+@pytest.mark.parametrize("dtype", [F32, F64])
+def test_lj_cell_list_sym_plus_ghost_put_equals_full(pd, dtype):
+    """vector_dist_symmetric_cell_list: LJ through getCellListSym (each pair once,
+    the reaction on the partner) plus ghost_put<add_> equals LJ through the full
+    cell list; FP64 within 1e-10 (|F| + F_rms), FP32 within 1e-4."""
+    from openfpm_pdata_b200 import workloads
+    x, _, L = workloads.lj_lattice(14, 1.1, 0.05, seed=9)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(x.shape[0], lo, hi, bc, 2.5, dtype=dtype,
+                       props=[(pd.PD_F64 if dtype == F64 else pd.PD_F32, 3)] * 2)
+    vd.hostToDevicePos(x.astype(dtype))
+    vd.map()
+    vd.ghost_get()
+    n = vd.size_local()
+    cl = vd.getCellListGPU(2.5)
+    vd.updateCellListGPU(cl)
+    pe, vir = vd.lj_forces(0, cl=cl)
+    ef = vd.deviceToHostProp(0)[:n].astype(F64)
+    cs = vd.getCellListSym(2.5)
+    vd.updateCellListGPU(cs)
+    pe_s, vir_s = vd.lj_forces(1, cl=cs)
+    vd.ghost_put([1])
+    f = vd.deviceToHostProp(1)[:n].astype(F64)
+    tol = 1e-10 if dtype == F64 else 1e-4
+    frms = np.sqrt((ef ** 2).sum(axis=1).mean())
+    assert np.all(np.abs(f - ef) <= tol * (np.abs(ef) + frms))
+    assert abs(pe_s - pe) <= tol * abs(pe) and abs(vir_s - vir) <= tol * abs(vir)

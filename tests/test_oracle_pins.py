@@ -9,6 +9,9 @@ assert, restated here on the same kinds of inputs:
 * ghost kernels on synthetic boxes ... Vector/cuda/vector_dist_cuda_func_test.cu:19-389
 * periodic ghost invariants .......... Vector/tests/vector_dist_unit_test.cpp:631-735
 * cell-list counts / in-cell order ... Vector/cuda/vector_dist_gpu_unit_tests.cu:425-567
+* symmetric list + ghost_put<add_> ... Vector/tests/vector_dist_cell_list_tests.cpp:443-649
+* remove_marked ...................... Vector/cuda/vector_dist_cuda_func_test.cu:945-1088
+* get_indexes_by_type ................ Vector/cuda/vector_dist_gpu_unit_tests.cu:1626-1694
 """
 import numpy as np
 import pytest
@@ -184,3 +187,76 @@ def test_md_lj_integrator_consistency(orc):
     assert E1[1:, 3].sum() < 100 and E0[1:, 3].sum() == 100
     np.testing.assert_allclose(E1[:, :3], E0[:, :3], rtol=1e-9, atol=1e-9)
     np.testing.assert_allclose(x1, x0, rtol=0, atol=1e-9)
+
+
+def test_symmetric_list_folds_to_full(orc):
+    """vector_dist_symmetric_verlet_list: each pair once in the half list; the
+    partner's share of a pair, put on its slot (a ghost for periodic pairs) and
+    folded by ghost_put<add_>, gives every particle the full list's count and
+    neighbour id set."""
+    rng = np.random.default_rng(5)
+    L, r = 6.0, 1.2
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    pos = orc.wrap(rng.uniform(0, L, size=(1500, 3)), lo, hi, bc)
+    n = pos.shape[0]
+    img, src, _ = orc.ghost_get(pos, lo, hi, bc, r)
+    allp = np.concatenate([pos, img])
+    G = orc.cl_geometry(lo, hi, r, r, verlet=True)
+    off, idx = orc.verlet(allp, n, G, r)
+    hoff, hidx = orc.verlet_sym(allp, n, off, idx)
+    assert off[-1] == 2 * hoff[-1] + n          # each pair twice plus p itself, vs each pair once
+    cnt = np.zeros(allp.shape[0], np.int64)
+    cnt[:n] = np.diff(hoff)
+    np.add.at(cnt, hidx, 1)
+    folded = orc.ghost_put(cnt, n, src, 1)
+    assert np.array_equal(folded, np.diff(off) - 1)
+    owner = np.concatenate([np.arange(n), src])
+    half_sets = [[] for _ in range(n)]
+    for i in range(n):
+        for q in hidx[hoff[i]:hoff[i + 1]]:
+            half_sets[i].append(int(owner[q]))
+            half_sets[owner[q]].append(i)
+    for i in range(0, n, 7):
+        row = idx[off[i]:off[i + 1]]
+        assert sorted(half_sets[i]) == sorted(owner[row[row != i]].tolist())
+
+
+def test_ghost_put_ops(orc):
+    """ghost_put merge ops on a hand-made case: source 0 has ghosts 2 and 4,
+    source 1 has ghost 3 (slots n + j)."""
+    a = np.array([1.0, 10.0, 5.0, -3.0, 7.0, 2.0])
+    n, src = 3, np.array([0, 1, 0])
+    assert np.array_equal(orc.ghost_put(a, n, src, 1), [1.0 - 3.0 + 2.0, 10.0 + 7.0, 5.0])
+    assert np.array_equal(orc.ghost_put(a, n, src, 2), [2.0, 10.0, 5.0])
+    assert np.array_equal(orc.ghost_put(a, n, src, 3), [2.0, 7.0, 5.0])
+
+
+@pytest.mark.parametrize("prp", [0, 1, 2, 3])
+def test_remove_marked_reference_case(orc, prp):
+    """vector_dist_remove_marked_type<prp>: props count up from 1, the mark is
+    ic % 3 == 0; a third is removed and no survivor holds a multiple of 3; with
+    all marks 0 nothing is removed, with all 1 everything is."""
+    n = 50000
+    base = np.arange(1, n + 1)
+    cols = [base.astype(F32), base.astype(F32), base.astype(np.int32), base.astype(np.int32)]
+    cols[prp] = (base % 3 == 0).astype(cols[prp].dtype)
+    out = orc.remove_marked(cols[prp], *cols)
+    kept = out[2:]
+    assert kept[0].shape[0] == n - n // 3
+    for c in range(4):
+        if c != prp:
+            assert np.all(kept[c].astype(np.int64) % 3 != 0)
+    assert np.all(out[1] == 1)                       # the mark is destroyed: 1 on survivors
+    none = orc.remove_marked(np.zeros(n, np.int32), base)
+    assert none[2].shape[0] == n and np.all(none[0] == 1)
+    assert orc.remove_marked(np.ones(n, np.int32), base)[2].shape[0] == 0
+
+
+def test_indexes_by_type_reference_case(orc):
+    """vector_dist_get_index_set with type_is_one: every returned id holds 1,
+    ascending, and none is missed."""
+    rng = np.random.default_rng(3)
+    t = (rng.random(10000) / 0.5).astype(np.int32)
+    ids = orc.indexes_by_type(t, 10000, 0, 1)
+    assert np.all(t[ids] == 1) and ids.shape[0] == int((t == 1).sum()) and np.all(np.diff(ids.astype(np.int64)) > 0)
+    assert orc.indexes_by_type(t, 5000, 0, 1).shape[0] == int((t[:5000] == 1).sum())
