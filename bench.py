@@ -276,6 +276,94 @@ def form_cell_list_every_step(pd, torch, steps=100, warmup=5):
             "gpu_launches_per_step": (pd.launch_count() - l0) / steps}
 
 
+def _ev_ms(torch, fn, reps):
+    """Mean ms of `fn` over `reps` calls between CUDA events (the calls synchronise themselves)."""
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def form_symmetric(pd, torch, x, L, reps=20):
+    """LJ forces on the 4,096,000-particle lattice from global-index rows: the full
+    Verlet list against the symmetric (half) list with reactions on the partners
+    and ghost_put<add_> folding the ghosts' share (FP64)."""
+    n = x.shape[0]
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(n, lo, hi, bc, R_CUT + SKIN, dtype=np.float64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    vd.hostToDevicePos(x)
+    vd.map()
+    vd.ghost_get()
+    rl = R_CUT + SKIN
+    full = vd.getVerlet(rl)
+    half = vd.getVerletSym(rl)
+    t_full_build = _ev_ms(torch, lambda: vd.updateVerlet(full), 3)
+    t_half_build = _ev_ms(torch, lambda: vd.updateVerlet(half), 3)
+    f_full = lambda: vd.lj_forces(0, vl=full, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+
+    def f_half():
+        vd.lj_forces(1, vl=half, eps=EPS, sigma=SIGMA, r_cut=R_CUT)
+        vd.ghost_put([1])
+    f_full()
+    f_half()
+    t_full = _ev_ms(torch, f_full, reps)
+    t_half = _ev_ms(torch, f_half, reps)
+    a = vd.deviceToHostProp(0, with_ghost=False)
+    b = vd.deviceToHostProp(1, with_ghost=False)
+    frms = np.sqrt((a ** 2).sum(axis=1).mean())
+    off, _ = full.get()
+    hoff, _ = half.get()
+    del full, half, vd
+    return {"workload": "LJ forces FP64, N=4,096,000 lattice (spacing 1.1), r_cut 2.5, list radius 2.8, "
+                        "global-index rows",
+            "full_list": {"ms": t_full, "entries": int(off[-1]), "build_ms": t_full_build},
+            "half_list_plus_ghost_put": {"ms": t_half, "entries": int(hoff[-1]), "build_ms": t_half_build},
+            "max_force_diff_over_frms": float(np.abs(a - b).max() / frms)}
+
+
+def form_compaction(pd, torch, n=4096000, frac=0.1, reps=5):
+    """remove_marked and get_indexes_by_type on 4,096,000 FP64 particles with two
+    3-component FP64 properties and an int mark (10 % marked)."""
+    rng = np.random.default_rng(21)
+    L = 176.0
+    x = rng.uniform(0, L, size=(n, 3))
+    v = rng.normal(size=(n, 3))
+    mark = (rng.random(n) < frac).astype(np.int32)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(n, lo, hi, bc, 1.0, dtype=np.float64,
+                       props=[(pd.PD_F64, 3), (pd.PD_F64, 3), (pd.PD_I32, 1)])
+    t_rm, t_ix = [], []
+    kept = 0
+    for it in range(reps + 1):
+        vd.resize(n)
+        vd.hostToDevicePos(x)
+        vd.hostToDeviceProp(0, v)
+        vd.hostToDeviceProp(1, v)
+        vd.hostToDeviceProp(2, mark)
+        t_ix.append(_ev_ms(torch, lambda: vd.get_indexes_by_type(2, 1), 1))
+        t_rm.append(_ev_ms(torch, lambda: vd.remove_marked(2), 1))
+        kept = vd.size_local()
+    t_rm, t_ix = float(np.mean(t_rm[1:])), float(np.mean(t_ix[1:]))
+    rec = 32 + 4 + 3 * 8 * 2 + 4  # position record, global id, two FP64 vectors, the mark
+    alg = n * rec + kept * rec
+    hbm, which = peaks()
+    del vd
+    return {"workload": "remove_marked / get_indexes_by_type, N=4,096,000 FP64 particles, props "
+                        "double[3], double[3], int mark, 10% marked",
+            "remove_marked_ms": t_rm, "kept": kept,
+            "remove_marked_roofline": {"bound": "hbm", "algorithmic_bytes": alg,
+                                       "achieved_gbs": alg / (t_rm / 1e3) / 1e9, "peak_gbs": hbm,
+                                       "frac": alg / (t_rm / 1e3) / 1e9 / hbm, "peak_kind": which,
+                                       "bytes": "read every record once, write every kept record once"},
+            "get_indexes_by_type_ms": t_ix,
+            "note": "both calls include their device-to-host count read and synchronise"}
+
+
 def form_sph(pd, torch, steps=200, warmup=5, dp=1.0 / 180):
     """WCSPH dam break, FP64 and FP32 storage."""
     from openfpm_pdata_b200 import workloads
@@ -447,7 +535,7 @@ def main():
                     help="fp64: plain FP64 path; mixed: FP32 cell-local positions, Kahan sums, FP64 wrap/energies")
     ap.add_argument("--forms", default="all",
                     help="other workloads reported beside the main line: all, none, or a comma list of "
-                         "precision,clustered,c1,sph,serving")
+                         "precision,clustered,c1,sph,serving,symmetric,compaction")
     ap.add_argument("--clustered-steps", type=int, default=200, help="steps of the clustered precision form")
     ap.add_argument("--serve-systems", type=int, default=600, help="systems in the serving sample")
     a = ap.parse_args()
@@ -586,7 +674,8 @@ def main():
         assert np.isfinite(E2).all()
 
     if rank == 0 and world == 1 and a.forms != "none":
-        want = a.forms.split(",") if a.forms != "all" else ["precision", "clustered", "c1", "sph", "serving"]
+        want = a.forms.split(",") if a.forms != "all" else ["precision", "clustered", "c1", "sph", "serving",
+                                                                     "symmetric", "compaction"]
         forms = {}
         if "precision" in want and not mixed:
             forms["precision"] = form_precision(pd, torch, x, v, L, a.steps, a.warmup, value)
@@ -598,6 +687,10 @@ def main():
             forms["sph"] = form_sph(pd, torch)
         if "serving" in want:
             forms["serving"] = form_serving(pd, torch, n_systems=a.serve_systems)
+        if "symmetric" in want:
+            forms["symmetric"] = form_symmetric(pd, torch, x, L)
+        if "compaction" in want:
+            forms["compaction"] = form_compaction(pd, torch)
         out["forms"] = forms
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -184,6 +184,15 @@ template <typename St> class vector_dist_gpu {
         if (prps.size() == 0) mask = ~0ul;
         check(pd_ghost_get(h_, mask, opt, stream_));
     }
+    // ghost_put<op_, prp...>() on one process -- vector_dist.hpp:2304 (op: PD_PUT_ADD / _MAX / _REPLACE)
+    void ghost_put(std::initializer_list<int> prps = {}, int op = PD_PUT_ADD) {
+        unsigned long mask = 0;
+        for (int p : prps) mask |= 1ul << p;
+        if (prps.size() == 0) mask = ~0ul;
+        check(pd_ghost_put(h_, mask, op, stream_));
+    }
+    // getCellListSym(r_cut) -- vector_dist.hpp:1062
+    CellList_gpu getCellListSym(St r_cut) { return getCellListGPU(r_cut, PD_CL_SYMMETRIC); }
     // getCellListGPU(r_cut, opt, NNIteratorBox, no_se3, ghostEnlargeFactor) -- vector_dist.hpp:1222
     CellList_gpu getCellListGPU(St r_cut, int opt = PD_CL_NON_SYMMETRIC, int nn_box = 1,
                                 double enlarge = (double)1.013f) {
@@ -210,6 +219,25 @@ template <typename St> class vector_dist_gpu {
         VerletList vl(v, size_local());
         check(pd_verlet_update(h_, v, stream_));
         return vl;
+    }
+    // getVerletSym(r_cut) -- vector_dist.hpp:1412
+    VerletList getVerletSym(St r_cut) {
+        pd_vl v = nullptr;
+        check(pd_verlet_create_sym(h_, (double)r_cut, &v));
+        VerletList vl(v, size_local());
+        check(pd_verlet_update(h_, v, stream_));
+        return vl;
+    }
+    // remove_marked<prp>(vd) -- vector_dist_cuda_funcs.cuh:333
+    void remove_marked(int prp) { check(pd_remove_marked(h_, prp, stream_)); }
+    // get_indexes_by_type<prp, functor>(vd, ids, end) -- vector_dist_cuda_funcs.cuh:449;
+    // the functor's check as a comparison cmp (PD_CMP_*) with value
+    std::vector<unsigned int> get_indexes_by_type(int prp, int cmp, long long value, long end = -1) {
+        std::vector<unsigned int> ids((size_t)(size_all() > 0 ? size_all() : 1));
+        long n = 0;
+        check(pd_get_indexes_by_type(h_, prp, cmp, value, end, ids.data(), (long)ids.size(), &n, stream_));
+        ids.resize((size_t)n);
+        return ids;
     }
     void updateVerlet(VerletList& vl) {
         check(pd_verlet_update(h_, vl.handle(), stream_));
