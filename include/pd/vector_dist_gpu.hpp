@@ -228,6 +228,17 @@ template <typename St> class vector_dist_gpu {
         check(pd_verlet_update(h_, v, stream_));
         return vl;
     }
+    // save(filename) / load(filename) -- vector_dist.hpp:2459-2476 (own checksummed binary format)
+    void save(const std::string& path) const { check(pd_save(h_, path.c_str())); }
+    void load(const std::string& path) { check(pd_load(h_, path.c_str())); }
+    // write(out, meta_info, opt) / write_frame(out, iteration, meta_info, opt) -- vector_dist.hpp:2498-2721
+    void write(const std::string& out, const std::string& meta = "", int opt = PD_VTK_WRITER) const {
+        check(pd_write(h_, out.c_str(), meta.c_str(), opt));
+    }
+    void write_frame(const std::string& out, long iteration, const std::string& meta = "",
+                     int opt = PD_VTK_WRITER) const {
+        check(pd_write_frame(h_, out.c_str(), iteration, meta.c_str(), opt));
+    }
     // remove_marked<prp>(vd) -- vector_dist_cuda_funcs.cuh:333
     void remove_marked(int prp) { check(pd_remove_marked(h_, prp, stream_)); }
     // get_indexes_by_type<prp, functor>(vd, ids, end) -- vector_dist_cuda_funcs.cuh:449;

@@ -28,6 +28,7 @@ extern "C" {
 #define PD_ETIMEOUT (-5)  /* a bounded device wait gave up */
 #define PD_EOVERFLOW (-6) /* a device-side capacity was exceeded; the result is void */
 #define PD_ESTATE (-7)    /* call out of order (e.g. restore_order without a reorder) */
+#define PD_EIO (-8)       /* a file could not be written / read, or is not of the expected format */
 
 /* ---- value types -------------------------------------------------------- */
 #define PD_F32 1
@@ -63,6 +64,12 @@ extern "C" {
 #define PD_PUT_ADD 1
 #define PD_PUT_MAX 2
 #define PD_PUT_REPLACE 3
+
+/* writer options of pd_write / pd_write_frame (VTK_WRITER, CSV_WRITER, FORMAT_BINARY
+ * of the reference; values are this library's own) */
+#define PD_VTK_WRITER 0
+#define PD_CSV_WRITER 1
+#define PD_FORMAT_BINARY 2
 
 /* comparisons of pd_get_indexes_by_type (the functor::check of the reference) */
 #define PD_CMP_EQ 0
@@ -219,6 +226,19 @@ int pd_remove_marked(pd_vd h, int prop, void* stream);
  * receives them; *n_out their count (PD_EOVERFLOW if above cap). */
 int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end, unsigned int* ids, long cap,
                            long* n_out, void* stream);
+/* save(filename) / load(filename) -- vector_dist.hpp:2459-2476: the domain
+ * particles (positions, global ids, properties) in this library's own binary
+ * checkpoint format (checksummed); load replaces the particles of a vector of
+ * the same dtype whose property list is the file's or empty (then added).
+ * Synchronous; PD_EIO on a file error or a corrupt/foreign file. */
+int pd_save(pd_vd h, const char* path);
+int pd_load(pd_vd h, const char* path);
+/* write(out, meta_info, opt) / write_frame(out, iteration, meta_info, opt) --
+ * vector_dist.hpp:2498-2721: VTK XML PolyData `<out>_0.vtp` (`<out>_0_<it>.vtp`;
+ * PD_FORMAT_BINARY for base64 binary arrays) or CSV `<out>_0.csv` with
+ * PD_CSV_WRITER.  meta "name = value" becomes a FieldData value.  Domain only. */
+int pd_write(pd_vd h, const char* out, const char* meta, int opt);
+int pd_write_frame(pd_vd h, const char* out, long iteration, const char* meta, int opt);
 /* the original index of every particle in its current storage slot */
 int pd_d2h_gid(pd_vd h, long* host, long offset, long count, void* stream);
 

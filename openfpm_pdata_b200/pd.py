@@ -27,10 +27,11 @@ CL_GPU_REORDER = CL_GPU_REORDER_POSITION | CL_GPU_REORDER_PROPERTY
 RED_ADD, RED_MAX = 1, 2
 PUT_ADD, PUT_MAX, PUT_REPLACE = 1, 2, 3
 CMP_EQ, CMP_NE, CMP_LT, CMP_LE, CMP_GT, CMP_GE = range(6)
+VTK_WRITER, CSV_WRITER, FORMAT_BINARY = 0, 1, 2
 
 _NP = {PD_F32: np.float32, PD_F64: np.float64, PD_I32: np.int32, PD_U32: np.uint32, PD_I64: np.int64}
 _CODES = {-1: "PD_EINVAL", -2: "PD_ENOMEM", -3: "PD_ECUDA", -4: "PD_ESTALE", -5: "PD_ETIMEOUT",
-          -6: "PD_EOVERFLOW", -7: "PD_ESTATE"}
+          -6: "PD_EOVERFLOW", -7: "PD_ESTATE", -8: "PD_EIO"}
 
 
 class PdError(RuntimeError):
@@ -121,6 +122,10 @@ def lib():
             "pd_verlet_create_sym": ([vp, ctypes.c_double, P(vp)], ip),
             "pd_ghost_put": ([vp, ctypes.c_ulong, ip, vp], ip),
             "pd_remove_marked": ([vp, ip, vp], ip),
+            "pd_save": ([vp, ctypes.c_char_p], ip),
+            "pd_load": ([vp, ctypes.c_char_p], ip),
+            "pd_write": ([vp, ctypes.c_char_p, ctypes.c_char_p, ip], ip),
+            "pd_write_frame": ([vp, ctypes.c_char_p, ctypes.c_long, ctypes.c_char_p, ip], ip),
             "pd_get_indexes_by_type": ([vp, ip, ip, ctypes.c_longlong, ctypes.c_long, vp, ctypes.c_long,
                                         P(ctypes.c_long), vp], ip),
             "pd_verlet_destroy": ([vp], ip),
@@ -255,6 +260,15 @@ class VerletList:
         if getattr(self, "h", None) and _lib is not None:
             _lib.pd_verlet_destroy(self.h)
             self.h = None
+
+
+def _prop_table(path):
+    """(type, ncomp) list of a checkpoint file (the header layout of pd_save)."""
+    with open(path, "rb") as f:
+        head = f.read(120)
+        nprops = int(np.frombuffer(head[8:24], np.uint32)[3])
+        t = np.frombuffer(f.read(8 * nprops), np.int32).reshape(-1, 2)
+    return [(int(a), int(b)) for a, b in t]
 
 
 class VectorDist:
@@ -392,6 +406,22 @@ class VectorDist:
         check(lib().pd_get_indexes_by_type(self.h, int(p), int(cmp), int(value), e, _ptr(ids), cap,
                                            ctypes.byref(n), None))
         return ids[: n.value]
+
+    def save(self, path):
+        """save(filename): domain particles to a checksummed binary checkpoint."""
+        check(lib().pd_save(self.h, os.fsencode(path)))
+
+    def load(self, path):
+        """load(filename): replace the particles by a checkpoint's (properties added if none)."""
+        check(lib().pd_load(self.h, os.fsencode(path)))
+        if not self.props:
+            self.props = _prop_table(path)
+
+    def write(self, out, meta="", opt=VTK_WRITER):
+        check(lib().pd_write(self.h, os.fsencode(out), meta.encode(), int(opt)))
+
+    def write_frame(self, out, iteration, meta="", opt=VTK_WRITER):
+        check(lib().pd_write_frame(self.h, os.fsencode(out), int(iteration), meta.encode(), int(opt)))
 
     def reduce_local(self, p, comp=0, op=RED_ADD):
         out = ctypes.c_double(0)
