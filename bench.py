@@ -392,13 +392,13 @@ def form_sph(pd, torch, steps=200, warmup=5, dp=1.0 / 180):
     return out
 
 
-def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
+def form_serving(pd, torch, n_systems=600, steps=50, slots=128, seed=6, loads=(0.4, 0.6, 0.8)):
     """Serving form: a bounded sample of the stream of independent LJ systems
     (N log-uniform in [512, 262144], density 0.8, 50 steps each).
-    (1) capacity: the first half of the sample submitted at once;
-    (2) Poisson arrivals of the second half at 0.8 x that capacity: p50/p99 latency
-        (arrival -> result) and aggregate throughput;
-    (3) plain: a subset run one after another through the single-system driver."""
+    (1) capacity: a quarter of the sample submitted at once;
+    (2) Poisson arrivals at `loads` x that capacity (a quarter of the sample each):
+        p50/p99 latency (arrival -> result) and aggregate throughput;
+    (3) isolated: systems run one after another through the single-system driver."""
     from openfpm_pdata_b200 import workloads
     sizes = workloads.serving_sizes(n_systems, seed=seed)
     systems = [workloads.serving_system(int(n), 0.8, seed=1000 + k) for k, n in enumerate(sizes)]
@@ -411,54 +411,61 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
         t = srv.submit(x, v, L, 2)
         srv.run_until_done([t])
         srv.release(t)
-    half = n_systems // 2
+    part = n_systems // (1 + len(loads))
     # (1) capacity
     st0 = srv.stats()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tickets = [srv.submit(x, v, L, steps) for (x, v, L) in systems[:half]]
+    tickets = [srv.submit(x, v, L, steps) for (x, v, L) in systems[:part]]
     srv.run_until_done(tickets)
     t_cap = time.perf_counter() - t0
     st1 = srv.stats()
     tm_cap = srv.timers()
     for t in tickets:
         srv.release(t)
-    srv.completed(1 << 20)  # drain: the Poisson phase polls its own tickets
+    srv.completed(1 << 20)  # drain: the Poisson phases poll their own tickets
     cap_ps = (st1["particle_steps"] - st0["particle_steps"]) / t_cap
-    cap_sys = half / t_cap
-    # (2) Poisson arrivals at 0.8 x capacity
-    rng = np.random.default_rng(seed + 1)
-    lam = 0.8 * cap_sys
-    arr = np.cumsum(rng.exponential(1.0 / lam, size=n_systems - half))
-    pend = list(range(n_systems - half))
-    live = {}
-    lat = []
-    t0 = time.perf_counter()
-    st0 = srv.stats()
-    while pend or live:
-        now = time.perf_counter() - t0
-        while pend and arr[pend[0]] <= now:
-            k = pend.pop(0)
-            x, v, L = systems[half + k]
-            live[srv.submit(x, v, L, steps)] = arr[k]
-        if not live:
-            time.sleep(max(0.0, min(arr[pend[0]] - now, 0.01)))
-            continue
-        srv.tick()
-        now = time.perf_counter() - t0
-        for t in srv.completed():
-            lat.append(now - live.pop(t))
-            srv.release(t)
-    t_run = time.perf_counter() - t0
-    st1 = srv.stats()
-    srv_ps = (st1["particle_steps"] - st0["particle_steps"]) / t_run
-    lat = np.array(lat)
+    cap_sys = part / t_cap
+
+    # (2) Poisson arrivals at each load
+    def poisson(load, subset, rseed):
+        rng = np.random.default_rng(rseed)
+        arr = np.cumsum(rng.exponential(1.0 / (load * cap_sys), size=len(subset)))
+        pend = list(range(len(subset)))
+        live, lat = {}, []
+        t0 = time.perf_counter()
+        s0 = srv.stats()
+        while pend or live:
+            now = time.perf_counter() - t0
+            while pend and arr[pend[0]] <= now:
+                k = pend.pop(0)
+                x, v, L = subset[k]
+                live[srv.submit(x, v, L, steps)] = arr[k]
+            if not live:
+                time.sleep(max(0.0, min(arr[pend[0]] - now, 0.01)))
+                continue
+            srv.tick()
+            now = time.perf_counter() - t0
+            for t in srv.completed():
+                lat.append(now - live.pop(t))
+                srv.release(t)
+        t_run = time.perf_counter() - t0
+        s1 = srv.stats()
+        lat = np.array(lat)
+        return {"offered_vs_capacity": load, "systems": len(subset),
+                "value": (s1["particle_steps"] - s0["particle_steps"]) / t_run, "unit": METRIC,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50))}
+    phases = []
+    for q, load in enumerate(loads):
+        phases.append(poisson(load, systems[part * (q + 1): part * (q + 2)], seed + 1 + q))
     tuned = srv.tuned()
     tm_all = srv.timers()
+    st_all = srv.stats()
     del srv
-    # (3) plain: the single-system mixed-precision driver, one system after another
+    # (3) isolated: the single-system mixed-precision driver, one system after another
     plain_lat, plain_ps = [], 0
-    sub = systems[half: half + 40]
+    sub = systems[part: part + 40]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for (x, v, L) in sub:
@@ -475,24 +482,28 @@ def form_serving(pd, torch, n_systems=400, steps=50, slots=128, seed=6):
         plain_ps += x.shape[0] * steps
         del md, vd
     t_plain = time.perf_counter() - t0
+    iso = plain_ps / t_plain
+    for ph in phases:
+        ph["vs_isolated"] = ph["value"] / iso
+        ph["vs_capacity"] = ph["value"] / cap_ps
+    ok = [ph for ph in phases if ph["p99_over_p50"] <= 3.0 and ph["vs_isolated"] >= 0.7]
     return {"workload": f"{n_systems} systems of the serving stream (N log-uniform in [512, 262144], density 0.8, "
                         f"r_cut 2.5, skin 0.3, {steps} velocity-Verlet steps, FP32 forces + Kahan, FP64 energies); "
-                        f"first {half} submitted at once (capacity), last {n_systems - half} Poisson at 0.8 x capacity",
+                        f"{part} submitted at once (capacity), then {part} Poisson arrivals at each of "
+                        f"{', '.join(str(l) for l in loads)} x capacity",
             "max_slots": slots, "mean_particles": float(sizes.mean()),
             "capacity": {"value": cap_ps, "unit": METRIC, "systems_per_s": cap_sys},
-            "poisson_0.8": {"value": srv_ps, "unit": METRIC, "offered_vs_capacity": 0.8,
-                            "vs_capacity": srv_ps / cap_ps,
-                            "note": "value = all particle-steps of the Poisson systems / (last completion - first "
-                                    "arrival), ramp-up and drain included",
-                            "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                            "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50))},
-            "plain_sequential": {"value": plain_ps / t_plain, "unit": METRIC, "systems": len(sub),
-                                 "p50_ms": float(np.percentile(plain_lat, 50) * 1e3),
-                                 "p99_ms": float(np.percentile(plain_lat, 99) * 1e3)},
+            "poisson": phases,
+            "isolated_sequential": {"value": iso, "unit": METRIC, "systems": len(sub),
+                                    "p50_ms": float(np.percentile(plain_lat, 50) * 1e3),
+                                    "p99_ms": float(np.percentile(plain_lat, 99) * 1e3)},
+            "target_p99_within_3x_p50_at_0.7_isolated": {
+                "met": bool(ok), "highest_load_meeting_it": max((ph["offered_vs_capacity"] for ph in ok), default=None)},
+            "note": "Poisson value = particle-steps of that phase / (last completion - first arrival), ramp-up and "
+                    "drain included; vs_isolated = that value / the isolated sequential throughput",
             "tuned_tile_width_by_log2_size": {str(k): v for k, v in tuned.items()},
-            "host_ms": {"capacity_phase": tm_cap, "total": tm_all, "ticks": st1["ticks"],
-                        "rebuilds": st1["rebuilds"]}}
+            "host_ms": {"capacity_phase": tm_cap, "total": tm_all, "ticks": st_all["ticks"],
+                        "rebuilds": st_all["rebuilds"]}}
 
 
 def max_over_ranks(ms, dist, device):
@@ -537,7 +548,7 @@ def main():
                     help="other workloads reported beside the main line: all, none, or a comma list of "
                          "precision,clustered,c1,sph,serving,symmetric,compaction")
     ap.add_argument("--clustered-steps", type=int, default=200, help="steps of the clustered precision form")
-    ap.add_argument("--serve-systems", type=int, default=600, help="systems in the serving sample")
+    ap.add_argument("--serve-systems", type=int, default=800, help="systems in the serving sample")
     a = ap.parse_args()
     TUNE.update(tiles=a.tiles, tx=a.tx, tpp=a.tpp, precision=a.precision)
     mixed = a.precision == "mixed"

@@ -29,7 +29,8 @@
 // build scratch) are kept after the system retires and reused by the next one
 // (buffers only grow), so admission and retirement allocate nothing in steady
 // state.  Admission: FIFO; a request is admitted when a slot is free and its
-// memory estimate fits the server's HBM budget and cudaMemGetInfo's free memory;
+// memory estimate fits the server's HBM budget, which is reserved in the server's
+// memory pool at creation (capped by the free memory then);
 // its first build and forces run through the single-system path, with the slot's
 // image capacity reserved beforehand with a margin for the batched rebuilds.
 // Autotuner: per size bucket (floor(log2 N)), the first admitted system times the
@@ -1588,6 +1589,9 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
         if (want > 0 && cudaMallocFromPoolAsync(&p, want, s->pool, s->as) == cudaSuccess) {
             cudaFreeAsync(p, s->as);
             cudaStreamSynchronize(s->as);
+            // admission counts against what the pool holds: no free-memory query per
+            // step (cudaMemGetInfo took 10-100 ms at times on a shared node)
+            s->budget = (long)std::min((size_t)s->budget, want);
         }
         cudaGetLastError();
     }
@@ -1674,10 +1678,6 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         s->adm_pending = false;
     }
     if (s->dirty && !s->active.empty()) PD_TRY(upload_tables(s));
-    // free device memory for the admission check, queried while the GPU is idle
-    // (the query waits for running work)
-    size_t fr = 0, tot = 0;
-    if (!s->queue.empty()) PD_CUDA(cudaMemGetInfo(&fr, &tot));
     // one velocity-Verlet step of every active system; admissions are prepared
     // meanwhile on the admission stream (host work and asynchronous copies only)
     const bool stepping = !s->active.empty();
@@ -1697,7 +1697,7 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
     std::vector<SrvReq*> admitted;
     while (!s->queue.empty() && (int)(s->active.size() + admitted.size()) < s->max_slots) {
         SrvReq* r = s->reqs[s->queue.front()].get();
-        if (s->used + r->bytes > (size_t)s->budget || r->bytes + (256ul << 20) > fr) break;
+        if (s->used + r->bytes > (size_t)s->budget) break;
         int slot = 0;
         while (used_slot[slot]) ++slot;
         s->queue.pop_front();
@@ -1710,7 +1710,6 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
             cudaStreamSynchronize(s->as);
             return rc;
         }
-        fr = fr > r->bytes ? fr - r->bytes : 0;
         used_slot[slot] = 1;
         admitted.push_back(r);
     }
