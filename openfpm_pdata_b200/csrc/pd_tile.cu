@@ -257,7 +257,7 @@ int tile_plan(pd_cl cl, long n_real, int TX_req, TileGeom& tg, long& ntiles) {
     if (TX <= 0) {
         double cells = (double)cl->div[0] * cl->div[1] * cl->div[2];
         double occ = cells > 0 ? (double)n_real / cells : 1.0;
-        TX = (int)(120.0 / (occ > 1e-3 ? occ : 1e-3) + 0.5);
+        TX = (int)(140.0 / (occ > 1e-3 ? occ : 1e-3) + 0.5);
     }
     if (TX < 1) TX = 1;
     if (TX > TXMAX) TX = TXMAX;
