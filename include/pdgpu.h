@@ -226,6 +226,13 @@ int pd_remove_marked(pd_vd h, int prop, void* stream);
  * receives them; *n_out their count (PD_EOVERFLOW if above cap). */
 int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end, unsigned int* ids, long cap,
                            long* n_out, void* stream);
+/* Failure detection of the bounded device waits (no reference counterpart): runs
+ * the tile kernels' staging pattern -- an mbarrier armed for one 16-byte
+ * cp.async.bulk copy, then a wait of at most `limit` polls -- on one CTA.  With
+ * issue_copy the copy completes the phase: PD_OK and out4 = in4.  Without it
+ * nothing completes the phase: the wait gives up, the kernel records the timeout
+ * and returns, and the call returns PD_ETIMEOUT with the context still usable. */
+int pd_selftest_wait(long limit, int issue_copy, const float* in4, float* out4);
 /* save(filename) / load(filename) -- vector_dist.hpp:2459-2476: the domain
  * particles (positions, global ids, properties) in this library's own binary
  * checkpoint format (checksummed); load replaces the particles of a vector of

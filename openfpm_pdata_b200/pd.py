@@ -123,6 +123,7 @@ def lib():
             "pd_ghost_put": ([vp, ctypes.c_ulong, ip, vp], ip),
             "pd_remove_marked": ([vp, ip, vp], ip),
             "pd_save": ([vp, ctypes.c_char_p], ip),
+            "pd_selftest_wait": ([ctypes.c_long, ip, vp, vp], ip),
             "pd_load": ([vp, ctypes.c_char_p], ip),
             "pd_write": ([vp, ctypes.c_char_p, ctypes.c_char_p, ip], ip),
             "pd_write_frame": ([vp, ctypes.c_char_p, ctypes.c_long, ctypes.c_char_p, ip], ip),
@@ -623,3 +624,11 @@ class Server:
         if getattr(self, "h", None) and _lib is not None:
             _lib.pd_srv_destroy(self.h)
             self.h = None
+
+
+def selftest_wait(limit, issue_copy):
+    """Bounded-wait self test: (status code, the 4 floats copied through shared memory)."""
+    a = np.array([1.5, -2.25, 3.0, 4.75], np.float32)
+    out = np.zeros(4, np.float32)
+    rc = lib().pd_selftest_wait(int(limit), int(bool(issue_copy)), _ptr(a), _ptr(out))
+    return rc, out
