@@ -453,6 +453,7 @@ def form_serving(pd, torch, n_systems=600, steps=50, slots=128, seed=6, loads=(0
         s1 = srv.stats()
         lat = np.array(lat)
         return {"offered_vs_capacity": load, "systems": len(subset),
+                "systems_per_s": len(subset) / t_run, "systems_vs_capacity": len(subset) / t_run / cap_sys,
                 "value": (s1["particle_steps"] - s0["particle_steps"]) / t_run, "unit": METRIC,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50))}
@@ -500,7 +501,8 @@ def form_serving(pd, torch, n_systems=600, steps=50, slots=128, seed=6, loads=(0
             "target_p99_within_3x_p50_at_0.7_isolated": {
                 "met": bool(ok), "highest_load_meeting_it": max((ph["offered_vs_capacity"] for ph in ok), default=None)},
             "note": "Poisson value = particle-steps of that phase / (last completion - first arrival), ramp-up and "
-                    "drain included; vs_isolated = that value / the isolated sequential throughput",
+                    "drain included; vs_isolated = that value / the isolated sequential throughput; "
+                    "systems_vs_capacity = systems completed per second / the capacity phase's systems per second",
             "tuned_tile_width_by_log2_size": {str(k): v for k, v in tuned.items()},
             "host_ms": {"capacity_phase": tm_cap, "total": tm_all, "ticks": st_all["ticks"],
                         "rebuilds": st_all["rebuilds"]}}

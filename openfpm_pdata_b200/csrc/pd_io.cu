@@ -323,6 +323,23 @@ int pd_load(pd_vd h, const char* path) {
             set_error("load: %s has an invalid property table", path);
             return PD_EIO;
         }
+    // the file must hold exactly the data its header announces (checked before any allocation)
+    {
+        size_t need = 8 + sizeof(hdr) + 8 + 72 + sizeof(bc) + pd_.size() * 4;
+        const size_t esz = hdr[2] == PD_F64 ? 8 : 4;
+        need += (size_t)n * (3 * esz + 4) + 8;
+        for (unsigned p = 0; p < hdr[3]; ++p) need += (size_t)type_size(pd_[2 * p]) * pd_[2 * p + 1] * (size_t)n;
+        const long here = ftell(f.f);
+        if (here < 0 || fseek(f.f, 0, SEEK_END) != 0) {
+            set_error("load: cannot size %s", path);
+            return PD_EIO;
+        }
+        const long size = ftell(f.f);
+        if (size < 0 || (size_t)size != need || fseek(f.f, here, SEEK_SET) != 0) {
+            set_error("load: %s holds %ld bytes, its header announces %zu", path, size, need);
+            return PD_EIO;
+        }
+    }
     const bool add = h->props.empty() && hdr[3] > 0;
     if (!add) {
         bool same = h->props.size() == hdr[3];
