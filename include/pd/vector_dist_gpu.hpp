@@ -184,6 +184,14 @@ template <typename St> class vector_dist_gpu {
         if (prps.size() == 0) mask = ~0ul;
         check(pd_ghost_get(h_, mask, opt, stream_));
     }
+    // Ighost_get<prp...>(opt) / ghost_wait() -- vector_dist.hpp:2241-2291
+    void Ighost_get(std::initializer_list<int> prps = {}, int opt = PD_RUN_ON_DEVICE) {
+        unsigned long mask = 0;
+        for (int p : prps) mask |= 1ul << p;
+        if (prps.size() == 0) mask = ~0ul;
+        check(pd_ighost_get(h_, mask, opt, stream_));
+    }
+    void ghost_wait() { check(pd_ghost_wait(h_, stream_)); }
     // ghost_put<op_, prp...>() on one process -- vector_dist.hpp:2304 (op: PD_PUT_ADD / _MAX / _REPLACE)
     void ghost_put(std::initializer_list<int> prps = {}, int op = PD_PUT_ADD) {
         unsigned long mask = 0;

@@ -191,6 +191,14 @@ int pd_map(pd_vd h, int opt, void* stream);
  * PD_NO_POSITION only properties are refreshed.  prop_mask selects the
  * properties copied on a replay (bit p = property p; ~0 = all). */
 int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream);
+/* Ighost_get<prp...>(opt) / ghost_wait() -- vector_dist.hpp:2241-2291: the ghost
+ * exchange enqueued on `stream` without a host synchronisation (images written
+ * into the storage's spare room, sized from the previous count with a margin);
+ * ghost_wait reads the image count (one synchronisation) and, if the room was too
+ * small, redoes the exchange synchronously.  Between the two calls the vector's
+ * sizes are not final: make no other call on it. */
+int pd_ighost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream);
+int pd_ghost_wait(pd_vd h, void* stream);
 /* the (source, shift id) record of every ghost (o_part_loc) */
 int pd_ghost_records(pd_vd h, int* src, int* shift_id, long cap, long* n_img);
 /* ghost_put<op, prp...>(opt) on one process -- vector_dist.hpp:2304-2310 ->

@@ -352,6 +352,55 @@ int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream) {
     return PD_OK;
 }
 
+int pd_ighost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream) {
+    if (!h) return PD_EINVAL;
+    if (h->ghost_pending) {
+        set_error("Ighost_get: the previous Ighost_get was not waited for");
+        return PD_ESTATE;
+    }
+    cudaStream_t st = S(stream);
+    h->pend_mask = prop_mask;
+    h->pend_opt = opt;
+    if ((opt & PD_SKIP_LABELLING) && h->img_valid) {
+        PD_TRY(ghost_replay(h, prop_mask, !(opt & PD_NO_POSITION), nullptr, h->n_img, st));
+        h->ghost_pending = true;
+        h->pend_replay = true;
+        return PD_OK;
+    }
+    // images written without a host read of their count: room for the previous count
+    // with a margin (growing the storage, if needed, synchronises once here); an
+    // overflow is detected by ghost_wait, which then redoes the call synchronously
+    h->n_total = h->n_real;
+    h->img_valid = false;
+    const long want = h->n_img + h->n_img / 4 + 1024;
+    PD_TRY(ensure_capacity(h, h->n_real + want + 1, st));
+    if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
+    PD_TRY(ghost_generate(h, h->cap - h->n_real - 1, false, st));
+    h->ghost_pending = true;
+    h->pend_replay = false;
+    return PD_OK;
+}
+
+int pd_ghost_wait(pd_vd h, void* stream) {
+    if (!h) return PD_EINVAL;
+    if (!h->ghost_pending) return PD_OK;
+    cudaStream_t st = S(stream);
+    h->ghost_pending = false;
+    if (h->pend_replay) return cudaStreamSynchronize(st) == cudaSuccess ? PD_OK : PD_ECUDA;
+    PD_TRY(read_ctrl(h, st));
+    if (h->ctrl_h->err & ERR_IMG_OVERFLOW) {
+        h->ctrl_h->err &= ~ERR_IMG_OVERFLOW;
+        PD_CUDA(cudaMemcpyAsync(&h->ctrl->err, &h->ctrl_h->err, sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+        return pd_ghost_get(h, h->pend_mask, h->pend_opt & ~PD_SKIP_LABELLING, stream);
+    }
+    h->n_img = h->ctrl_h->n_img;
+    h->n_total = h->n_real + h->n_img;
+    h->img_valid = true;
+    h->img_gen_order = true;
+    h->epoch++;
+    return PD_OK;
+}
+
 int pd_ghost_put(pd_vd h, unsigned long prop_mask, int op, void* stream) {
     if (!h || (op != PD_PUT_ADD && op != PD_PUT_MAX && op != PD_PUT_REPLACE)) return PD_EINVAL;
     if (!h->img_valid || !h->img_gen_order) {

@@ -142,6 +142,10 @@ struct pd_vd_s {
     long n_img = 0;
     bool img_valid = false;
     bool img_gen_order = false;  // images in generation order (ghost_put can fold them)
+    bool ghost_pending = false;  // an Ighost_get waits for its ghost_wait
+    bool pend_replay = false;
+    unsigned long pend_mask = 0;
+    int pend_opt = 0;
     pd::Ctrl* ctrl = nullptr;    // device
     pd::Ctrl* ctrl_h = nullptr;  // pinned host mirror
     pd::Buf scan_scratch, tmp, tmp2, red;

@@ -121,6 +121,8 @@ def lib():
             "pd_verlet_create": ([vp, ctypes.c_double, P(vp)], ip),
             "pd_verlet_create_sym": ([vp, ctypes.c_double, P(vp)], ip),
             "pd_ghost_put": ([vp, ctypes.c_ulong, ip, vp], ip),
+            "pd_ighost_get": ([vp, ctypes.c_ulong, ip, vp], ip),
+            "pd_ghost_wait": ([vp, vp], ip),
             "pd_remove_marked": ([vp, ip, vp], ip),
             "pd_save": ([vp, ctypes.c_char_p], ip),
             "pd_selftest_wait": ([ctypes.c_long, ip, vp, vp], ip),
@@ -352,6 +354,14 @@ class VectorDist:
     def ghost_get(self, props=None, opt=RUN_ON_DEVICE):
         mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
         check(lib().pd_ghost_get(self.h, ctypes.c_ulong(mask), int(opt), None))
+
+    def Ighost_get(self, props=None, opt=RUN_ON_DEVICE, stream=None):
+        """Ighost_get<prp...>(opt): enqueue the ghost exchange without waiting for it."""
+        mask = (1 << 64) - 1 if props is None else sum(1 << p for p in props)
+        check(lib().pd_ighost_get(self.h, ctypes.c_ulong(mask), int(opt), stream))
+
+    def ghost_wait(self, stream=None):
+        check(lib().pd_ghost_wait(self.h, stream))
 
     def ghost_put(self, props=None, op=PUT_ADD):
         """ghost_put<op_, prp...>(): merge every ghost's values onto its source."""

@@ -118,3 +118,52 @@ def test_ghost_get_mixed_boundaries(pd, orc, bc):
     assert np.array_equal(got, img)
     gsrc, gshf = vd.ghost_records()
     assert np.array_equal(gsrc, src) and np.array_equal(gshf, shf)
+
+
+def test_ighost_get_equals_ghost_get(pd):
+    """Ighost_get + ghost_wait (vector_dist.hpp:2241-2291) give the images of
+    ghost_get bit for bit: the first call overflows its estimated room (no
+    previous count) and is redone synchronously, the second fits; the
+    SKIP_LABELLING replay refreshes moved sources."""
+    rng = np.random.default_rng(9)
+    n = 40000
+    x = rng.random((n, 3))
+    p = rng.normal(size=(n, 3))
+
+    def make():
+        vd = pd.VectorDist(n, np.zeros(3), np.ones(3), np.ones(3, np.int32), 0.1, dtype=F64,
+                           props=[(pd.PD_F64, 3)])
+        vd.hostToDevicePos(x)
+        vd.hostToDeviceProp(0, p)
+        vd.map()
+        return vd
+    a, b = make(), make()
+    a.ghost_get()
+    b.Ighost_get()
+    b.ghost_wait()
+    assert b.size_local_with_ghost() == a.size_local_with_ghost() > n
+    assert np.array_equal(b.deviceToHostPos(), a.deviceToHostPos())
+    assert np.array_equal(b.deviceToHostProp(0), a.deviceToHostProp(0))
+    assert all(np.array_equal(u, w) for u, w in zip(b.ghost_records(), a.ghost_records()))
+    # second exchange after a small move: the room from the first count suffices
+    x2 = x + rng.uniform(-0.01, 0.01, size=x.shape)
+    for vd in (a, b):
+        vd.hostToDevicePos(x2)
+        vd.map()
+    a.ghost_get()
+    b.Ighost_get()
+    b.ghost_wait()
+    assert np.array_equal(b.deviceToHostPos(), a.deviceToHostPos())
+    # replay of the same images after the sources' properties changed
+    p2 = rng.normal(size=(n, 3))
+    for vd in (a, b):
+        vd.hostToDeviceProp(0, p2)
+    a.ghost_get([0], opt=pd.RUN_ON_DEVICE | pd.SKIP_LABELLING)
+    b.Ighost_get([0], opt=pd.RUN_ON_DEVICE | pd.SKIP_LABELLING)
+    b.ghost_wait()
+    assert np.array_equal(b.deviceToHostProp(0), a.deviceToHostProp(0))
+    # a second Ighost_get before the wait is refused
+    b.Ighost_get()
+    with pytest.raises(RuntimeError):
+        b.Ighost_get()
+    b.ghost_wait()
