@@ -5,7 +5,8 @@
 //   vector_dist_gpu<3,St,aggregate<...>> vd(n, box, bc, ghost);
 // with
 //   pd::vector_dist_gpu<St> vd(n, lo, hi, bc, ghost, {{PD_F64,3}, ...});
-// and keeps the calls: getPos/getProp (host mirror), hostToDevicePos/Prop,
+// and keeps the calls: getPos/getProp (host mirror), add/getLastPos/getLastProp,
+// hostToDevicePos/Prop,
 // map, ghost_get, getCellListGPU/updateCellListGPU/restoreOrder,
 // getVerlet/updateVerlet, getDomainIteratorGPU, toKernel.  Errors throw
 // std::runtime_error with the library's message (the reference's
@@ -13,6 +14,7 @@
 // device transfer is explicit, as in the reference.
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <cstdint>
 #include <memory>
@@ -102,17 +104,43 @@ template <typename St> class vector_dist_gpu {
     pd_vd h_ = nullptr;
     std::vector<prop_desc> props_;
     std::vector<St> pos_;                      // host mirror, AoS xyz
-    std::vector<std::vector<unsigned char>> prp_;  // host mirrors, component-major
+    std::vector<std::vector<unsigned char>> prp_;  // host mirrors, component-major [ncomp][mcap_]
+    long mcap_ = 0;                            // particles the host mirrors hold room for
+    long pending_ = 0;                         // particles added on the host, not yet on the device
     void* stream_ = nullptr;
 
     long size_all() const {
         long a = 0, b = 0;
         check(pd_size(h_, &a, &b));
+        return b + pending_;
+    }
+    // room for n particles in the host mirrors (component columns moved to the new stride)
+    void mirror(long n) {
+        if (n <= mcap_) return;
+        long nc = std::max<long>(n, 2 * mcap_);
+        pos_.resize(3 * (size_t)nc);
+        for (size_t p = 0; p < props_.size(); ++p) {
+            const size_t es = (size_t)type_bytes(props_[p].type);
+            std::vector<unsigned char> t((size_t)nc * props_[p].ncomp * es, 0);
+            for (int c = 0; c < props_[p].ncomp && mcap_ > 0; ++c)
+                std::copy(prp_[p].begin() + (size_t)c * mcap_ * es, prp_[p].begin() + (size_t)(c + 1) * mcap_ * es,
+                          t.begin() + (size_t)c * nc * es);
+            prp_[p].swap(t);
+        }
+        mcap_ = nc;
+    }
+    long device_all() const {
+        long a = 0, b = 0;
+        check(pd_size(h_, &a, &b));
         return b;
     }
-    void mirror(long n) {
-        pos_.resize(3 * n);
-        for (size_t p = 0; p < props_.size(); ++p) prp_[p].resize((size_t)n * props_[p].ncomp * type_bytes(props_[p].type));
+    // the device vector takes the particles added on the host
+    void flush_added() {
+        if (pending_ == 0) return;
+        long a = 0, b = 0;
+        check(pd_size(h_, &a, &b));
+        check(pd_resize(h_, a + pending_));
+        pending_ = 0;
     }
 
   public:
@@ -141,38 +169,55 @@ template <typename St> class vector_dist_gpu {
     long size_local() const {
         long a = 0, b = 0;
         check(pd_size(h_, &a, &b));
-        return a;
+        return a + pending_;
     }
     long size_local_with_ghost() const { return size_all(); }
 
     // host mirror accessors (getPos(p)[k], getProp<prp>(p)[k])
     St* getPos(long p) { return pos_.data() + 3 * p; }
     template <typename T> T& getProp(int prp, long p, int comp = 0) {
-        long cap = (long)(prp_[prp].size() / (props_[prp].ncomp * type_bytes(props_[prp].type)));
-        return reinterpret_cast<T*>(prp_[prp].data())[(long)comp * cap + p];
+        return reinterpret_cast<T*>(prp_[prp].data())[(long)comp * mcap_ + p];
     }
+    // add() / getLastPos() / getLastProp -- vector_dist.hpp:923-984: a particle appended
+    // on the host; the device vector takes it at the next hostToDevicePos/Prop
+    void add() {
+        mirror(size_local() + 1);
+        ++pending_;
+    }
+    St* getLastPos() { return getPos(size_local() - 1); }
+    template <typename T> T& getLastProp(int prp, int comp = 0) { return getProp<T>(prp, size_local() - 1, comp); }
 
-    void hostToDevicePos() { check(pd_h2d_pos(h_, pos_.data(), 0, size_local(), stream_)); }
+    void hostToDevicePos() {
+        flush_added();
+        check(pd_h2d_pos(h_, pos_.data(), 0, size_local(), stream_));
+    }
     void deviceToHostPos() {
-        long n = size_all();
+        long n = device_all();
         mirror(n);
         if (n) check(pd_d2h_pos(h_, pos_.data(), 0, n, stream_));
     }
     void hostToDeviceProp(int prp) {
+        flush_added();
         long n = size_local();
-        long cap = (long)(prp_[prp].size() / (props_[prp].ncomp * type_bytes(props_[prp].type)));
-        // pack [ncomp][n] from the [ncomp][cap] mirror
+        // pack [ncomp][n] from the [ncomp][mcap_] mirror
         std::vector<unsigned char> tmp((size_t)n * props_[prp].ncomp * type_bytes(props_[prp].type));
         int es = type_bytes(props_[prp].type);
         for (int c = 0; c < props_[prp].ncomp; ++c)
-            std::copy(prp_[prp].begin() + (size_t)c * cap * es, prp_[prp].begin() + ((size_t)c * cap + n) * es,
+            std::copy(prp_[prp].begin() + (size_t)c * mcap_ * es, prp_[prp].begin() + ((size_t)c * mcap_ + n) * es,
                       tmp.begin() + (size_t)c * n * es);
         check(pd_h2d_prop(h_, prp, tmp.data(), 0, n, stream_));
     }
     void deviceToHostProp(int prp) {
-        long n = size_all();
+        long n = device_all();
         mirror(n);
-        if (n) check(pd_d2h_prop(h_, prp, prp_[prp].data(), 0, n, stream_));
+        if (n == 0) return;
+        // [ncomp][n] from the device, spread to the [ncomp][mcap_] mirror
+        const int es = type_bytes(props_[prp].type);
+        std::vector<unsigned char> tmp((size_t)n * props_[prp].ncomp * es);
+        check(pd_d2h_prop(h_, prp, tmp.data(), 0, n, stream_));
+        for (int c = 0; c < props_[prp].ncomp; ++c)
+            std::copy(tmp.begin() + (size_t)c * n * es, tmp.begin() + (size_t)(c + 1) * n * es,
+                      prp_[prp].begin() + (size_t)c * mcap_ * es);
     }
 
     // map(RUN_ON_DEVICE) -- vector_dist.hpp:2158

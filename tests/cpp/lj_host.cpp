@@ -13,14 +13,17 @@ int main(int argc, char** argv) {
     long n;
     double L;
     if (scanf("%ld %lf", &n, &L) != 2) return 2;
-    pd::vector_dist_gpu<double> vd(n, {0, 0, 0}, {L, L, L}, {PD_PERIODIC, PD_PERIODIC, PD_PERIODIC},
+    // an empty vector filled with add() / getLastPos() / getLastProp, as the reference's examples do
+    pd::vector_dist_gpu<double> vd(0, {0, 0, 0}, {L, L, L}, {PD_PERIODIC, PD_PERIODIC, PD_PERIODIC},
                                    {2.8, 2.8, 2.8}, {{PD_F64, 3}, {PD_F64, 3}});
     for (long i = 0; i < n; ++i) {
-        double* x = vd.getPos(i);
+        vd.add();
+        double* x = vd.getLastPos();
         double v[3];
         if (scanf("%lf %lf %lf %lf %lf %lf", &x[0], &x[1], &x[2], &v[0], &v[1], &v[2]) != 6) return 2;
-        for (int d = 0; d < 3; ++d) vd.getProp<double>(0, i, d) = v[d];
+        for (int d = 0; d < 3; ++d) vd.getLastProp<double>(0, d) = v[d];
     }
+    if (vd.size_local() != n) return 3;
     vd.hostToDevicePos();
     vd.hostToDeviceProp(0);
     vd.map();
