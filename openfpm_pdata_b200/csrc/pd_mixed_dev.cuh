@@ -143,28 +143,36 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
         }
         __syncthreads();
         const unsigned int base = S.oR[4] - S.cR[4][0];
-        const int sub = threadIdx.x % P;
-        const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
-        for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
-            const unsigned int i = ib + t / P;
-            const bool active = i < ie;
+        // rounds of the whole CTA over the tile's particles: P lanes per row while a
+        // round is full, more lanes per row (up to a warp) in the last, partial round;
+        // every thread takes part in every round (the shuffles need whole warps)
+        unsigned int first = ib;
+        while (first < ie) {
+            const unsigned int left = ie - first;
+            unsigned int q = P;
+            while (q < 32u && left * (q << 1) <= (unsigned int)FBLOCK_T) q <<= 1;
+            const unsigned int cnt = min(left, (unsigned int)FBLOCK_T / q);
+            const int sub = (int)(threadIdx.x % q);
+            const int Q = (int)q;
+            const bool active = threadIdx.x / q < cnt;
+            const unsigned int i = first + (active ? threadIdx.x / q : 0u);
             const unsigned int li = base + i;
-            const float4 xi = sm[active ? li : 0];
+            const float4 xi = sm[li];
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             Kahan kx = {0.f, 0.f}, ky = {0.f, 0.f}, kz = {0.f, 0.f}, ke = {0.f, 0.f}, kw = {0.f, 0.f};
             const unsigned int* row = nbr + i;
             // row words read four iterations ahead (register shift ring) to cover the memory latency
             unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
-            unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
-            unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
-            unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
+            unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+            unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+            unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
 #pragma unroll 2
-            for (int k = sub; k < words; k += P) {
+            for (int k = sub; k < words; k += Q) {
                 const unsigned int pair = q0;
                 q0 = q1;
                 q1 = q2;
                 q2 = q3;
-                q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
+                q3 = k + 4 * Q < words ? __ldg(row + (long)(k + 4 * Q) * stride) : 0u;
                 float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -192,8 +200,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                 kw.add(w);
             }
             double Fx = kx.value(), Fy = ky.value(), Fz = kz.value(), Ee = ke.value(), Ww = kw.value();
-#pragma unroll
-            for (int o = 1; o < P; o <<= 1) {
+            for (unsigned int o = 1; o < q; o <<= 1) {
                 Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
                 Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
                 Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
@@ -207,6 +214,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                 pe += 0.5 * Ee;
                 vir += 0.5 * Ww;
             }
+            first += cnt;
         }
     }
     return false;

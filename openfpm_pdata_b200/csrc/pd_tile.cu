@@ -121,7 +121,8 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build3(const typename V4<T>::t
 }
 
 // P threads per domain particle split its row (words w = sub, sub+P, ...; two
-// entries per word); partial sums meet through shuffles.  Energies: one FP64
+// entries per word) -- more in a tile's last, partial round; partial sums meet
+// through shuffles.  Energies: one FP64
 // partial per block (fixed-order tree), reduced in fixed order afterwards.
 template <class T, bool ENERGY, int P>
 __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::type* __restrict__ pos, long n_real,
@@ -141,29 +142,38 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
     bool staged = ib != ie && tile_stage<T>(pos, pos + n_real, S, sm, cap, err);
     if (staged) {
         const unsigned int base = S.oR[4] - S.cR[4][0];
-        const int sub = threadIdx.x % P;
-        // whole warps iterate together (the shuffles below need all 32 lanes)
-        const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
-        for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
-            const unsigned int i = ib + t / P;
-            const bool active = i < ie;
+        // Rounds of the whole CTA over the tile's domain particles: P lanes share a
+        // row while a round is full; the last, partial round spreads its particles
+        // over more lanes (up to a warp each) so that it ends about as soon as the
+        // full ones instead of leaving most warps idle at the block's barrier.
+        // Every thread takes part in every round (the shuffles need whole warps).
+        unsigned int first = ib;
+        while (first < ie) {
+            const unsigned int left = ie - first;
+            unsigned int q = P;
+            while (q < 32u && left * (q << 1) <= (unsigned int)FBLOCK_T) q <<= 1;
+            const unsigned int cnt = min(left, (unsigned int)FBLOCK_T / q);
+            const int sub = (int)(threadIdx.x % q);
+            const bool active = threadIdx.x / q < cnt;
+            const unsigned int i = first + (active ? threadIdx.x / q : 0u);
             const unsigned int li = base + i;
-            T4 xi = sm[active ? li : 0];
+            T4 xi = sm[li];
             const int words = active ? (nn[i] + 1) >> 1 : 0;
+            const int Q = (int)q;
             T fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             const unsigned int* row = nbr + i;
             // row words read four iterations ahead (register shift ring) to cover the memory latency
             unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
-            unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
-            unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
-            unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
+            unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+            unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+            unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
 #pragma unroll 2
-            for (int k = sub; k < words; k += P) {
+            for (int k = sub; k < words; k += Q) {
                 const unsigned int pair = q0;
                 q0 = q1;
                 q1 = q2;
                 q2 = q3;
-                q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
+                q3 = k + 4 * Q < words ? __ldg(row + (long)(k + 4 * Q) * stride) : 0u;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
@@ -185,8 +195,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
                     }
                 }
             }
-#pragma unroll
-            for (int o = 1; o < P; o <<= 1) {
+            for (unsigned int o = 1; o < q; o <<= 1) {
                 fx += __shfl_xor_sync(0xffffffffu, fx, o);
                 fy += __shfl_xor_sync(0xffffffffu, fy, o);
                 fz += __shfl_xor_sync(0xffffffffu, fz, o);
@@ -204,6 +213,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
                     vir += 0.5 * (double)w;
                 }
             }
+            first += cnt;
         }
     }
     if (ENERGY) {
