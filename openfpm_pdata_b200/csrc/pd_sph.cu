@@ -218,29 +218,37 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
     if (!__syncthreads_and(waited ? 1 : 0)) return;
 
     const unsigned int base = S.oR[4] - S.cR[4][0];
-    const int sub = threadIdx.x % P;
-    const unsigned int span = (((ie - ib) * P + 31u) / 32u) * 32u;
-    for (unsigned int t = threadIdx.x; t < span; t += FBLOCK_T) {
-        const unsigned int i = ib + t / P;
-        const bool active = i < ie;
+    // rounds of the whole CTA over the tile's particles: P lanes per row while a
+    // round is full, more lanes per row (up to a warp) in the last, partial round;
+    // every thread takes part in every round (the shuffles need whole warps)
+    unsigned int first = ib;
+    while (first < ie) {
+        const unsigned int left = ie - first;
+        unsigned int q = P;
+        while (q < 32u && left * (q << 1) <= (unsigned int)FBLOCK_T) q <<= 1;
+        const unsigned int cnt = min(left, (unsigned int)FBLOCK_T / q);
+        const int sub = (int)(threadIdx.x % q);
+        const int Q = (int)q;
+        const bool active = threadIdx.x / q < cnt;
+        const unsigned int i = first + (active ? threadIdx.x / q : 0u);
         const unsigned int li = base + i;
-        const T4 xi = sp[active ? li : 0];
-        const T4 ai = sa[active ? li : 0];
+        const T4 xi = sp[li];
+        const T4 ai = sa[li];
         const T pa_r = xi.w;
         const int words = active ? (nn[i] + 1) >> 1 : 0;
         T ax = 0, ay = 0, az = 0, dr = 0;
         const unsigned int* row = nbr + i;
         // row words read four iterations ahead (register shift ring)
         unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
-        unsigned int q1 = sub + P < words ? __ldg(row + (long)(sub + P) * stride) : 0u;
-        unsigned int q2 = sub + 2 * P < words ? __ldg(row + (long)(sub + 2 * P) * stride) : 0u;
-        unsigned int q3 = sub + 3 * P < words ? __ldg(row + (long)(sub + 3 * P) * stride) : 0u;
-        for (int k = sub; k < words; k += P) {
+        unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+        unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+        unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
+        for (int k = sub; k < words; k += Q) {
             const unsigned int pair = q0;
             q0 = q1;
             q1 = q2;
             q2 = q3;
-            q3 = k + 4 * P < words ? __ldg(row + (long)(k + 4 * P) * stride) : 0u;
+            q3 = k + 4 * Q < words ? __ldg(row + (long)(k + 4 * Q) * stride) : 0u;
 #pragma unroll
             for (int hh = 0; hh < 2; ++hh) {
                 const unsigned int l = hh ? (pair >> 16) : (pair & 0xffffu);
@@ -266,8 +274,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
                 }
             }
         }
-#pragma unroll
-        for (int o = 1; o < P; o <<= 1) {
+        for (unsigned int o = 1; o < q; o <<= 1) {
             ax += __shfl_xor_sync(0xffffffffu, ax, o);
             ay += __shfl_xor_sync(0xffffffffu, ay, o);
             az += __shfl_xor_sync(0xffffffffu, az, o);
@@ -280,6 +287,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
             acc[2 * cap_p + i] = fluid ? az + K.gz : T(0);
             drho[i] = dr;
         }
+        first += cnt;
     }
 }
 
