@@ -165,15 +165,13 @@ __device__ __forceinline__ void tile_rows(const TileSh& S, const unsigned int (*
             for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
                 const float4 xq = sm[q];
                 const float d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
-                if (d2 < hi_thr) {
-                    if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
-                        if (cnt < max_nn) {
-                            if (cnt & 1) out[(long)(cnt >> 1) * stride] = pend | (q << 16);
-                            else pend = q;
-                        }
-                        cnt++;
-                    }
-                }
+                // accept without a divergent branch (the rare band candidates aside)
+                bool acc = d2 < lo_thr;
+                if (!acc && d2 < hi_thr) acc = exact_in<T>(pos, i, __float_as_int(xq.w), r2);
+                const bool odd = (cnt & 1) != 0;
+                if (acc && odd && cnt < max_nn) out[(long)(cnt >> 1) * stride] = pend | (q << 16);
+                pend = (acc && !odd) ? q : pend;
+                cnt += acc ? 1 : 0;
             }
         }
         // odd rows end with the particle itself, which the pair kernel skips
@@ -266,15 +264,14 @@ __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned
                 for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
                     const float4 xq = sm[q - base];
                     const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
-                    if (d2 < hi_thr) {
-                        if (d2 < lo_thr || exact_in<T>(pos, i, __float_as_int(xq.w), r2)) {
-                            if (c < max_nn) {
-                                if (c & 1) out[(long)(c >> 1) * stride] = pd_ | (q << 16);
-                                else pd_ = q;
-                            }
-                            c++;
-                        }
-                    }
+                    // accept without a divergent branch (the rare band candidates aside):
+                    // the pending half-word and the count by selects, the word store predicated
+                    bool acc = d2 < lo_thr;
+                    if (!acc && d2 < hi_thr) acc = exact_in<T>(pos, i, __float_as_int(xq.w), r2);
+                    const bool odd = (c & 1) != 0;
+                    if (acc && odd && c < max_nn) out[(long)(c >> 1) * stride] = pd_ | (q << 16);
+                    pd_ = (acc && !odd) ? q : pd_;
+                    c += acc ? 1 : 0;
                 }
             }
             cnt[m] = c;
