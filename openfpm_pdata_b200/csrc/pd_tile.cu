@@ -180,18 +180,19 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
                     T4 xq = sm[l];
                     T dx = xi.x - xq.x, dy = xi.y - xq.y, dz = xi.z - xq.z;
                     T r2 = dist2(dx, dy, dz);
-                    if (r2 < Pr.rc2 && l != li) {
-                        T ir2 = recip(r2);
-                        T s2 = Pr.sig2 * ir2;
-                        T s6 = s2 * s2 * s2;
-                        T ff = Pr.eps24 * ir2 * s6 * (T(2) * s6 - T(1));
-                        fx += ff * dx;
-                        fy += ff * dy;
-                        fz += ff * dz;
-                        if (ENERGY) {
-                            e += Pr.eps4 * s6 * (s6 - T(1));
-                            w += ff * r2;
-                        }
+                    // every pair through the same instructions (most lanes of a warp have a
+                    // pair inside the cutoff at every step); the others contribute zero
+                    const bool in = r2 < Pr.rc2 && l != li;
+                    const T ir2 = recip(in ? r2 : T(1));
+                    const T s2 = Pr.sig2 * ir2;
+                    const T s6 = s2 * s2 * s2;
+                    const T ff = in ? Pr.eps24 * ir2 * s6 * (T(2) * s6 - T(1)) : T(0);
+                    fx += ff * dx;
+                    fy += ff * dy;
+                    fz += ff * dz;
+                    if (ENERGY) {
+                        e += in ? Pr.eps4 * s6 * (s6 - T(1)) : T(0);
+                        w += ff * r2;
                     }
                 }
             }
