@@ -181,17 +181,17 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                     const float dx = fmaf(xi.w - xq.w, sx, xi.x - xq.x);
                     const float dy = xi.y - xq.y, dz = xi.z - xq.z;
                     const float r2 = dist2(dx, dy, dz);
-                    if (r2 < Pr.rc2 && l != li) {
-                        float ir2 = recip(r2);
-                        float s2 = Pr.sig2 * ir2;
-                        float s6 = s2 * s2 * s2;
-                        float ff = Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f);
-                        fx += ff * dx;
-                        fy += ff * dy;
-                        fz += ff * dz;
-                        e += Pr.eps4 * s6 * (s6 - 1.f);
-                        w += ff * r2;
-                    }
+                    // every pair through the same instructions; pairs outside select zero
+                    const bool in = r2 < Pr.rc2 && l != li;
+                    const float ir2 = recip(in ? r2 : 1.f);
+                    const float s2 = Pr.sig2 * ir2;
+                    const float s6 = s2 * s2 * s2;
+                    const float ff = in ? Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f) : 0.f;
+                    fx += ff * dx;
+                    fy += ff * dy;
+                    fz += ff * dz;
+                    e += in ? Pr.eps4 * s6 * (s6 - 1.f) : 0.f;
+                    w += ff * r2;
                 }
                 kx.add(fx);
                 ky.add(fy);
