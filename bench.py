@@ -668,22 +668,33 @@ def main():
     if rank == 0 and world == 1 and not a.no_e2e:
         # end to end through the public C ABI: pinned host buffers in, K steps, energies and
         # final state out; wall clock around create + H2D + run + D2H
+        # host data in the ABI's layouts (positions [n][3], velocities [3][n]) in pinned memory
         xp = torch.from_numpy(x).pin_memory().numpy()
-        vp = torch.from_numpy(v).pin_memory().numpy()
+        vt = np.ascontiguousarray(v.T.astype(np.float32 if mixed else np.float64))
+        vp = torch.from_numpy(vt).pin_memory().numpy()
+        xo = torch.empty(x.shape, dtype=torch.float64).pin_memory().numpy()
+        vo = torch.empty(vt.shape, dtype=torch.float32 if mixed else torch.float64).pin_memory().numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        vd2, md2 = build_system(pd, xp, vp, L)
+        lo2, hi2, bc2 = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+        pt2 = pd.PD_F32 if mixed else pd.PD_F64
+        vd2 = pd.VectorDist(n, lo2, hi2, bc2, R_CUT + SKIN, dtype=np.float64, props=[(pt2, 3), (pt2, 3)])
+        vd2.hostToDevicePos(xp)
+        vd2.hostToDevicePropSoA(0, vp)
+        md2 = pd.MD(vd2, 0, 1, dt=DT, mass=MASS, skin=SKIN, eps=EPS, sigma=SIGMA, r_cut=R_CUT,
+                    precision=pd.PREC_MIXED if mixed else pd.PREC_FP64)
+        md2.set_tiles(bool(TUNE["tiles"]), TUNE["tx"], TUNE["tpp"])
         E2 = md2.run(a.steps)
-        xo = vd2.deviceToHostPos(with_ghost=False)
-        vo = vd2.deviceToHostProp(0, with_ghost=False)
+        vd2.deviceToHostPos(with_ghost=False, out=xo)
+        vd2.deviceToHostPropSoA(0, out=vo, with_ghost=False)
         torch.cuda.synchronize()
         t_e2e = time.perf_counter() - t0
         del md2, vd2
         out["e2e"] = {"value": n * a.steps / t_e2e, "unit": METRIC,
                       "h2d_bytes_per_step": (x.nbytes + v.nbytes) / a.steps,
                       "d2h_bytes_per_step": 32 + (xo.nbytes + vo.nbytes) / a.steps,
-                      "includes": "create, H2D of positions+velocities, first list build, K steps, "
-                                  "per-step energies and final state D2H"}
+                      "includes": "create, H2D of positions+velocities from pinned memory, first list build, "
+                                  "K steps, per-step energies and final state D2H into pinned memory"}
         assert np.isfinite(E2).all()
 
     if rank == 0 and world == 1 and a.forms != "none":

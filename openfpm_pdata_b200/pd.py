@@ -320,9 +320,13 @@ class VectorDist:
         x = np.ascontiguousarray(x, dtype=self.dtype).reshape(-1, 3)
         check(lib().pd_h2d_pos(self.h, _ptr(x), int(offset), int(x.shape[0]), None))
 
-    def deviceToHostPos(self, offset=0, count=None, with_ghost=True):
+    def deviceToHostPos(self, offset=0, count=None, with_ghost=True, out=None):
+        """positions [n][3]; `out` (e.g. pinned memory) receives them when given"""
         n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
-        out = np.zeros((n, 3), self.dtype)
+        if out is None:
+            out = np.zeros((n, 3), self.dtype)
+        elif out.dtype != self.dtype or not out.flags.c_contiguous or out.size < 3 * n:
+            raise ValueError("deviceToHostPos: out must be C-contiguous, of the vector's dtype, with room for n x 3")
         if n:
             check(lib().pd_d2h_pos(self.h, _ptr(out), int(offset), int(n), None))
         return out
@@ -332,6 +336,26 @@ class VectorDist:
         a = np.asarray(a, dtype=_NP[t]).reshape(-1, nc)
         cm = np.ascontiguousarray(a.T)
         check(lib().pd_h2d_prop(self.h, int(p), _ptr(cm), int(offset), int(a.shape[0]), None))
+
+    def hostToDevicePropSoA(self, p, cm, offset=0):
+        """property p from component-major host data [ncomp][n] (the ABI's layout: no
+        transpose, so pinned memory is copied directly)"""
+        t, nc = self.props[p]
+        if cm.dtype != _NP[t] or not cm.flags.c_contiguous or cm.shape[0] != nc:
+            raise ValueError("hostToDevicePropSoA: C-contiguous [ncomp][n] array of the property's type expected")
+        check(lib().pd_h2d_prop(self.h, int(p), _ptr(cm), int(offset), int(cm.shape[1]), None))
+
+    def deviceToHostPropSoA(self, p, out=None, offset=0, count=None, with_ghost=True):
+        """property p as component-major [ncomp][n] (into `out` when given)"""
+        t, nc = self.props[p]
+        n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
+        if out is None:
+            out = np.zeros((nc, n), _NP[t])
+        elif out.dtype != _NP[t] or not out.flags.c_contiguous or out.shape != (nc, n):
+            raise ValueError("deviceToHostPropSoA: C-contiguous [ncomp][n] output of the property's type expected")
+        if n:
+            check(lib().pd_d2h_prop(self.h, int(p), _ptr(out), int(offset), int(n), None))
+        return out
 
     def deviceToHostProp(self, p, offset=0, count=None, with_ghost=True):
         t, nc = self.props[p]
