@@ -8,6 +8,7 @@
 //   props  one allocation per property, component-major [ncomp][cap].
 // Real particles occupy [0, n_real) (the reference's ghostMarker), periodic
 // images [n_real, n_total).
+#include <algorithm>
 #include <cstdarg>
 #include <mutex>
 
@@ -47,6 +48,10 @@ void dev_free(void* p) {
 
 int Buf::ensure(size_t b) {
     if (b <= bytes && p) return PD_OK;
+    // a buffer that has to grow grows by a quarter at least: sizes that creep up
+    // from one rebuild to the next (images, rows, staging) reallocate rarely, and a
+    // reallocation outside a stream-ordered pool synchronises the device
+    if (p && bytes > 0) b = std::max(b, bytes + bytes / 4);
     dev_free(p);
     p = nullptr;
     bytes = 0;
