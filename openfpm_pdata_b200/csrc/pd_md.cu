@@ -850,6 +850,7 @@ int pd_md_destroy(pd_md md) {
 
 int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     if (!md || steps < 0) return PD_EINVAL;
+    if (md_cluster_eligible(md)) return md_run_cluster(md, steps, S(stream), E);
     if (md->mp.use_cell_list && md->physics == 0 && !md->mixed && !md->timing)
         return md_run_cl_graph(md, steps, S(stream), E);
     pd_vd h = md->h;

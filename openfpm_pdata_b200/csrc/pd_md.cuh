@@ -52,4 +52,7 @@ int force_blocks(long n);
 int md_rebuild(pd_md md, cudaStream_t st);
 // forces of the current state into the force property
 int md_forces(pd_md md, cudaStream_t st);
+// cell-list mode of a small system: every step of a run in one thread-block cluster (pd_cluster.cu)
+bool md_cluster_eligible(pd_md md);
+int md_run_cluster(pd_md md, int steps, cudaStream_t st, double* E);
 }  // namespace pd
