@@ -638,6 +638,7 @@ def main():
     rho = n / (L * L * L)
     in_cut = 4.18879 * R_CUT ** 3 * rho
     flops = n * (8 * mean_nn + 29 * in_cut)
+    fma_peak = pd.measure_fma_rate(pd.PD_F32 if mixed else pd.PD_F64)
     kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_f64" if a.tiles else "k_lj_verlet_f64")
     traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
 
@@ -658,8 +659,10 @@ def main():
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0,
                      "arith": {"unit": "TFLOP/s", "dtype": "f32" if mixed else "f64",
                                "achieved": flops / f_avg_s / 1e12, "flops_per_launch": flops,
-                               "nominal_peak": 75.0 if mixed else 37.0,
-                               "peak_kind": "nominal per-GPU vector FP32/FP64 figure, not measured on this pool"}},
+                               "peak": fma_peak, "frac": flops / f_avg_s / 1e12 / fma_peak,
+                               "peak_kind": "measured: vector FMA throughput kernel on this GPU "
+                                            "(pd_measure_fma_rate, an FMA counts two flops)",
+                               "nominal_peak": 75.0 if mixed else 37.0}},
         "phases_ms_per_step": {k: (tv[0] / max(tv[1], 1)) for k, tv in timers.items()},
         "gpu_launches": int(launches),
         "clocks": ck,

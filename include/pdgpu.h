@@ -241,6 +241,9 @@ int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end
  * nothing completes the phase: the wait gives up, the kernel records the timeout
  * and returns, and the call returns PD_ETIMEOUT with the context still usable. */
 int pd_selftest_wait(long limit, int issue_copy, const float* in4, float* out4);
+/* Measured vector FMA throughput of this GPU in TFLOP/s (an FMA counts two flops),
+ * FP32 or FP64: the denominator of the pair kernels' arithmetic roofline. */
+int pd_measure_fma_rate(int dtype, double* tflops);
 /* save(filename) / load(filename) -- vector_dist.hpp:2459-2476: the domain
  * particles (positions, global ids, properties) in this library's own binary
  * checkpoint format (checksummed); load replaces the particles of a vector of

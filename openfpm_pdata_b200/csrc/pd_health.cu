@@ -31,6 +31,50 @@ __global__ void k_wait_selftest(const float4* __restrict__ src, float4* __restri
     }
 }
 
+// Vector FMA throughput: eight independent chains per thread (enough in flight to
+// hide the pipeline latency), a*b+c with b, c fixed; each FMA counts two flops.
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_rate(T* __restrict__ out, int iters, T b, T c) {
+    T a0 = (T)threadIdx.x, a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3), a4 = a0 + T(4), a5 = a0 + T(5),
+      a6 = a0 + T(6), a7 = a0 + T(7);
+    for (int k = 0; k < iters; ++k) {
+        a0 = fma(a0, b, c);
+        a1 = fma(a1, b, c);
+        a2 = fma(a2, b, c);
+        a3 = fma(a3, b, c);
+        a4 = fma(a4, b, c);
+        a5 = fma(a5, b, c);
+        a6 = fma(a6, b, c);
+        a7 = fma(a7, b, c);
+    }
+    out[blockIdx.x * (long)blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+
+template <class T> static int fma_rate(double* tflops) {
+    int dev = 0, sms = 148;
+    PD_CUDA(cudaGetDevice(&dev));
+    PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    Buf out;
+    PD_TRY(out.ensure(sizeof(T) * (size_t)blocks * threads));
+    cudaEvent_t e0, e1;
+    PD_CUDA(cudaEventCreate(&e0));
+    PD_CUDA(cudaEventCreate(&e1));
+    const T b = (T)0.999999, c = (T)1e-7;
+    pd::launch(k_fma_rate<T>, blocks, threads, 0, (cudaStream_t)0, out.as<T>(), iters, b, c);  // warm-up
+    PD_CUDA(cudaEventRecord(e0, 0));
+    pd::launch(k_fma_rate<T>, blocks, threads, 0, (cudaStream_t)0, out.as<T>(), iters, b, c);
+    PD_CUDA(cudaEventRecord(e1, 0));
+    PD_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    PD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    out.release();
+    *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
+    return PD_OK;
+}
+
 }  // namespace pd
 
 using namespace pd;
@@ -64,6 +108,11 @@ int pd_selftest_wait(long limit, int issue_copy, const float* in4, float* out4) 
         return PD_ETIMEOUT;
     }
     return PD_OK;
+}
+
+int pd_measure_fma_rate(int dtype, double* tflops) {
+    if (!tflops || (dtype != PD_F32 && dtype != PD_F64)) return PD_EINVAL;
+    return dtype == PD_F64 ? fma_rate<double>(tflops) : fma_rate<float>(tflops);
 }
 
 }  // extern "C"

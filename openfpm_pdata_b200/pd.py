@@ -126,6 +126,7 @@ def lib():
             "pd_remove_marked": ([vp, ip, vp], ip),
             "pd_save": ([vp, ctypes.c_char_p], ip),
             "pd_selftest_wait": ([ctypes.c_long, ip, vp, vp], ip),
+            "pd_measure_fma_rate": ([ip, P(ctypes.c_double)], ip),
             "pd_load": ([vp, ctypes.c_char_p], ip),
             "pd_write": ([vp, ctypes.c_char_p, ctypes.c_char_p, ip], ip),
             "pd_write_frame": ([vp, ctypes.c_char_p, ctypes.c_long, ctypes.c_char_p, ip], ip),
@@ -666,3 +667,10 @@ def selftest_wait(limit, issue_copy):
     out = np.zeros(4, np.float32)
     rc = lib().pd_selftest_wait(int(limit), int(bool(issue_copy)), _ptr(a), _ptr(out))
     return rc, out
+
+
+def measure_fma_rate(dtype):
+    """Measured vector FMA throughput in TFLOP/s (PD_F32 or PD_F64; an FMA is two flops)."""
+    out = ctypes.c_double(0)
+    check(lib().pd_measure_fma_rate(int(dtype), ctypes.byref(out)))
+    return out.value
