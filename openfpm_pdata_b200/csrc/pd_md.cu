@@ -233,6 +233,45 @@ __global__ void __launch_bounds__(FBLOCK) k_kick_drift(typename V4<T>::type* __r
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
 }
 
+// The end of one step and the start of the next in one pass: v += h f (the
+// closing half kick, kinetic energy partials of that step), then v += h f and
+// x += dt v (the next step's opening half kick and drift), largest |x - xb|^2.
+// The same operations in the same order as k_kick followed by k_kick_drift.
+template <class T>
+__global__ void __launch_bounds__(FBLOCK) k_kick_kick_drift(typename V4<T>::type* __restrict__ pos,
+                                                            const typename V4<T>::type* __restrict__ xb,
+                                                            T* __restrict__ v, const T* __restrict__ f, long cap, long n,
+                                                            T half, T dt, double mass,
+                                                            unsigned long long* __restrict__ maxd2,
+                                                            double* __restrict__ part) {
+    double ke = 0, mx = 0;
+    for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
+        const T fx = f[i], fy = f[cap + i], fz = f[2 * cap + i];
+        T vx = v[i] + half * fx;
+        T vy = v[cap + i] + half * fy;
+        T vz = v[2 * cap + i] + half * fz;
+        ke += 0.5 * mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+        vx = vx + half * fx;
+        vy = vy + half * fy;
+        vz = vz + half * fz;
+        typename V4<T>::type x = ld4(pos, i);
+        x.x += dt * vx;
+        x.y += dt * vy;
+        x.z += dt * vz;
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        st4(pos, i, x);
+        typename V4<T>::type b = ld4(xb, i);
+        T dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
+        mx = fmax(mx, (double)dist2(dx, dy, dz));
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
+    ke = block_sum<double, FBLOCK>(ke);
+    if (threadIdx.x == 0) part[blockIdx.x] = ke;
+}
+
 // v += h f ; kinetic energy partial sums
 template <class T>
 __global__ void __launch_bounds__(FBLOCK) k_kick(T* __restrict__ v, const T* __restrict__ f, long cap, long n, T half,
@@ -842,9 +881,28 @@ int pd_md_destroy(pd_md md) {
     md->eidx.release();
     if (md->gcl) cudaGraphExecDestroy(md->gcl);
     if (md->gst) cudaStreamDestroy(md->gst);
-    for (int i = 0; i < 8; ++i)
-        if (md->ev[i]) cudaEventDestroy(md->ev[i]);
+    for (cudaEvent_t e : md->evp) cudaEventDestroy(e);
     delete md;
+    return PD_OK;
+}
+
+// energies of step s of the plain LJ path (kinetic partials in kpart, pair partials
+// of that step's force launch, the rebuild flag in the control block)
+static int md_energy(pd_md md, int s, cudaStream_t st) {
+    pd_vd h = md->h;
+    if (md->tiles_active) {
+        const int nb2 = 256;
+        long chunk = (md->ntiles + nb2 - 1) / nb2;
+        double* stage = md->tpart.as<double>() + 2 * md->ntiles;
+        pd::launch(k_sum_pairs, nb2, 256, 0, st, (const double*)md->tpart.as<double>(), md->ntiles, chunk, stage);
+        pd::launch(k_energy, 1, 256, 0, st, (const double*)stage, nb2, (const double*)md->kpart.as<double>(),
+                   md->nblk, (const unsigned int*)&h->ctrl->rebuild, md->E.as<double>() + 4 * s);
+    } else {
+        pd::launch(k_energy, 1, 256, 0, st, (const double*)md->fpart.as<double>(), md->nblk,
+                   (const double*)md->kpart.as<double>(), md->nblk, (const unsigned int*)&h->ctrl->rebuild,
+                   md->E.as<double>() + 4 * s);
+    }
+    PD_LAUNCH_CHECK();
     return PD_OK;
 }
 
@@ -867,11 +925,36 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     double half = 0.5 * md->mp.dt / md->mp.mass;
     double lim = 0.5 * md->mp.skin;
     double lim2 = lim * lim;
+    // plain LJ: a step's closing half kick is fused with the next step's kick-drift
+    // (k_kick_kick_drift); the step's energies follow it, the last step's closing
+    // kick runs after the loop
+    const bool fused = md->physics == 0 && !md->mixed;
+    // timing: six events per step, read after the run (no synchronisation in the loop)
+    if (md->timing)
+        while (md->evp.size() < (size_t)6 * steps) {
+            cudaEvent_t e;
+            PD_CUDA(cudaEventCreate(&e));
+            md->evp.push_back(e);
+        }
+    std::vector<unsigned char> rebuilt_at(md->timing ? steps : 0, 0);
+#define PD_EV(k) \
+    if (md->timing) PD_CUDA(cudaEventRecord(md->evp[6 * (size_t)s + (k)], st))
     for (int s = 0; s < steps; ++s) {
         unsigned int rebuilt = 0;
-        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[0], st));
+        PD_EV(0);
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-        if (md->physics == 1)
+        if (fused && s > 0) {
+            if (h->dtype == PD_F64)
+                pd::launch(k_kick_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos,
+                           (const double4*)md->xb.as<double4>(), (double*)V.d, (const double*)F.d, h->cap, n, half,
+                           md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>());
+            else
+                pd::launch(k_kick_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos,
+                           (const float4*)md->xb.as<float4>(), (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
+                           (float)md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>());
+            PD_LAUNCH_CHECK();
+            PD_TRY(md_energy(md, s - 1, st));
+        } else if (md->physics == 1)
             PD_TRY(sph_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
                                   md->mp.dt, st));
         else if (md->mixed)
@@ -886,7 +969,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
                                                              (const float*)F.d, h->cap, n, (float)half,
                                                              (float)md->mp.dt, &h->ctrl->maxdisp2);
         PD_LAUNCH_CHECK();
-        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[1], st));
+        PD_EV(1);
         bool rb = md->mp.skin <= 0 || md->mp.use_cell_list;
         if (!rb) {
             PD_CUDA(cudaMemcpyAsync(&h->ctrl_h->maxdisp2, &h->ctrl->maxdisp2, sizeof(unsigned long long),
@@ -896,7 +979,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             memcpy(&d2, &h->ctrl_h->maxdisp2, sizeof(double));
             rb = d2 > lim2;
         }
-        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[2], st));
+        PD_EV(2);
         if (rb) {
             PD_TRY(md_rebuild(md, st));
             rebuilt = 1;
@@ -905,9 +988,19 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         } else {
             PD_TRY(ghost_replay(h, 0ul, true, nullptr, h->n_img, st));
         }
-        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[3], st));
+        PD_EV(3);
         PD_TRY(md_forces(md, st));
-        if (md->timing) PD_CUDA(cudaEventRecord(md->ev[4], st));
+        PD_EV(4);
+        if (md->timing) rebuilt_at[s] = (unsigned char)rebuilt;
+        if (fused) {
+            // the rebuild flag of this step, read by its energies at the next launch
+            h->ctrl_h->rebuild = rebuilt;
+            PD_CUDA(cudaMemcpyAsync(&h->ctrl->rebuild, &h->ctrl_h->rebuild, sizeof(unsigned int),
+                                    cudaMemcpyHostToDevice, st));
+            md->steps++;
+            PD_EV(5);
+            continue;
+        }
         if (md->physics == 1)
             PD_TRY(sph_kick(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->nblk, md->mp.dt,
                             md->kpart.as<double>(), md->rpart.as<double>(), st));
@@ -941,27 +1034,36 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
                        md->E.as<double>() + 4 * s);
         PD_LAUNCH_CHECK();
         md->steps++;
-        if (md->timing) {
-            PD_CUDA(cudaEventRecord(md->ev[5], st));
-            PD_CUDA(cudaEventSynchronize(md->ev[5]));
-            float a = 0, b = 0, c = 0, d = 0;
-            cudaEventElapsedTime(&a, md->ev[0], md->ev[1]);
-            cudaEventElapsedTime(&b, md->ev[2], md->ev[3]);
-            cudaEventElapsedTime(&c, md->ev[3], md->ev[4]);
-            cudaEventElapsedTime(&d, md->ev[4], md->ev[5]);
-            md->ms[0] += a + d;
-            md->cnt[0] += 1;
-            md->ms[rebuilt ? 1 : 2] += b;
-            md->cnt[rebuilt ? 1 : 2] += 1;
-            md->ms[3] += c;
-            md->cnt[3] += 1;
-        }
+        PD_EV(5);
+    }
+#undef PD_EV
+    if (fused && steps > 0) {
+        // the last step's closing half kick and energies
+        if (h->dtype == PD_F64)
+            pd::launch(k_kick<double>, md->nblk, FBLOCK, 0, st, (double*)V.d, (const double*)F.d, h->cap, n, half,
+                       md->mp.mass, md->kpart.as<double>());
+        else
+            pd::launch(k_kick<float>, md->nblk, FBLOCK, 0, st, (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
+                       md->mp.mass, md->kpart.as<double>());
+        PD_LAUNCH_CHECK();
+        PD_TRY(md_energy(md, steps - 1, st));
     }
     if (md->mixed) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));  // the vector's positions are current
     if (E && steps > 0) {
         PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));
     }
     PD_CUDA(cudaStreamSynchronize(st));
+    if (md->timing)
+        for (int s = 0; s < steps; ++s) {
+            float t[5];
+            for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], md->evp[6 * (size_t)s + k], md->evp[6 * (size_t)s + k + 1]);
+            md->ms[0] += t[0] + t[4];  // (fused) kick-drift and the previous step's energies; closing kick
+            md->cnt[0] += 1;
+            md->ms[rebuilt_at[s] ? 1 : 2] += t[2];
+            md->cnt[rebuilt_at[s] ? 1 : 2] += 1;
+            md->ms[3] += t[3];
+            md->cnt[3] += 1;
+        }
     PD_TRY(read_ctrl(h, st));
     if (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW)) {
         set_error("pd_md_run: device capacity overflow (err=0x%x)", h->ctrl_h->err);
@@ -972,8 +1074,6 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
 
 int pd_md_set_timing(pd_md md, int on) {
     if (!md) return PD_EINVAL;
-    if (on && !md->ev[0])
-        for (int i = 0; i < 8; ++i) PD_CUDA(cudaEventCreate(&md->ev[i]));
     md->timing = on != 0;
     for (int i = 0; i < 4; ++i) {
         md->ms[i] = 0;

@@ -1,6 +1,7 @@
 // pd_md.cuh -- the integrator handle, shared by the single-system driver
 // (pd_md.cu) and the serving loop (pd_serve.cu).
 #pragma once
+#include <vector>
 #include "pd_internal.cuh"
 #include "pd_tile.cuh"
 
@@ -41,7 +42,7 @@ struct pd_md_s {
     pd::Buf eidx;
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
-    cudaEvent_t ev[8] = {};
+    std::vector<cudaEvent_t> evp;  // six per step of a timed run, recorded without synchronising
     double ms[4] = {0, 0, 0, 0};   // integrate, rebuild, images, force
     long cnt[4] = {0, 0, 0, 0};
 };
