@@ -928,7 +928,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     // plain LJ: a step's closing half kick is fused with the next step's kick-drift
     // (k_kick_kick_drift); the step's energies follow it, the last step's closing
     // kick runs after the loop
-    const bool fused = md->physics == 0 && !md->mixed;
+    const bool fused = md->physics == 0;
     // timing: six events per step, read after the run (no synchronisation in the loop)
     if (md->timing)
         while (md->evp.size() < (size_t)6 * steps) {
@@ -943,7 +943,11 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         unsigned int rebuilt = 0;
         PD_EV(0);
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-        if (fused && s > 0) {
+        if (fused && s > 0 && md->mixed) {
+            PD_TRY(mixed_kick_kick_drift(h, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+                                         md->mp.dt, md->mp.mass, md->kpart.as<double>(), st));
+            PD_TRY(md_energy(md, s - 1, st));
+        } else if (fused && s > 0) {
             if (h->dtype == PD_F64)
                 pd::launch(k_kick_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos,
                            (const double4*)md->xb.as<double4>(), (double*)V.d, (const double*)F.d, h->cap, n, half,
@@ -1037,7 +1041,11 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         PD_EV(5);
     }
 #undef PD_EV
-    if (fused && steps > 0) {
+    if (fused && steps > 0 && md->mixed) {
+        PD_TRY(mixed_kick(h, md->mp.vel_prop, md->mp.force_prop, md->nblk, half, md->mp.mass, md->kpart.as<double>(),
+                          st));
+        PD_TRY(md_energy(md, steps - 1, st));
+    } else if (fused && steps > 0) {
         // the last step's closing half kick and energies
         if (h->dtype == PD_F64)
             pd::launch(k_kick<double>, md->nblk, FBLOCK, 0, st, (double*)V.d, (const double*)F.d, h->cap, n, half,

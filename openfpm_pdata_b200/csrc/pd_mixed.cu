@@ -101,6 +101,41 @@ __global__ void __launch_bounds__(256) k_kick_drift32(float4* __restrict__ off, 
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
 }
 
+// k_kick32 of one step and k_kick_drift32 of the next in one pass (the same
+// operations in the same order; kinetic energy partials of the closing kick)
+__global__ void __launch_bounds__(256) k_kick_kick_drift32(float4* __restrict__ off, const float4* __restrict__ ob,
+                                                           float* __restrict__ v, const float* __restrict__ f,
+                                                           long cap, long n, float half, float dt, double mass,
+                                                           unsigned long long* __restrict__ maxd2,
+                                                           double* __restrict__ part) {
+    double mx = 0, ke = 0;
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
+        const float fx = f[i], fy = f[cap + i], fz = f[2 * cap + i];
+        float vx = v[i] + half * fx;
+        float vy = v[cap + i] + half * fy;
+        float vz = v[2 * cap + i] + half * fz;
+        ke += 0.5 * mass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+        vx = vx + half * fx;
+        vy = vy + half * fy;
+        vz = vz + half * fz;
+        float4 o = off[i];
+        o.x += dt * vx;
+        o.y += dt * vy;
+        o.z += dt * vz;
+        v[i] = vx;
+        v[cap + i] = vy;
+        v[2 * cap + i] = vz;
+        off[i] = o;
+        float4 b = ob[i];
+        float dx = o.x - b.x, dy = o.y - b.y, dz = o.z - b.z;
+        mx = fmax(mx, (double)dist2(dx, dy, dz));
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
+    ke = block_sum<double, 256>(ke);
+    if (threadIdx.x == 0) part[blockIdx.x] = ke;
+}
+
 __global__ void __launch_bounds__(256) k_kick32(float* __restrict__ v, const float* __restrict__ f, long cap, long n,
                                                 float half, double mass, double* __restrict__ part) {
     double ke = 0;
@@ -202,6 +237,16 @@ int mixed_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_p
     Prop& F = h->props[force_prop];
     pd::launch(k_kick_drift32, nblk, 256, 0, st, off.as<float4>(), (const float4*)ob.as<float4>(), (float*)V.d,
                (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, &h->ctrl->maxdisp2);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_kick_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
+                          double dt, double mass, double* kpart, cudaStream_t st) {
+    Prop& V = h->props[vel_prop];
+    Prop& F = h->props[force_prop];
+    pd::launch(k_kick_kick_drift32, nblk, 256, 0, st, off.as<float4>(), (const float4*)ob.as<float4>(), (float*)V.d,
+               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, mass, &h->ctrl->maxdisp2, kpart);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }

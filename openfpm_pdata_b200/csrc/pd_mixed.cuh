@@ -10,6 +10,9 @@ int mixed_to_positions(pd_vd h, pd_cl cl, const Buf& off, cudaStream_t st);
 int mixed_replay(pd_vd h, Buf& off, const Buf& K, cudaStream_t st);
 int mixed_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
                      double dt, cudaStream_t st);
+// mixed_kick of one step and mixed_kick_drift of the next in one pass
+int mixed_kick_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
+                          double dt, double mass, double* kpart, cudaStream_t st);
 int mixed_kick(pd_vd h, int vel_prop, int force_prop, int nblk, double half, double mass, double* kpart,
                cudaStream_t st);
 int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
