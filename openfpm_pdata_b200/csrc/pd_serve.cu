@@ -1589,11 +1589,12 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
         if (want > 0 && cudaMallocFromPoolAsync(&p, want, s->pool, s->as) == cudaSuccess) {
             cudaFreeAsync(p, s->as);
             cudaStreamSynchronize(s->as);
-            // admission counts against what the pool holds: no free-memory query per
-            // step (cudaMemGetInfo took 10-100 ms at times on a shared node)
-            s->budget = (long)std::min((size_t)s->budget, want);
         }
         cudaGetLastError();
+        // admission counts against the budget capped by the free memory at creation
+        // (held by the pool when the reservation above succeeded): no free-memory query
+        // per step (cudaMemGetInfo took 10-100 ms at times on a shared node)
+        s->budget = (long)std::min((size_t)s->budget, want);
     }
     for (int lk = 0; lk < 4 && r == PD_OK; ++lk) r = capture_graph(s, lk);
     if (r != PD_OK) {
