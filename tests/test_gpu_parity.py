@@ -375,3 +375,26 @@ def test_md_cell_list_both_paths(pd, orc):
         d = vd.deviceToHostPos(with_ghost=False) - xo[gid]
         d -= L * np.round(d / L)
         assert np.max(np.abs(d)) < 1e-8, (side, np.max(np.abs(d)))
+
+
+@pytest.mark.parametrize("cell_list", [False, True])
+def test_md_fp32_storage_follows_oracle(pd, orc, cell_list):
+    """A vector with FP32 positions and FP32 properties through the tiled Verlet path
+    and the cell-list path: 20 steps stay within FP32 accuracy of the FP64 oracle
+    (per-step total energy within 1e-4 relative, positions within 1e-4)."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(10, 1.1, 0.05, seed=13)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    skin = 0.0 if cell_list else 0.3
+    vd = make_vd(pd, x.astype(F32), lo, hi, bc, 2.5 + skin, F32, props=[(pd.PD_F32, 3), (pd.PD_F32, 3)])
+    vd.hostToDeviceProp(0, v.astype(F32))
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=skin, use_cell_list=cell_list)
+    E = md.run(20)
+    xo, vo, Eo = orc.md_lj(x.astype(F32).astype(np.float64), v.astype(F32).astype(np.float64), lo, hi, bc,
+                           2.5 + skin, 2.5, skin, 1.0, 1.0, 0.005, 1.0, 20)
+    tot, toto = E[:, 0] + E[:, 1], Eo[1:, 0] + Eo[1:, 1]
+    assert np.max(np.abs(tot - toto) / np.abs(toto)) < 1e-4
+    gid = vd.gid(with_ghost=False)
+    d = vd.deviceToHostPos(with_ghost=False).astype(np.float64) - xo[gid]
+    d -= L * np.round(d / L)
+    assert np.max(np.abs(d)) < 1e-4
