@@ -640,6 +640,23 @@ static int md_step_cl_any(pd_md md, cudaStream_t st, long img_cap) {
     return md->h->dtype == PD_F64 ? md_step_cl<double>(md, st, img_cap) : md_step_cl<float>(md, st, img_cap);
 }
 
+// every buffer address and size a captured cell-list step uses: the graph holds
+// them as raw values, so it is captured again when any of them changed
+static std::vector<uintptr_t> cl_graph_key(pd_md md) {
+    pd_vd h = md->h;
+    pd_cl cl = md->cl;
+    std::vector<uintptr_t> k = {(uintptr_t)h->pos, (uintptr_t)h->gid, (uintptr_t)h->cap, (uintptr_t)h->n_real,
+                                (uintptr_t)md->E.p, (uintptr_t)md->eidx.p, (uintptr_t)md->kpart.p,
+                                (uintptr_t)md->fpart.p, (uintptr_t)md->xb.p, (uintptr_t)cl->cell_start.p,
+                                (uintptr_t)cl->cell_cnt.p, (uintptr_t)cl->sorted.p, (uintptr_t)cl->sorted_tmp.p,
+                                (uintptr_t)cl->cell_of.p, (uintptr_t)cl->slot.p, (uintptr_t)h->tmp.p,
+                                (uintptr_t)h->tmp2.p, (uintptr_t)h->img_src.p, (uintptr_t)h->img_shift.p,
+                                (uintptr_t)h->img_cnt.p, (uintptr_t)h->img_start.p, (uintptr_t)h->boxes.p,
+                                (uintptr_t)h->shifts.p, (uintptr_t)h->scan_scratch.p, (uintptr_t)md->gcl_img_cap};
+    for (auto& P : h->props) k.push_back((uintptr_t)P.d);
+    return k;
+}
+
 // cell-list mode: the first step of a run sizes every buffer, the step is
 // captured once as a CUDA graph (on a private stream: the legacy stream cannot
 // capture) and the remaining steps are graph launches on the caller's stream
@@ -655,6 +672,12 @@ static int md_run_cl_graph(pd_md md, int steps, cudaStream_t st, double* E) {
     PD_TRY(md->eidx.ensure(sizeof(int)));
     PD_CUDA(cudaMemsetAsync(md->eidx.p, 0, sizeof(int), st));
     int s0 = 0;
+    if (md->gcl && cl_graph_key(md) != md->gcl_key) {
+        // something the graph captured was reallocated or resized since: capture again
+        PD_CUDA(cudaStreamSynchronize(st));
+        cudaGraphExecDestroy(md->gcl);
+        md->gcl = nullptr;
+    }
     if (!md->gcl) {
         PD_TRY(read_ctrl(h, st));
         const long m = h->ctrl_h->n_img;
@@ -685,6 +708,7 @@ static int md_run_cl_graph(pd_md md, int steps, cudaStream_t st, double* E) {
             set_error("cell-list step graph: %s", cudaGetErrorString(ce));
             return PD_ECUDA;
         }
+        md->gcl_key = cl_graph_key(md);
     }
     for (int s = s0; s < steps; ++s) PD_CUDA(cudaGraphLaunch(md->gcl, st));
     __atomic_fetch_add(&g_launches, (unsigned long long)(steps - s0) * md->gcl_kernels, __ATOMIC_RELAXED);

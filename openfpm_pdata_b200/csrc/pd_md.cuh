@@ -1,6 +1,7 @@
 // pd_md.cuh -- the integrator handle, shared by the single-system driver
 // (pd_md.cu) and the serving loop (pd_serve.cu).
 #pragma once
+#include <cstdint>
 #include <vector>
 #include "pd_internal.cuh"
 #include "pd_tile.cuh"
@@ -38,6 +39,7 @@ struct pd_md_s {
     cudaGraphExec_t gcl = nullptr;
     cudaStream_t gst = nullptr;
     long gcl_img_cap = 0;
+    std::vector<uintptr_t> gcl_key;  // the buffers and sizes the graph captured
     unsigned long long gcl_kernels = 0;
     pd::Buf eidx;
     // optional per-phase device timing (CUDA events on the run's stream)

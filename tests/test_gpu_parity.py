@@ -398,3 +398,28 @@ def test_md_fp32_storage_follows_oracle(pd, orc, cell_list):
     d = vd.deviceToHostPos(with_ghost=False).astype(np.float64) - xo[gid]
     d -= L * np.round(d / L)
     assert np.max(np.abs(d)) < 1e-4
+
+
+def test_md_cell_list_graph_recaptured_after_growth(pd):
+    """The cell-list step graph holds raw buffer addresses: a second, longer run
+    (its energy buffer grows) makes the driver capture it again.  Runs of 3 + 10
+    steps equal one run of 13 bit for bit."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(42, 1.1, 0.05, seed=17)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    out = []
+    for split in (True, False):
+        vd = make_vd(pd, x, lo, hi, bc, 2.5, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+        vd.hostToDeviceProp(0, v)
+        md = pd.MD(vd, 0, 1, dt=0.005, skin=0.0, use_cell_list=True)
+        if split:
+            E = np.concatenate([md.run(3), md.run(10)])
+        else:
+            E = md.run(13)
+        out.append(E)
+        gid = vd.gid(with_ghost=False)
+        xs = np.zeros_like(x)
+        xs[gid] = vd.deviceToHostPos(with_ghost=False)
+        out.append(xs)
+    assert np.array_equal(out[0], out[2])
+    assert np.array_equal(out[1], out[3])
