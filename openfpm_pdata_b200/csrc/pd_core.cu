@@ -540,6 +540,10 @@ int pd_d2h_gid(pd_vd h, long* host, long offset, long count, void* stream) {
 int pd_map(pd_vd h, int opt, void* stream) {
     (void)opt;
     if (!h) return PD_EINVAL;
+    if (h->ghost_pending) {
+        set_error("map: an Ighost_get is waiting for its ghost_wait");
+        return PD_ESTATE;
+    }
     // drop the ghost (vector_dist_comm.hpp:1969-1970), wrap (apply_bc_each_part)
     h->n_total = h->n_real;
     h->img_valid = false;

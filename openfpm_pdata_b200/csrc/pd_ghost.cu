@@ -334,6 +334,10 @@ extern "C" {
 
 int pd_ghost_get(pd_vd h, unsigned long prop_mask, int opt, void* stream) {
     if (!h) return PD_EINVAL;
+    if (h->ghost_pending) {
+        set_error("ghost_get: an Ighost_get is waiting for its ghost_wait");
+        return PD_ESTATE;
+    }
     cudaStream_t st = S(stream);
     if ((opt & PD_SKIP_LABELLING) && h->img_valid) {
         // ghost_get_ with SKIP_LABELLING: positions unless NO_POSITION, properties in the mask

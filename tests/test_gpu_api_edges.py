@@ -162,8 +162,13 @@ def test_ighost_get_equals_ghost_get(pd):
     b.Ighost_get([0], opt=pd.RUN_ON_DEVICE | pd.SKIP_LABELLING)
     b.ghost_wait()
     assert np.array_equal(b.deviceToHostProp(0), a.deviceToHostProp(0))
-    # a second Ighost_get before the wait is refused
+    # a second Ighost_get, a ghost_get or a map before the wait are refused
     b.Ighost_get()
     with pytest.raises(RuntimeError):
         b.Ighost_get()
+    with pytest.raises(RuntimeError):
+        b.ghost_get()
+    with pytest.raises(RuntimeError):
+        b.map()
     b.ghost_wait()
+    b.map()
