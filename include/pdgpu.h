@@ -158,6 +158,13 @@ typedef struct {
 const char* pd_last_error(void);
 /* number of CUDA kernels this library has launched so far (all handles) */
 unsigned long long pd_launch_count(void);
+/* Device blocks freed by the library (outside the serving loop) are cached for
+ * reuse up to a limit (4 GiB by default): pd_empty_cache returns them to the
+ * driver; pd_set_cache_limit sets the limit (bytes < 0: unchanged) and reports
+ * the bytes held.  No counterpart in the reference package (its device memory
+ * comes from a dependency's allocator). */
+int pd_empty_cache(void);
+int pd_set_cache_limit(long bytes, long* held);
 int pd_device_info(int* sm_count, long* free_bytes, long* total_bytes);
 
 /* ---- vector_dist -------------------------------------------------------- */

@@ -10,7 +10,9 @@
 // images [n_real, n_total).
 #include <algorithm>
 #include <cstdarg>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
@@ -33,17 +35,107 @@ thread_local AllocCtx* g_alloc_ctx = nullptr;
 
 // Device allocations of the library.  Inside an AllocScope (the serving loop) they
 // come from the scope's memory pool, ordered on the scope's stream (freed memory
-// is reused without a device-wide synchronisation); elsewhere plain cudaMalloc /
-// cudaFree, which synchronise.
+// is reused without a device-wide synchronisation).  Elsewhere from cudaMalloc
+// through a bounded block cache: a freed block is kept (up to the cache limit,
+// 4 GiB by default) and handed out again for a request of 1/2 to 1 times its size.
+// cudaFree synchronises the device; the cache keeps that guarantee by
+// synchronising once before a block freed since the last synchronisation is
+// reused, so no kernel of the block's previous owner can still be running.
+// Creating and destroying vectors one after another then costs no
+// cudaMalloc / cudaFree (each of which took milliseconds for large blocks).
+// A cudaMalloc that fails empties the cache and is tried once more.
+thread_local bool g_capturing = false;  // set around the library's own stream captures
+
+namespace {
+struct BlockCache {
+    struct Block {
+        size_t bytes;
+        int dev;
+    };
+    std::mutex mu;
+    std::multimap<std::pair<int, size_t>, void*> free_blocks;  // by (device, size)
+    std::unordered_map<void*, Block> block_of;                 // every block from cudaMalloc on this path
+    size_t held = 0;
+    size_t limit = (size_t)4 << 30;
+    std::unordered_map<int, bool> dirty;  // per device: blocks freed since its last synchronisation
+
+    // return every cached block to the driver (caller holds mu)
+    void drain() {
+        if (free_blocks.empty()) return;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        int dev = -1;
+        for (auto& kv : free_blocks) {
+            if (kv.first.first != dev) {
+                dev = kv.first.first;
+                cudaSetDevice(dev);
+                cudaDeviceSynchronize();
+            }
+            block_of.erase(kv.second);
+            cudaFree(kv.second);
+        }
+        cudaSetDevice(cur);
+        free_blocks.clear();
+        held = 0;
+        dirty.clear();
+    }
+};
+BlockCache& block_cache() {
+    static BlockCache* c = new BlockCache();  // never destroyed: no CUDA calls at process exit
+    return *c;
+}
+size_t block_round(size_t b) {
+    return b <= ((size_t)1 << 20) ? ((b + 511) & ~(size_t)511) : ((b + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1));
+}
+}  // namespace
+
 cudaError_t dev_alloc(void** p, size_t b) {
     if (g_alloc_ctx) return cudaMallocFromPoolAsync(p, b, g_alloc_ctx->pool, g_alloc_ctx->st);
-    return cudaMalloc(p, b);
+    if (g_capturing) return cudaMalloc(p, b);
+    const size_t rb = block_round(b);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    BlockCache& C = block_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    auto it = C.free_blocks.lower_bound({dev, rb});
+    if (it != C.free_blocks.end() && it->first.first == dev && it->first.second <= 2 * rb) {
+        if (C.dirty[dev]) {
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return e;
+            C.dirty[dev] = false;
+        }
+        *p = it->second;
+        C.held -= it->first.second;
+        C.free_blocks.erase(it);
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(p, rb);
+    if (e == cudaErrorMemoryAllocation && !C.free_blocks.empty()) {
+        cudaGetLastError();
+        C.drain();
+        e = cudaMalloc(p, rb);
+    }
+    if (e == cudaSuccess) C.block_of[*p] = {rb, dev};
+    return e;
 }
 
 void dev_free(void* p) {
     if (!p) return;
-    if (g_alloc_ctx) cudaFreeAsync(p, g_alloc_ctx->st);
-    else cudaFree(p);
+    if (g_alloc_ctx) {
+        cudaFreeAsync(p, g_alloc_ctx->st);
+        return;
+    }
+    BlockCache& C = block_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    auto it = C.block_of.find(p);
+    if (it == C.block_of.end() || g_capturing || C.held + it->second.bytes > C.limit) {
+        if (it != C.block_of.end()) C.block_of.erase(it);
+        cudaFree(p);
+        return;
+    }
+    C.free_blocks.insert({{it->second.dev, it->second.bytes}, p});
+    C.held += it->second.bytes;
+    C.dirty[it->second.dev] = true;
 }
 
 int Buf::ensure(size_t b) {
@@ -335,6 +427,24 @@ extern "C" {
 const char* pd_last_error(void) { return g_err.c_str(); }
 
 unsigned long long pd_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int pd_empty_cache(void) {
+    BlockCache& C = block_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    C.drain();
+    return PD_OK;
+}
+
+int pd_set_cache_limit(long bytes, long* held) {
+    BlockCache& C = block_cache();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (bytes >= 0) {
+        C.limit = (size_t)bytes;
+        if (C.held > C.limit) C.drain();
+    }
+    if (held) *held = (long)C.held;
+    return PD_OK;
+}
 
 int pd_device_info(int* sm_count, long* free_bytes, long* total_bytes) {
     int dev = 0;

@@ -65,6 +65,7 @@ struct AllocCtx {
     cudaMemPool_t pool;
 };
 extern thread_local AllocCtx* g_alloc_ctx;
+extern thread_local bool g_capturing;  // the library is capturing a stream on this thread
 struct AllocScope {
     AllocCtx ctx;
     AllocCtx* prev;

@@ -692,7 +692,9 @@ static int md_run_cl_graph(pd_md md, int steps, cudaStream_t st, double* E) {
         cudaGraph_t g = nullptr;
         const unsigned long long l0 = pd_launch_count();
         PD_CUDA(cudaStreamBeginCapture(md->gst, cudaStreamCaptureModeThreadLocal));
+        g_capturing = true;
         int rc = md_step_cl_any(md, md->gst, md->gcl_img_cap);
+        g_capturing = false;
         cudaError_t ce = cudaStreamEndCapture(md->gst, &g);
         md->gcl_kernels = pd_launch_count() - l0;
         __atomic_fetch_sub(&g_launches, md->gcl_kernels, __ATOMIC_RELAXED);  // captured, not launched

@@ -49,6 +49,22 @@ __global__ void k_off_to_x64(const float4* __restrict__ off, long n, CellGeom C,
     }
 }
 
+// offsets -> positions written in id order as x,y,z triples (a finished
+// system's result, ready for one contiguous copy to the host)
+__global__ void k_off_to_x64_by_id(const float4* __restrict__ off, long n, CellGeom C, const int* __restrict__ gid,
+                                   double* __restrict__ out) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        float4 o = off[k];
+        double cx, cy, cz;
+        C.centre(__float_as_uint(o.w), cx, cy, cz);
+        const long g = gid[k];
+        if (g < 0 || g >= n) continue;
+        out[3 * g] = cx + (double)o.x;
+        out[3 * g + 1] = cy + (double)o.y;
+        out[3 * g + 2] = cz + (double)o.z;
+    }
+}
+
 // image offset = source offset + K, K formed in FP64 at the rebuild
 __global__ void k_image_k(const double4* __restrict__ pos, const float4* __restrict__ off, long n_real, long m,
                           const int* __restrict__ src, CellGeom C, float4* __restrict__ K) {
@@ -218,6 +234,15 @@ int mixed_to_positions(pd_vd h, pd_cl cl, const Buf& off, cudaStream_t st) {
     if (n > 0)
         pd::launch(k_off_to_x64, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n, cell_geom(cl),
                    (double4*)h->pos);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int mixed_to_positions_by_id(pd_vd h, pd_cl cl, const Buf& off, double* out, cudaStream_t st) {
+    long n = h->n_real;
+    if (n > 0)
+        pd::launch(k_off_to_x64_by_id, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n,
+                   cell_geom(cl), (const int*)h->gid, out);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }

@@ -7,6 +7,8 @@ namespace pd {
 
 int mixed_from_positions(pd_vd h, pd_cl cl, Buf& off, Buf& K, cudaStream_t st);
 int mixed_to_positions(pd_vd h, pd_cl cl, const Buf& off, cudaStream_t st);
+// positions of the real particles in id order, x,y,z per particle, into `out` (3 n doubles)
+int mixed_to_positions_by_id(pd_vd h, pd_cl cl, const Buf& off, double* out, cudaStream_t st);
 int mixed_replay(pd_vd h, Buf& off, const Buf& K, cudaStream_t st);
 int mixed_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
                      double dt, cudaStream_t st);

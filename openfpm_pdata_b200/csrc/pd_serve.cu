@@ -871,13 +871,88 @@ struct SrvSlot {
     }
 };
 
+// A ring of pinned host memory (mapped for the device) whose regions are taken
+// in order and freed at the front: a region freed out of order is kept until all
+// older ones are freed.  take() returns nullptr when the ring has no room; the
+// caller then falls back to host vectors.
+struct PinnedFifo {
+    struct Region {
+        long ticket;
+        size_t lo, hi;
+        cudaEvent_t ev;  // work that reads the region (none: free once marked)
+        bool done;
+    };
+    char* base = nullptr;
+    const char* dev = nullptr;
+    size_t bytes = 0;
+    std::deque<Region> q;
+
+    int create(size_t b) {
+        bytes = b;
+        void* d = nullptr;
+        if (cudaMallocHost((void**)&base, b) != cudaSuccess || cudaHostGetDevicePointer(&d, base, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return PD_ENOMEM;
+        }
+        dev = static_cast<const char*>(d);
+        return PD_OK;
+    }
+    void destroy() {
+        for (auto& g : q)
+            if (g.ev) cudaEventDestroy(g.ev);
+        q.clear();
+        if (base) cudaFreeHost(base);
+        base = nullptr;
+    }
+    // free the regions at the front that are marked and whose work has finished
+    void trim(std::vector<cudaEvent_t>& ev_free) {
+        while (!q.empty()) {
+            Region& f = q.front();
+            if (!f.done) break;
+            if (f.ev && cudaEventQuery(f.ev) != cudaSuccess) {
+                cudaGetLastError();  // cudaErrorNotReady
+                break;
+            }
+            if (f.ev) ev_free.push_back(f.ev);
+            q.pop_front();
+        }
+    }
+    // a region of `need` bytes after the newest one (wrapping to the start), or
+    // nullptr when it would reach the oldest region still held
+    char* take(long ticket, size_t need, long& lo_out, std::vector<cudaEvent_t>& ev_free) {
+        need = (need + 255) & ~(size_t)255;
+        trim(ev_free);
+        size_t lo = 0;
+        if (!q.empty()) {
+            const size_t T = q.front().lo, H = q.back().hi;
+            const bool wrapped = q.back().lo < T;
+            if (!wrapped && H + need <= bytes) lo = H;
+            else if (!wrapped && need <= T) lo = 0;
+            else if (wrapped && H + need <= T) lo = H;
+            else return nullptr;
+        } else if (need > bytes) {
+            return nullptr;
+        }
+        q.push_back({ticket, lo, lo + need, nullptr, false});
+        lo_out = (long)lo;
+        return base + lo;
+    }
+    Region* find(long ticket) {
+        for (auto& g : q)
+            if (g.ticket == ticket) return &g;
+        return nullptr;
+    }
+};
+
 struct SrvReq {
     long ticket = 0;
     long n = 0;
     double L = 0;
     int steps = 0;
     int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
-    std::vector<double> x, v, xo, E;
+    std::vector<double> x, v, xo, E;  // x, v: the submitted state when it is not in the inbox
+    long in_lo = -1;                   // offset of the submitted state in the pinned inbox, or -1
+    long out_lo = -1;                  // offset of the result in the pinned outbox, or -1 (xo, E)
     double t_submit = 0, t_admit = 0, t_done = 0;
     size_t bytes = 0;
     int slot = -1;
@@ -912,7 +987,8 @@ struct pd_srv_s {
     cudaMemPool_t pool = nullptr;  // device memory of the slots (stream-ordered on `as`)
     cudaEvent_t ev_adm = nullptr;  // end of the last admissions on `as`
     // pinned staging: a ring for the admissions' uploads (a region is reused once
-    // the event recorded after its copies has completed) and a buffer for downloads
+    // the event recorded after its copies has completed) and a buffer for downloads,
+    // both 1/64 of the budget within [8 MB, 256 MB]
     char* up = nullptr;
     size_t up_bytes = 0, up_head = 0;
     struct UpUse {
@@ -923,6 +999,13 @@ struct pd_srv_s {
     std::vector<cudaEvent_t> ev_free;
     char* down = nullptr;
     size_t down_bytes = 0;
+    // pinned inbox: a submitted state is copied here once when there is room and
+    // read by the admission's upload kernel; regions are taken in submission order
+    // and freed in admission order, the same FIFO order
+    PinnedFifo inbox;
+    // pinned outbox: a finished system's positions and energies are copied here by
+    // the GPU and read by pd_srv_result; regions are freed at pd_srv_release
+    PinnedFifo outbox;
     bool adm_pending = false;
     cudaGraphExec_t gstep[4] = {nullptr, nullptr, nullptr, nullptr};  // 1, 2, 4, 8 steps per launch
     bool dirty = true;
@@ -1269,6 +1352,30 @@ static int slot_scratch(pd_srv s, SrvSlot& sl, SrvReq* r) {
     return PD_OK;
 }
 
+// the admission of `r` has launched everything that reads its inbox region: the
+// region is freed once the work queued so far on the admission stream is done
+static void inbox_release(pd_srv s, SrvReq* r) {
+    if (r->in_lo < 0) return;
+    if (PinnedFifo::Region* g = s->inbox.find(r->ticket)) {
+        cudaEvent_t ev = nullptr;
+        if (!s->ev_free.empty()) {
+            ev = s->ev_free.back();
+            s->ev_free.pop_back();
+        } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            ev = nullptr;
+        }
+        if (ev && cudaEventRecord(ev, s->as) != cudaSuccess) {
+            s->ev_free.push_back(ev);
+            ev = nullptr;
+        }
+        if (!ev) cudaStreamSynchronize(s->as);  // no event: wait here instead
+        cudaGetLastError();
+        g->ev = ev;
+        g->done = true;
+    }
+    r->in_lo = -1;
+}
+
 // a region of `need` bytes of the upload ring, after the copies that last used it
 static char* ring_take(pd_srv s, size_t need, size_t& lo_out) {
     need = (need + 255) & ~(size_t)255;
@@ -1305,44 +1412,92 @@ static int ring_mark(pd_srv s, size_t lo, size_t need) {
     return PD_OK;
 }
 
-// staging layout: ghost boxes, shift vectors, position records, velocities
+// staging layout: ghost boxes, shift vectors, positions and velocities as submitted
 static size_t stage_off_shifts() { return (sizeof(BoxSet<double>) + 63) & ~(size_t)63; }
 static size_t stage_off_pos() { return (stage_off_shifts() + 81 * sizeof(double) + 63) & ~(size_t)63; }
 
+// the submitted state read from pinned host memory (x, v: n x,y,z triples) into
+// the slot: FP64 position records and FP32 velocity components (stride cap);
+// each block stages its 256 triples through shared memory so the host reads
+// are contiguous
+__global__ void __launch_bounds__(256) k_srv_unpack(const double* __restrict__ x, const double* __restrict__ v, long n,
+                                                    double4* __restrict__ pos, float* __restrict__ V, long cap) {
+    __shared__ double sx[3 * 256], sv[3 * 256];
+    for (long base = (long)blockIdx.x * 256; base < n; base += (long)gridDim.x * 256) {
+        const int m = (int)min(256L, n - base);
+        for (int j = threadIdx.x; j < 3 * m; j += 256) {
+            sx[j] = x[3 * base + j];
+            sv[j] = v[3 * base + j];
+        }
+        __syncthreads();
+        const int t = threadIdx.x;
+        if (t < m) {
+            pos[base + t] = make_double4(sx[3 * t], sx[3 * t + 1], sx[3 * t + 2], 0.0);
+            V[base + t] = (float)sv[3 * t];
+            V[cap + base + t] = (float)sv[3 * t + 1];
+            V[2 * cap + base + t] = (float)sv[3 * t + 2];
+        }
+        __syncthreads();
+    }
+}
+
 // upload the submitted state and the ghost boxes of the box, stream-ordered on the
-// admission stream from the pinned upload ring (the host does not wait)
+// admission stream from the pinned upload ring (the host does not wait): the host
+// copies the submitted arrays as they are, a kernel forms the slot's layout
 static int load_state(pd_srv s, SrvSlot& sl, SrvReq* r) {
     pd_vd h = sl.h;
     const long n = r->n;
-    const size_t opos = stage_off_pos(), ov = opos + sizeof(double4) * n;
-    const size_t need = ov + sizeof(float) * 3 * n;
+    const bool inbox = r->in_lo >= 0;  // the state is in the inbox: only the boxes go through the ring
+    const size_t ox = stage_off_pos(), ov = ox + ((sizeof(double) * 3 * n + 63) & ~(size_t)63);
+    const size_t need = inbox ? ox : ov + sizeof(double) * 3 * n;
     size_t lo = 0;
     char* st = ring_take(s, need, lo);
-    std::vector<char> tmp;
-    if (!st) {  // larger than the ring: pageable staging, waited for below
-        tmp.resize(need);
-        st = tmp.data();
+    char* tmp = nullptr;
+    if (!st) {  // larger than the ring: pinned staging of its own, waited for below
+        if (cudaMallocHost((void**)&tmp, need) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("serving: pinned staging of %zu bytes failed", need);
+            return PD_ENOMEM;
+        }
+        st = tmp;
     }
     BoxSet<double>* B = reinterpret_cast<BoxSet<double>*>(st);
     double* sh = reinterpret_cast<double*>(st + stage_off_shifts());
-    PD_TRY(ghost_boxes_host(h, B, sh));
-    PD_TRY(h->boxes.ensure(sizeof(BoxSet<double>)));
-    PD_TRY(h->shifts.ensure(sizeof(double) * 81));
-    PD_CUDA(cudaMemcpyAsync(h->boxes.p, B, sizeof(BoxSet<double>), cudaMemcpyHostToDevice, s->as));
-    PD_CUDA(cudaMemcpyAsync(h->shifts.p, sh, sizeof(double) * 81, cudaMemcpyHostToDevice, s->as));
-    h->nbox = B->nb;
-    double4* P = reinterpret_cast<double4*>(st + opos);
-    for (long i = 0; i < n; ++i) P[i] = make_double4(r->x[3 * i], r->x[3 * i + 1], r->x[3 * i + 2], 0.0);
-    PD_CUDA(cudaMemcpyAsync(h->pos, P, sizeof(double4) * n, cudaMemcpyHostToDevice, s->as));
-    float* V = reinterpret_cast<float*>(st + ov);
-    for (int d = 0; d < 3; ++d) {
-        for (long i = 0; i < n; ++i) V[(size_t)d * n + i] = (float)r->v[3 * i + d];
-        PD_CUDA(cudaMemcpyAsync(h->props[sl.vp].d + (size_t)d * h->cap * sizeof(float), V + (size_t)d * n,
-                                sizeof(float) * n, cudaMemcpyHostToDevice, s->as));
+    int rc = ghost_boxes_host(h, B, sh);
+    if (rc == PD_OK) rc = h->boxes.ensure(sizeof(BoxSet<double>));
+    if (rc == PD_OK) rc = h->shifts.ensure(sizeof(double) * 81);
+    void* dst = nullptr;
+    if (rc == PD_OK) {
+        h->nbox = B->nb;
+        if (!inbox) {
+            memcpy(st + ox, r->x.data(), sizeof(double) * 3 * n);
+            memcpy(st + ov, r->v.data(), sizeof(double) * 3 * n);
+        }
+        cudaError_t ce = cudaMemcpyAsync(h->boxes.p, B, sizeof(BoxSet<double>), cudaMemcpyHostToDevice, s->as);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(h->shifts.p, sh, sizeof(double) * 81, cudaMemcpyHostToDevice, s->as);
+        const char* xs = nullptr;  // device view of the submitted positions; velocities follow
+        if (ce == cudaSuccess && !inbox) {
+            ce = cudaHostGetDevicePointer(&dst, st, 0);
+            xs = static_cast<const char*>(dst) + ox;
+        } else if (ce == cudaSuccess) {
+            xs = s->inbox.dev + r->in_lo;  // the inbox region: positions, then velocities at the same distance
+        }
+        if (ce == cudaSuccess && n > 0) {
+            pd::launch(k_srv_unpack, (unsigned)std::min((n + 255) / 256, 148L * 8), 256, 0, s->as,
+                       reinterpret_cast<const double*>(xs), reinterpret_cast<const double*>(xs + (ov - ox)), n,
+                       (double4*)h->pos, (float*)h->props[sl.vp].d, h->cap);
+            ce = cudaGetLastError();
+        }
+        if (ce != cudaSuccess) {
+            set_error("serving: upload failed: %s", cudaGetErrorString(ce));
+            rc = PD_ECUDA;
+        }
     }
-    if (tmp.empty()) return ring_mark(s, lo, need);
-    PD_CUDA(cudaStreamSynchronize(s->as));
-    return PD_OK;
+    if (!tmp) return rc == PD_OK ? ring_mark(s, lo, need) : rc;
+    cudaStreamSynchronize(s->as);
+    cudaFreeHost(tmp);
+    return rc;
 }
 
 static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r);
@@ -1438,72 +1593,79 @@ static int admit_one(pd_srv s, SrvReq* r, int slot) {
     return PD_OK;
 }
 
-// retire the finished systems: final positions (offsets -> FP64), ids and
-// energies to the slots' pinned staging, one wait, results reordered by id
+// download bytes of one finished system: positions in id order, energies
+static size_t retire_bytes(const SrvReq* r) {
+    return (sizeof(double) * 3 * r->n + sizeof(double) * 4 * r->steps + 127) & ~(size_t)63;
+}
+
+// retire the finished systems: each system's final positions are formed in
+// FP64 and written in id order on the GPU, then copied with its energies to the
+// pinned outbox, where pd_srv_result reads them; when the outbox has no room, to
+// the download buffer and from there to host vectors, in groups that fit that
+// buffer, one wait per group
 static int retire_all(pd_srv s, std::vector<std::pair<SrvReq*, bool>>& fin) {
-    // download layout per system: position records, ids, energies (64-byte aligned)
-    std::vector<size_t> off(fin.size(), 0);
-    size_t need = 0;
-    for (size_t k = 0; k < fin.size(); ++k) {
-        if (fin[k].second) continue;
-        const long n = fin[k].first->n;
-        off[k] = need;
-        need += (sizeof(double4) * n + sizeof(int) * n + sizeof(double) * 4 * fin[k].first->steps + 192) &
-                ~(size_t)63;
-    }
-    if (need > s->down_bytes) {
-        if (s->down) cudaFreeHost(s->down);
-        s->down = nullptr;
-        s->down_bytes = 0;
-        const size_t b = need + need / 2;
-        if (cudaMallocHost((void**)&s->down, b) != cudaSuccess) {
-            cudaGetLastError();
-            s->down = nullptr;
-            set_error("serving: pinned download buffer of %zu bytes failed", b);
-            return PD_ENOMEM;
-        }
-        s->down_bytes = b;
-    }
-    bool any = false;
-    for (size_t k = 0; k < fin.size(); ++k) {
-        if (fin[k].second) continue;
-        SrvReq* r = fin[k].first;
-        SrvSlot& sl = s->slots[r->slot];
-        pd_vd h = sl.h;
-        const long n = r->n;
-        PD_TRY(mixed_to_positions(h, sl.md->vl->cl, sl.md->off, s->as));
-        char* st = s->down + off[k];
-        const size_t og = sizeof(double4) * n, oe = (og + sizeof(int) * n + 63) & ~(size_t)63;
-        PD_CUDA(cudaMemcpyAsync(st, h->pos, og, cudaMemcpyDeviceToHost, s->as));
-        PD_CUDA(cudaMemcpyAsync(st + og, h->gid, sizeof(int) * n, cudaMemcpyDeviceToHost, s->as));
-        PD_CUDA(cudaMemcpyAsync(st + oe, sl.Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost, s->as));
-        any = true;
-    }
-    if (any) PD_CUDA(cudaStreamSynchronize(s->as));
-    for (size_t k = 0; k < fin.size(); ++k) {
-        SrvReq* r = fin[k].first;
-        if (!fin[k].second) {
-            const long n = r->n;
-            const char* st = s->down + off[k];
-            const size_t og = sizeof(double4) * n, oe = (og + sizeof(int) * n + 63) & ~(size_t)63;
-            const double4* P = reinterpret_cast<const double4*>(st);
-            const int* gid = reinterpret_cast<const int*>(st + og);
-            const double* E = reinterpret_cast<const double*>(st + oe);
-            r->xo.assign(3 * (size_t)n, 0.0);
-            for (long i = 0; i < n; ++i) {
-                const size_t g = (size_t)gid[i];
-                r->xo[3 * g] = P[i].x;
-                r->xo[3 * g + 1] = P[i].y;
-                r->xo[3 * g + 2] = P[i].z;
+    std::vector<char*> dst(fin.size(), nullptr);
+    size_t k0 = 0;
+    while (k0 < fin.size()) {
+        size_t k1 = k0, used = 0;
+        for (; k1 < fin.size(); ++k1) {
+            if (fin[k1].second) continue;
+            SrvReq* r = fin[k1].first;
+            const size_t b = retire_bytes(r);
+            if ((dst[k1] = s->outbox.take(r->ticket, b, r->out_lo, s->ev_free))) continue;
+            if (b > s->down_bytes) {  // larger than the download buffer: alone in a group, buffer grown
+                if (used > 0) break;
+                if (s->down) cudaFreeHost(s->down);
+                s->down = nullptr;
+                s->down_bytes = 0;
+                if (cudaMallocHost((void**)&s->down, b) != cudaSuccess) {
+                    cudaGetLastError();
+                    s->down = nullptr;
+                    set_error("serving: pinned download buffer of %zu bytes failed", b);
+                    return PD_ENOMEM;
+                }
+                s->down_bytes = b;
             }
-            r->E.assign(E, E + 4 * (size_t)r->steps);
-            for (int k = 0; k < r->steps; ++k) s->rebuilds += E[4 * k + 3] != 0.0 ? 1 : 0;
+            if (used + b > s->down_bytes) break;
+            dst[k1] = s->down + used;
+            used += b;
         }
-        r->state = fin[k].second ? 3 : 2;
-        r->t_done = now_s(s);
-        s->used -= r->bytes;
-        s->systems_done++;
-        s->completed.push_back(r->ticket);
+        bool any = false;
+        for (size_t k = k0; k < k1; ++k) {
+            if (fin[k].second) continue;
+            SrvReq* r = fin[k].first;
+            SrvSlot& sl = s->slots[r->slot];
+            pd_vd h = sl.h;
+            const long n = r->n;
+            double* xo = reinterpret_cast<double*>(h->pos);  // 24 n bytes of the 32 n held
+            PD_TRY(mixed_to_positions_by_id(h, sl.md->vl->cl, sl.md->off, xo, s->as));
+            const size_t ox = sizeof(double) * 3 * n, oe = (ox + 63) & ~(size_t)63;
+            PD_CUDA(cudaMemcpyAsync(dst[k], xo, ox, cudaMemcpyDeviceToHost, s->as));
+            PD_CUDA(cudaMemcpyAsync(dst[k] + oe, sl.Edev.p, sizeof(double) * 4 * r->steps, cudaMemcpyDeviceToHost,
+                                    s->as));
+            any = true;
+        }
+        if (any) PD_CUDA(cudaStreamSynchronize(s->as));
+        for (size_t k = k0; k < k1; ++k) {
+            SrvReq* r = fin[k].first;
+            if (!fin[k].second) {
+                const long n = r->n;
+                const size_t ox = sizeof(double) * 3 * n, oe = (ox + 63) & ~(size_t)63;
+                const double* E = reinterpret_cast<const double*>(dst[k] + oe);
+                if (r->out_lo < 0) {
+                    const double* X = reinterpret_cast<const double*>(dst[k]);
+                    r->xo.assign(X, X + 3 * (size_t)n);
+                    r->E.assign(E, E + 4 * (size_t)r->steps);
+                }
+                for (int j = 0; j < r->steps; ++j) s->rebuilds += E[4 * j + 3] != 0.0 ? 1 : 0;
+            }
+            r->state = fin[k].second ? 3 : 2;
+            r->t_done = now_s(s);
+            s->used -= r->bytes;
+            s->systems_done++;
+            s->completed.push_back(r->ticket);
+        }
+        k0 = k1;
     }
     fin.clear();
     return PD_OK;
@@ -1564,9 +1726,14 @@ int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj
         (r = s->ovf_b.ensure(sizeof(long) * s->tpart_cap)) != PD_OK ||
         cudaMallocHost(&s->flags_h, sizeof(unsigned int) * max_slots) != cudaSuccess ||
         cudaMallocHost((void**)&s->up, (s->up_bytes = std::min((size_t)256 << 20,
-                                                               std::max((size_t)32 << 20,
+                                                               std::max((size_t)8 << 20,
                                                                         (size_t)hbm_budget_bytes / 64)))) !=
             cudaSuccess ||
+        cudaMallocHost((void**)&s->down, (s->down_bytes = s->up_bytes)) != cudaSuccess ||
+        s->inbox.create(std::min((size_t)1 << 30, std::max((size_t)8 << 20, (size_t)hbm_budget_bytes / 32))) !=
+            PD_OK ||
+        s->outbox.create(std::min((size_t)1 << 30, std::max((size_t)8 << 20, (size_t)hbm_budget_bytes / 32))) !=
+            PD_OK ||
         cudaMallocHost(&s->errs_h, sizeof(unsigned int) * max_slots) != cudaSuccess) {
         cudaGetLastError();
         pd_srv_destroy(s);
@@ -1618,6 +1785,8 @@ int pd_srv_destroy(pd_srv s) {
     for (cudaEvent_t e : s->ev_free) cudaEventDestroy(e);
     if (s->up) cudaFreeHost(s->up);
     if (s->down) cudaFreeHost(s->down);
+    s->inbox.destroy();
+    s->outbox.destroy();
     s->slots.clear();
     for (auto& ge : s->gstep)
         if (ge) cudaGraphExecDestroy(ge);
@@ -1653,13 +1822,21 @@ int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const doub
     r->n = n;
     r->L = box;
     r->steps = steps;
-    r->x.assign(x_host, x_host + 3 * n);
-    r->v.assign(v_host, v_host + 3 * n);
     r->bytes = estimate_bytes(n);
     r->t_submit = now_s(s);
     if ((long)r->bytes > s->budget) {
         set_error("pd_srv_submit: system of %ld particles exceeds the HBM budget", n);
         return PD_ENOMEM;
+    }
+    // the state to the pinned inbox (positions, then velocities at the staging
+    // layout's distance), else to host vectors staged at admission
+    const size_t half = (sizeof(double) * 3 * n + 63) & ~(size_t)63;
+    if (char* p = s->inbox.take(r->ticket, half + sizeof(double) * 3 * n, r->in_lo, s->ev_free)) {
+        memcpy(p, x_host, sizeof(double) * 3 * n);
+        memcpy(p + half, v_host, sizeof(double) * 3 * n);
+    } else {
+        r->x.assign(x_host, x_host + 3 * n);
+        r->v.assign(v_host, v_host + 3 * n);
     }
     *ticket = r->ticket;
     s->queue.push_back(r->ticket);
@@ -1704,6 +1881,7 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
         s->queue.pop_front();
         s->used += r->bytes;
         int rc = admit_one(s, r, slot);
+        inbox_release(s, r);
         if (rc != PD_OK) {
             r->state = 3;
             s->used -= r->bytes;
@@ -1750,7 +1928,9 @@ int pd_srv_tick(pd_srv s, int* n_active, int* n_queued) {
     s->active.swap(keep);
     if (s->active.empty() && !s->finished.empty()) {
         // nothing left to step: retire now rather than at the next tick
+        t_ret = now_s(s);
         PD_TRY(retire_all(s, s->finished));
+        s->ms[3] += 1e3 * (now_s(s) - t_ret);
     }
     if (n_queued) *n_queued = (int)s->queue.size();
     if (n_active) *n_active = (int)s->active.size();
@@ -1783,8 +1963,15 @@ int pd_srv_result(pd_srv s, long ticket, double* x_out, double* E_out, double* t
     if (it == s->reqs.end()) return PD_EINVAL;
     SrvReq* r = it->second.get();
     if (r->state != 2) return PD_ESTATE;
-    if (x_out) memcpy(x_out, r->xo.data(), sizeof(double) * r->xo.size());
-    if (E_out) memcpy(E_out, r->E.data(), sizeof(double) * r->E.size());
+    if (r->out_lo >= 0) {  // in the pinned outbox: positions, then energies 64-byte aligned
+        const char* b = s->outbox.base + r->out_lo;
+        const size_t ox = sizeof(double) * 3 * r->n, oe = (ox + 63) & ~(size_t)63;
+        if (x_out) memcpy(x_out, b, ox);
+        if (E_out) memcpy(E_out, b + oe, sizeof(double) * 4 * r->steps);
+    } else {
+        if (x_out) memcpy(x_out, r->xo.data(), sizeof(double) * r->xo.size());
+        if (E_out) memcpy(E_out, r->E.data(), sizeof(double) * r->E.size());
+    }
     if (times) {
         times[0] = r->t_submit;
         times[1] = r->t_admit;
@@ -1797,6 +1984,10 @@ int pd_srv_release(pd_srv s, long ticket) {
     if (!s) return PD_EINVAL;
     auto it = s->reqs.find(ticket);
     if (it == s->reqs.end() || (it->second->state != 2 && it->second->state != 3)) return PD_EINVAL;
+    if (it->second->out_lo >= 0) {
+        if (PinnedFifo::Region* g = s->outbox.find(ticket)) g->done = true;
+        s->outbox.trim(s->ev_free);
+    }
     s->reqs.erase(it);
     return PD_OK;
 }

@@ -143,6 +143,8 @@ def lib():
             "pd_md_set_timing": ([vp, ip], ip),
             "pd_md_timers": ([vp, P(ctypes.c_double), P(ctypes.c_long)], ip),
             "pd_launch_count": ([], ctypes.c_ulonglong),
+            "pd_empty_cache": ([], ip),
+            "pd_set_cache_limit": ([lp, P(ctypes.c_long)], ip),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
@@ -191,6 +193,18 @@ def _ptr(a):
 def launch_count():
     """Kernels launched by libpdgpu.so so far."""
     return int(lib().pd_launch_count())
+
+
+def empty_cache():
+    """Return the device blocks the library keeps for reuse to the driver."""
+    check(lib().pd_empty_cache())
+
+
+def set_cache_limit(limit_bytes=-1):
+    """Set the limit of the device block cache (-1: unchanged); returns the bytes held."""
+    held = ctypes.c_long(0)
+    check(lib().pd_set_cache_limit(int(limit_bytes), ctypes.byref(held)))
+    return held.value
 
 
 def selftest_recip(x):

@@ -97,3 +97,57 @@ def test_admission_by_budget(pd):
     times = [srv.result(t)[2] for t in tickets]
     assert times[0][2] <= times[1][1] and times[1][2] <= times[2][1]   # FIFO, one at a time
     assert srv.stats()["systems_done"] == 3
+
+
+def test_staging_paths_alone_equals_in_mix(pd):
+    # a 512 MB budget: 8 MB upload ring and download buffer, 16 MB inbox and
+    # outbox.  Six finished systems that are not released hold 14.4 MB of the
+    # outbox; then the 350k system uploads through staging of its own (it does not
+    # fit the inbox) and retires through the grown download buffer, the 120k
+    # system through the download buffer, the 60k system through the outbox.
+    # Every result equals the system served alone, bit for bit.
+    fillers = [_sys(100000, 70 + k) for k in range(6)]
+    systems = [_sys(n, 40 + k) for k, n in enumerate([350000, 120000, 60000])]
+    srv = pd.Server(512 << 20, max_slots=4, dt=0.005, skin=0.3, autotune=False, tx=5)
+    held = [srv.submit(x, v, L, 10) for (x, v, L) in fillers]
+    srv.run_until_done(held)
+    tickets = [srv.submit(x, v, L, 10) for (x, v, L) in systems]
+    srv.run_until_done(tickets)
+    for t, s in zip(tickets + held, systems + fillers):
+        xm, Em, _ = srv.result(t)
+        (xa, Ea, _), = _serve(pd, [s], steps=10, budget=512 << 20, slots=4)[0]
+        assert np.array_equal(Em, Ea)
+        assert np.array_equal(xm, xa)
+        assert xm.shape == s[0].shape and np.all(np.isfinite(xm))
+
+
+def test_inbox_wraps_and_falls_back(pd):
+    # 16 MB inbox: the first wave fills it (the last systems fall back to host
+    # copies), the second wave is submitted while the first runs and reuses the
+    # regions freed by its admissions; every result equals the system served alone
+    rng = np.random.default_rng(5)
+    sizes = [int(n) for n in rng.integers(20000, 60000, size=18)]
+    systems = [_sys(n, 60 + k) for k, n in enumerate(sizes)]
+    srv = pd.Server(512 << 20, max_slots=4, dt=0.005, skin=0.3, autotune=False, tx=5)
+    tickets = [srv.submit(x, v, L, 10) for (x, v, L) in systems[:12]]
+    for _ in range(6):
+        srv.tick()
+    tickets += [srv.submit(x, v, L, 10) for (x, v, L) in systems[12:]]
+    srv.run_until_done(tickets)
+    for t, s in zip(tickets, systems):
+        xm, Em, _ = srv.result(t)
+        (xa, Ea, _), = _serve(pd, [s], steps=10, budget=512 << 20, slots=4)[0]
+        assert np.array_equal(Em, Ea)
+        assert np.array_equal(xm, xa)
+    # results released out of order free the outbox from its oldest region on;
+    # a third wave then retires into the freed space
+    for t in reversed(tickets):
+        srv.release(t)
+    third = systems[:6]
+    t3 = [srv.submit(x, v, L, 10) for (x, v, L) in third]
+    srv.run_until_done(t3)
+    for t, s in zip(t3, third):
+        xm, Em, _ = srv.result(t)
+        (xa, Ea, _), = _serve(pd, [s], steps=10, budget=512 << 20, slots=4)[0]
+        assert np.array_equal(Em, Ea)
+        assert np.array_equal(xm, xa)
