@@ -50,6 +50,15 @@ def test_bad_arguments_rejected_without_gpu():
     assert L.pd_destroy(None) == -1
     assert L.pd_map(None, 0, None) == -1
     assert b"invalid" in L.pd_last_error()
+    # the device block cache: nothing held, emptying it makes no CUDA call
+    held = ctypes.c_long(-1)
+    assert L.pd_set_cache_limit(ctypes.c_long(-1), ctypes.byref(held)) == 0 and held.value == 0
+    assert L.pd_empty_cache() == 0
+    # serving entry points refuse a null server
+    t = ctypes.c_long(0)
+    assert L.pd_srv_submit(None, ctypes.c_long(10), ctypes.c_double(10.0), None, None, 5, ctypes.byref(t)) == -1
+    assert L.pd_srv_result(None, ctypes.c_long(0), None, None, None) == -1
+    assert L.pd_srv_release(None, ctypes.c_long(0)) == -1
 
 
 def test_package_fails_loudly_without_library(tmp_path, monkeypatch):
