@@ -1,0 +1,75 @@
+"""Slab decomposition with the library computing each rank's forces on the GPU.
+
+Two ranks (gloo processes on the host, exchanging host tensors) share the one
+GPU of this run: each builds its extended slab (own particles, then the halo
+from the neighbouring slabs) as a vector with the split axis non-periodic and
+computes LJ forces with the library's cell list.  Their forces, put together,
+equal the library's forces of the whole periodic system within 1e-10 of
+(|F| + F_rms).  The kernels of the two ranks never wait on each other.
+"""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, nside, q):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200 import workloads
+    from openfpm_pdata_b200.decomp import DistParticles, SlabDecomposition, lj_forces_distributed
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        x, _, L = workloads.lj_lattice(nside, 1.1, 0.05, seed=21)
+        n = x.shape[0]
+        dec = SlabDecomposition(np.zeros(3), np.full(3, L), (1, 1, 1), 2.5, world)
+        dp = DistParticles(dec)
+        xs = torch.from_numpy(x) if rank == 0 else torch.zeros((0, 3), dtype=torch.float64)
+        gs = torch.arange(n, dtype=torch.int32) if rank == 0 else torch.zeros(0, dtype=torch.int32)
+        xl, (gl,) = dp.map(xs, [gs])
+        f = lj_forces_distributed(dp, xl)
+        q.put((rank, gl.numpy(), f.numpy()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_decomposed_forces_equal_whole_system():
+    import torch.multiprocessing as mp
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200 import workloads
+    from openfpm_pdata_b200.decomp import lj_forces_library
+    nside, world = 20, 2
+    x, _, L = workloads.lj_lattice(nside, 1.1, 0.05, seed=21)
+    n = x.shape[0]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, nside, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    f = np.full((n, 3), np.nan)
+    for _, gl, fl in out:
+        f[gl] = fl
+    fw = lj_forces_library(x, np.zeros(3), np.full(3, L), (1, 1, 1))
+    frms = np.sqrt((fw ** 2).sum(axis=1).mean())
+    assert np.all(np.abs(f - fw) <= 1e-10 * (np.abs(fw) + frms))
