@@ -190,3 +190,21 @@ def lj_forces_distributed(dp, x, force_fn=lj_forces_library, **kw):
     allx = torch.cat([x, xh]).cpu().numpy()
     f = force_fn(allx, lo, hi, bc, **kw)
     return torch.from_numpy(np.ascontiguousarray(f[: x.shape[0]])).to(x.device)
+
+
+def md_distributed(dp, x, v, steps, props=(), dt=0.005, mass=1.0, force_fn=lj_forces_library, **kw):
+    """Velocity-Verlet steps of the decomposed system (x, v and `props` of this
+    rank's particles after `map`): each step kicks, drifts, migrates the
+    particles to their owners (`map`, carrying v and props) and exchanges the
+    halo for the new forces.  Returns (x, v, props) held here at the end."""
+    h = 0.5 * dt / mass
+    props = list(props)
+    f = lj_forces_distributed(dp, x, force_fn, **kw)
+    for _ in range(steps):
+        v = v + h * f
+        x = x + dt * v
+        x, moved = dp.map(x, [v] + props)
+        v, props = moved[0], moved[1:]
+        f = lj_forces_distributed(dp, x, force_fn, **kw)
+        v = v + h * f
+    return x, v, props

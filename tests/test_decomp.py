@@ -135,6 +135,71 @@ def test_map_ghost_get_and_forces(world, bc):
     assert np.max(np.abs(f - fw)) <= 1e-12 * frms
 
 
+def _rank_md(rank, world, port, nside, steps, q):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200.decomp import DistParticles, SlabDecomposition, md_distributed
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        from openfpm_pdata_b200 import workloads
+        x, v, L = workloads.lj_lattice(nside, 1.1, 0.05, seed=9)
+        n = x.shape[0]
+        dp = DistParticles(SlabDecomposition(np.zeros(3), np.full(3, L), (1, 1, 1), RC, world, axis=0))
+        xs = torch.from_numpy(x) if rank == 0 else torch.zeros((0, 3), dtype=torch.float64)
+        vs = torch.from_numpy(v) if rank == 0 else torch.zeros((0, 3), dtype=torch.float64)
+        gs = torch.arange(n, dtype=torch.int32) if rank == 0 else torch.zeros(0, dtype=torch.int32)
+        xl, (vl, gl) = dp.map(xs, [vs, gs])
+        xl, vl, (gl,) = md_distributed(dp, xl, vl, steps, props=[gl], force_fn=brute_lj)
+        q.put((rank, gl.numpy(), xl.numpy(), vl.numpy()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_md_over_ranks_follows_the_whole_system():
+    """Velocity Verlet with map and ghost_get every step on 2 ranks follows the
+    same steps on the whole periodic system (positions within 1e-10)."""
+    import torch.multiprocessing as mp
+    nside, steps, world = 7, 8, 2
+    x, v, L = _system_v(nside, 9)
+    n = x.shape[0]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_md, args=(r, world, port, nside, steps, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    xd, vd = np.full((n, 3), np.nan), np.full((n, 3), np.nan)
+    for _, gl, xl, vl in out:
+        xd[gl], vd[gl] = xl, vl
+    lo, hi, bc = np.zeros(3), np.full(3, L), (1, 1, 1)
+    h = 0.5 * 0.005
+    f = brute_lj(x, lo, hi, bc)
+    for _ in range(steps):
+        v = v + h * f
+        x = x + 0.005 * v
+        x = np.mod(x, L)
+        f = brute_lj(x, lo, hi, bc)
+        v = v + h * f
+    d = xd - x
+    d -= L * np.round(d / L)
+    assert np.max(np.abs(d)) < 1e-10
+    assert np.max(np.abs(vd - v)) < 1e-9
+
+
+def _system_v(nside, seed):
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200 import workloads
+    return workloads.lj_lattice(nside, 1.1, 0.05, seed=seed)
+
+
 def test_slab_narrower_than_ghost_refused():
     sys.path.insert(0, ROOT)
     from openfpm_pdata_b200.decomp import SlabDecomposition
