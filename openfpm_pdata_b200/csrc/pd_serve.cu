@@ -41,6 +41,8 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <condition_variable>
+#include <mutex>
 #include <system_error>
 #include <thread>
 #include <vector>
@@ -963,6 +965,89 @@ struct SrvReq {
     bool first = true;  // the next step graph runs its first build and forces
 };
 
+// Copies of the submitted arrays into pinned memory: one core copies at about
+// 6 GB/s, so a submission of a megabyte or more is cut into pieces of at least
+// 512 KB that the caller and up to three workers copy.  The workers start at
+// the first such submission and live as long as the server; if they cannot be
+// started the caller copies everything.
+struct CopyJob {
+    char* dst;
+    const char* src;
+    size_t bytes;
+};
+
+struct CopyPool {
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable wake, done;
+    std::vector<CopyJob> pieces;
+    size_t next = 0, left = 0;
+    bool stop = false, tried = false;
+
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        wake.notify_all();
+        for (auto& t : workers) t.join();
+    }
+    // take and copy pieces until none is left
+    void drain() {
+        for (;;) {
+            CopyJob c;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (next >= pieces.size()) return;
+                c = pieces[next++];
+            }
+            memcpy(c.dst, c.src, c.bytes);
+            std::lock_guard<std::mutex> lk(mu);
+            if (--left == 0) done.notify_all();
+        }
+    }
+    void worker() {
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                wake.wait(lk, [this] { return stop || next < pieces.size(); });
+                if (stop) return;
+            }
+            drain();
+        }
+    }
+    void copy(const CopyJob* jobs, int nj) {
+        size_t total = 0;
+        for (int j = 0; j < nj; ++j) total += jobs[j].bytes;
+        if (total < ((size_t)1 << 20)) {
+            for (int j = 0; j < nj; ++j) memcpy(jobs[j].dst, jobs[j].src, jobs[j].bytes);
+            return;
+        }
+        if (!tried) {
+            tried = true;
+            try {
+                for (int k = 0; k < 3; ++k) workers.emplace_back([this] { worker(); });
+            } catch (const std::system_error&) {
+            }
+        }
+        const size_t T = std::min<size_t>(workers.size() + 1, std::max<size_t>(1, total / ((size_t)512 << 10)));
+        const size_t want = (total + T - 1) / T;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            pieces.clear();
+            for (int j = 0; j < nj; ++j)
+                for (size_t a = 0; a < jobs[j].bytes; a += want)
+                    pieces.push_back({jobs[j].dst + a, jobs[j].src + a, std::min(want, jobs[j].bytes - a)});
+            next = 0;
+            left = pieces.size();
+        }
+        wake.notify_all();
+        drain();
+        std::unique_lock<std::mutex> lk(mu);
+        done.wait(lk, [this] { return left == 0; });
+    }
+};
+
 struct pd_srv_s {
     long budget = 0;
     int max_slots = 0;
@@ -1008,6 +1093,7 @@ struct pd_srv_s {
     // pinned outbox: a finished system's positions and energies are copied here by
     // the GPU and read by pd_srv_result; regions are freed at pd_srv_release
     PinnedFifo outbox;
+    std::unique_ptr<CopyPool> copier;  // submissions' copies into the inbox
     bool adm_pending = false;
     cudaGraphExec_t gstep[4] = {nullptr, nullptr, nullptr, nullptr};  // 1, 2, 4, 8 steps per launch
     bool dirty = true;
@@ -1812,48 +1898,6 @@ int pd_srv_set_tuning(pd_srv s, int autotune, int tx) {
     return PD_OK;
 }
 
-// Copies into pinned memory of the submitted arrays: one core copies at about
-// 6 GB/s, so a submission of a megabyte or more is split into pieces of at
-// least 512 KB copied by up to four threads (the caller's among them); if a
-// thread cannot be started, the caller copies its piece.
-struct CopyJob {
-    char* dst;
-    const char* src;
-    size_t bytes;
-};
-static void copy_jobs(const CopyJob* jobs, int nj) {
-    size_t total = 0;
-    for (int j = 0; j < nj; ++j) total += jobs[j].bytes;
-    const size_t piece_min = (size_t)512 << 10;
-    const int T = (int)std::min<size_t>(4, std::max<size_t>(1, total / piece_min));
-    if (T <= 1 || total < ((size_t)1 << 20)) {
-        for (int j = 0; j < nj; ++j) memcpy(jobs[j].dst, jobs[j].src, jobs[j].bytes);
-        return;
-    }
-    // pieces of about total / T bytes, cut across the jobs
-    std::vector<CopyJob> pieces;
-    const size_t want = (total + T - 1) / T;
-    for (int j = 0; j < nj; ++j)
-        for (size_t a = 0; a < jobs[j].bytes; a += want)
-            pieces.push_back({jobs[j].dst + a, jobs[j].src + a, std::min(want, jobs[j].bytes - a)});
-    std::vector<std::thread> th;
-    std::vector<const CopyJob*> mine;
-    for (size_t k = 0; k < pieces.size(); ++k) {
-        const CopyJob* c = &pieces[k];
-        if (k % (size_t)T == 0) {
-            mine.push_back(c);
-            continue;
-        }
-        try {
-            th.emplace_back([c] { memcpy(c->dst, c->src, c->bytes); });
-        } catch (const std::system_error&) {
-            mine.push_back(c);
-        }
-    }
-    for (const CopyJob* c : mine) memcpy(c->dst, c->src, c->bytes);
-    for (auto& t : th) t.join();
-}
-
 int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const double* v_host, int steps,
                   long* ticket) {
     if (!s || n < 1 || !(box > 0) || !x_host || !v_host || steps < 1 || !ticket) return PD_EINVAL;
@@ -1878,7 +1922,8 @@ int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const doub
     if (char* p = s->inbox.take(r->ticket, half + sizeof(double) * 3 * n, r->in_lo, s->ev_free)) {
         const CopyJob jobs[2] = {{p, reinterpret_cast<const char*>(x_host), sizeof(double) * 3 * n},
                                  {p + half, reinterpret_cast<const char*>(v_host), sizeof(double) * 3 * n}};
-        copy_jobs(jobs, 2);
+        if (!s->copier) s->copier.reset(new CopyPool());
+        s->copier->copy(jobs, 2);
     } else {
         r->x.assign(x_host, x_host + 3 * n);
         r->v.assign(v_host, v_host + 3 * n);
