@@ -180,7 +180,9 @@ int pd_size(pd_vd h, long* size_local, long* size_with_ghost);
 /* resize of the local part (drops ghosts) -- vector_dist.hpp:923-984 add/resize */
 int pd_resize(pd_vd h, long n);
 /* hostToDevicePos / deviceToHostPos -- vector_dist.hpp:2984-3030; host AoS xyz in
- * the vector's dtype, particles [offset, offset+count) */
+ * the vector's dtype, particles [offset, offset+count).  These four copies also
+ * take a device pointer (unified addressing picks the direction), so device
+ * arrays of another library are read and written without a host round trip. */
 int pd_h2d_pos(pd_vd h, const void* host_xyz, long offset, long count, void* stream);
 int pd_d2h_pos(pd_vd h, void* host_xyz, long offset, long count, void* stream);
 /* hostToDeviceProp<prp> / deviceToHostProp<prp>; host component-major [ncomp][count] */

@@ -574,7 +574,7 @@ int pd_h2d_pos(pd_vd h, const void* host_xyz, long offset, long count, void* str
     cudaStream_t st = S(stream);
     size_t es = h->dtype == PD_F64 ? 8 : 4;
     PD_TRY(h->tmp.ensure(es * 3 * count));
-    PD_CUDA(cudaMemcpyAsync(h->tmp.p, host_xyz, es * 3 * count, cudaMemcpyHostToDevice, st));
+    PD_CUDA(cudaMemcpyAsync(h->tmp.p, host_xyz, es * 3 * count, cudaMemcpyDefault, st));  // host or device source
     unsigned g = grid_for(count, 256);
     if (h->dtype == PD_F64)
         pd::launch(k_expand_pos<double>, g, 256, 0, st, h->tmp.as<double>(), count, (double4*)h->pos, offset);
@@ -599,7 +599,7 @@ int pd_d2h_pos(pd_vd h, void* host_xyz, long offset, long count, void* stream) {
     else
         pd::launch(k_pack_pos<float>, g, 256, 0, st, (const float4*)h->pos, offset, count, h->tmp.as<float>());
     PD_LAUNCH_CHECK();
-    PD_CUDA(cudaMemcpyAsync(host_xyz, h->tmp.p, es * 3 * count, cudaMemcpyDeviceToHost, st));
+    PD_CUDA(cudaMemcpyAsync(host_xyz, h->tmp.p, es * 3 * count, cudaMemcpyDefault, st));  // host or device target
     PD_CUDA(cudaStreamSynchronize(st));
     return PD_OK;
 }
@@ -615,7 +615,7 @@ int pd_h2d_prop(pd_vd h, int prop, const void* host, long offset, long count, vo
     for (int c = 0; c < P.ncomp; ++c)
         PD_CUDA(cudaMemcpyAsync(P.d + ((size_t)c * h->cap + offset) * P.esize,
                                 (const char*)host + (size_t)c * count * P.esize, (size_t)count * P.esize,
-                                cudaMemcpyHostToDevice, st));
+                                cudaMemcpyDefault, st));  // host or device source
     return PD_OK;
 }
 
@@ -630,7 +630,7 @@ int pd_d2h_prop(pd_vd h, int prop, void* host, long offset, long count, void* st
     for (int c = 0; c < P.ncomp; ++c)
         PD_CUDA(cudaMemcpyAsync((char*)host + (size_t)c * count * P.esize,
                                 P.d + ((size_t)c * h->cap + offset) * P.esize, (size_t)count * P.esize,
-                                cudaMemcpyDeviceToHost, st));
+                                cudaMemcpyDefault, st));  // host or device target
     PD_CUDA(cudaStreamSynchronize(st));
     return PD_OK;
 }

@@ -167,11 +167,13 @@ class DistParticles:
 
 
 def lj_forces_library(x, lo, hi, bc, r_cut=2.5, eps=1.0, sigma=1.0):
-    """LJ forces of the particles x [n, 3] (float64) in the box (lo, hi, bc),
-    computed by the single-GPU library (cell list of side r_cut, periodic images
-    of the periodic axes)."""
+    """LJ forces of the particles x [n, 3] (float64; a host array, or a CUDA
+    tensor kept on the GPU) in the box (lo, hi, bc), computed by the single-GPU
+    library (cell list of side r_cut, periodic images of the periodic axes)."""
     from . import pd
-    x = np.ascontiguousarray(np.asarray(x, np.float64))
+    on_gpu = isinstance(x, torch.Tensor) and x.is_cuda
+    if not on_gpu:
+        x = np.ascontiguousarray(np.asarray(x, np.float64))
     n = x.shape[0]
     vd = pd.VectorDist(n, lo, hi, np.asarray(bc, np.int32), r_cut, dtype=np.float64, props=[(pd.PD_F64, 3)])
     vd.hostToDevicePos(x)
@@ -179,16 +181,20 @@ def lj_forces_library(x, lo, hi, bc, r_cut=2.5, eps=1.0, sigma=1.0):
     cl = vd.getCellListGPU(r_cut)
     vd.updateCellListGPU(cl)
     vd.lj_forces(0, cl=cl, eps=eps, sigma=sigma, r_cut=r_cut)
-    return vd.deviceToHostProp(0)[:n]
+    return vd.deviceToHostProp(0, count=n, device=on_gpu)
 
 
 def lj_forces_distributed(dp, x, force_fn=lj_forces_library, **kw):
     """Forces of this rank's particles x (after `map`): halo exchange, then the
-    single-GPU forces on the extended slab; `force_fn(x_all, lo, hi, bc, **kw)`."""
+    single-GPU forces on the extended slab; `force_fn(x_all, lo, hi, bc, **kw)`.
+    CUDA tensors stay on the GPU (the library reads and writes them in place of
+    host arrays); host tensors go through numpy."""
     xh, _ = dp.ghost_get(x)
     lo, hi, bc = dp.dec.local_box(dp.rank)
-    allx = torch.cat([x, xh]).cpu().numpy()
-    f = force_fn(allx, lo, hi, bc, **kw)
+    allx = torch.cat([x, xh])
+    if allx.is_cuda and force_fn is lj_forces_library:
+        return force_fn(allx.contiguous(), lo, hi, bc, **kw)[: x.shape[0]]
+    f = force_fn(allx.cpu().numpy(), lo, hi, bc, **kw)
     return torch.from_numpy(np.ascontiguousarray(f[: x.shape[0]])).to(x.device)
 
 

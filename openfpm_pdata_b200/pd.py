@@ -190,6 +190,17 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _is_cuda_tensor(a):
+    return getattr(a, "is_cuda", False) and hasattr(a, "data_ptr")
+
+
+def _check_tensor(a, dtype):
+    import torch
+    want = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+    if a.dtype != want:
+        raise TypeError("tensor of %s expected, got %s" % (want, a.dtype))
+
+
 def launch_count():
     """Kernels launched by libpdgpu.so so far."""
     return int(lib().pd_launch_count())
@@ -332,6 +343,13 @@ class VectorDist:
 
     # -- host <-> device
     def hostToDevicePos(self, x, offset=0):
+        """positions [n][3] from a host array, or from a CUDA tensor of the
+        vector's dtype without a host round trip"""
+        if _is_cuda_tensor(x):
+            x = x.contiguous().reshape(-1, 3)
+            _check_tensor(x, self.dtype)
+            check(lib().pd_h2d_pos(self.h, ctypes.c_void_p(x.data_ptr()), int(offset), int(x.shape[0]), None))
+            return
         x = np.ascontiguousarray(x, dtype=self.dtype).reshape(-1, 3)
         check(lib().pd_h2d_pos(self.h, _ptr(x), int(offset), int(x.shape[0]), None))
 
@@ -372,9 +390,17 @@ class VectorDist:
             check(lib().pd_d2h_prop(self.h, int(p), _ptr(out), int(offset), int(n), None))
         return out
 
-    def deviceToHostProp(self, p, offset=0, count=None, with_ghost=True):
+    def deviceToHostProp(self, p, offset=0, count=None, with_ghost=True, device=False):
+        """property p as [n] or [n][ncomp]; device=True returns a CUDA tensor
+        (copied on the GPU, no host round trip)"""
         t, nc = self.props[p]
         n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
+        if device:
+            import torch
+            cm = torch.empty((nc, max(n, 0)), dtype=getattr(torch, np.dtype(_NP[t]).name), device="cuda")
+            if n:
+                check(lib().pd_d2h_prop(self.h, int(p), ctypes.c_void_p(cm.data_ptr()), int(offset), int(n), None))
+            return cm.t().contiguous() if nc > 1 else cm[0].clone()
         cm = np.zeros((nc, n), _NP[t])
         if n:
             check(lib().pd_d2h_prop(self.h, int(p), _ptr(cm), int(offset), int(n), None))

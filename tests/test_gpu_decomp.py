@@ -73,3 +73,23 @@ def test_decomposed_forces_equal_whole_system():
     fw = lj_forces_library(x, np.zeros(3), np.full(3, L), (1, 1, 1))
     frms = np.sqrt((fw ** 2).sum(axis=1).mean())
     assert np.all(np.abs(f - fw) <= 1e-10 * (np.abs(fw) + frms))
+
+
+def test_library_reads_and_writes_cuda_tensors():
+    """The copies of the C ABI take device pointers: forces from a CUDA tensor
+    of positions (kept on the GPU) equal those from the host array, bit for bit,
+    and so do the one-rank decomposition's forces on CUDA tensors."""
+    import torch
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200 import workloads
+    from openfpm_pdata_b200.decomp import DistParticles, SlabDecomposition, lj_forces_distributed, lj_forces_library
+    x, _, L = workloads.lj_lattice(14, 1.1, 0.05, seed=23)
+    lo, hi = np.zeros(3), np.full(3, L)
+    fh = lj_forces_library(x, lo, hi, (1, 1, 1))
+    xt = torch.from_numpy(x).cuda()
+    fd = lj_forces_library(xt, lo, hi, (1, 1, 1))
+    assert fd.is_cuda and np.array_equal(fd.cpu().numpy(), fh)
+    dp = DistParticles(SlabDecomposition(lo, hi, (1, 1, 1), 2.5, 1))
+    xl, _ = dp.map(xt)
+    f1 = lj_forces_distributed(dp, xl)
+    assert f1.is_cuda and np.array_equal(f1.cpu().numpy(), fh)

@@ -151,3 +151,23 @@ def test_inbox_wraps_and_falls_back(pd):
         (xa, Ea, _), = _serve(pd, [s], steps=10, budget=512 << 20, slots=4)[0]
         assert np.array_equal(Em, Ea)
         assert np.array_equal(xm, xa)
+
+
+def test_result_and_release_follow_the_request_state(pd):
+    # a result is refused until the system is done (PD_ESTATE), a release until it
+    # is done or failed; after the release the ticket is unknown; the result read
+    # twice from the outbox is the same
+    srv = pd.Server(1 << 30, max_slots=2, dt=0.005, skin=0.3, autotune=False, tx=5)
+    x, v, L = _sys(3000, 90)
+    t = srv.submit(x, v, L, 5)
+    with pytest.raises(pd.PdError):
+        srv.result(t)
+    with pytest.raises(pd.PdError):
+        srv.release(t)
+    srv.run_until_done([t])
+    x1, E1, _ = srv.result(t)
+    x2, E2, _ = srv.result(t)
+    assert np.array_equal(x1, x2) and np.array_equal(E1, E2)
+    srv.release(t)
+    with pytest.raises(pd.PdError):
+        srv.release(t)
