@@ -164,6 +164,14 @@ unsigned long long pd_launch_count(void);
  * the bytes held.  No counterpart in the reference package (its device memory
  * comes from a dependency's allocator). */
 int pd_empty_cache(void);
+/* Halo selection of a slab decomposition (one sub-domain per rank): of the n
+ * positions x [n][3] (double, device memory), the ascending indices i with
+ * x[i][axis] < lo_thr (to the lower neighbour) and with x[i][axis] >= hi_thr (to
+ * the upper one), written to idx_lo / idx_hi (device or host, room for n each),
+ * their counts to *n_lo / *n_hi.  The reference selects the particles of each
+ * neighbouring sub-domain's ghost box (vector_dist_comm.hpp:1398-1596). */
+int pd_slab_halo(const double* x, long n, int axis, double lo_thr, double hi_thr, int* idx_lo, int* idx_hi,
+                 long* n_lo, long* n_hi, void* stream);
 int pd_set_cache_limit(long bytes, long* held);
 int pd_device_info(int* sm_count, long* free_bytes, long* total_bytes);
 

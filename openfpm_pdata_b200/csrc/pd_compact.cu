@@ -16,6 +16,8 @@
 // get_indexes_by_type<prp, functor>: flag p < end whose property satisfies the
 // comparison (mark_indexes :414-423), scan, and write p at its scan offset
 // (fill_indexes :425-438): the indexes come out ascending.
+#include <mutex>
+
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
 
@@ -85,6 +87,16 @@ __global__ void k_fill_indexes(const unsigned int* __restrict__ flag, const unsi
 }
 
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// halo flags of a slab: x[i][axis] below the lower threshold, at or above the upper
+__global__ void k_slab_mark(const double* __restrict__ x, long n, int axis, double lo_thr, double hi_thr,
+                            unsigned int* __restrict__ f0, unsigned int* __restrict__ f1) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double a = x[3 * i + axis];
+        f0[i] = a < lo_thr ? 1u : 0u;
+        f1[i] = a >= hi_thr ? 1u : 0u;
+    }
+}
 
 }  // namespace pd
 
@@ -202,6 +214,49 @@ int pd_get_indexes_by_type(pd_vd h, int prop, int cmp, long long value, long end
         PD_CUDA(cudaMemcpyAsync(ids, out, sizeof(unsigned int) * m, cudaMemcpyDefault, st));
         PD_CUDA(cudaStreamSynchronize(st));
     }
+    return PD_OK;
+}
+
+int pd_slab_halo(const double* x, long n, int axis, double lo_thr, double hi_thr, int* idx_lo, int* idx_hi,
+                 long* n_lo, long* n_hi, void* stream) {
+    if (!x || n < 0 || axis < 0 || axis > 2 || !n_lo || !n_hi) return PD_EINVAL;
+    *n_lo = 0;
+    *n_hi = 0;
+    if (n == 0) return PD_OK;
+    if (n >= (1L << 31)) return PD_EINVAL;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, x) != cudaSuccess ||
+        (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+        cudaGetLastError();
+        set_error("pd_slab_halo: positions must be in device memory");
+        return PD_EINVAL;
+    }
+    cudaStream_t st = S(stream);
+    // scratch of the calls (one at a time): flags, offsets, index lists, totals
+    static std::mutex mu;
+    static Buf work, scratch;
+    std::lock_guard<std::mutex> lk(mu);
+    PD_TRY(work.ensure(sizeof(unsigned int) * (6 * (size_t)n + 2)));
+    unsigned int* f0 = work.as<unsigned int>();
+    unsigned int *f1 = f0 + n, *o0 = f1 + n, *o1 = o0 + n, *l0 = o1 + n, *l1 = l0 + n, *tot = l1 + n;
+    const unsigned g = grid_for(n, 256);
+    pd::launch(k_slab_mark, g, 256, 0, st, x, n, axis, lo_thr, hi_thr, f0, f1);
+    PD_LAUNCH_CHECK();
+    PD_TRY(scan_u32(f0, o0, n, tot, scratch, st));
+    PD_TRY(scan_u32(f1, o1, n, tot + 1, scratch, st));
+    pd::launch(k_fill_indexes, g, 256, 0, st, (const unsigned int*)f0, (const unsigned int*)o0, n, l0);
+    pd::launch(k_fill_indexes, g, 256, 0, st, (const unsigned int*)f1, (const unsigned int*)o1, n, l1);
+    PD_LAUNCH_CHECK();
+    unsigned int m[2] = {0, 0};
+    PD_CUDA(cudaMemcpyAsync(m, tot, sizeof(m), cudaMemcpyDeviceToHost, st));
+    PD_CUDA(cudaStreamSynchronize(st));
+    *n_lo = m[0];
+    *n_hi = m[1];
+    if ((m[0] && !idx_lo) || (m[1] && !idx_hi)) return PD_EINVAL;
+    // the lists may go to device or host memory (unified addressing)
+    if (m[0]) PD_CUDA(cudaMemcpyAsync(idx_lo, l0, sizeof(int) * m[0], cudaMemcpyDefault, st));
+    if (m[1]) PD_CUDA(cudaMemcpyAsync(idx_hi, l1, sizeof(int) * m[1], cudaMemcpyDefault, st));
+    PD_CUDA(cudaStreamSynchronize(st));
     return PD_OK;
 }
 

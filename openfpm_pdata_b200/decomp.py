@@ -76,6 +76,11 @@ class SlabDecomposition:
         if self.P == 1:
             return []
         a = self.axis
+        lo_thr, hi_thr = self.edges[rank] + self.g, self.edges[rank + 1] - self.g
+        native = None
+        if x.is_cuda and x.dtype == torch.float64:
+            from . import pd  # the library's selection kernel (same comparisons, ascending indices)
+            native = pd.slab_halo(x, a, lo_thr, hi_thr)
         out = []
         for side in (+1, -1):
             dest, shift = rank + side, 0.0
@@ -84,10 +89,10 @@ class SlabDecomposition:
                     continue
                 dest = dest % self.P
                 shift = -self.L if side > 0 else self.L
-            if side > 0:
-                sel = x[:, a] >= self.edges[rank + 1] - self.g
-            else:
-                sel = x[:, a] < self.edges[rank] + self.g
+            if native is not None:
+                out.append((dest, native[1] if side > 0 else native[0], shift))
+                continue
+            sel = x[:, a] >= hi_thr if side > 0 else x[:, a] < lo_thr
             out.append((dest, torch.nonzero(sel).flatten(), shift))
         return out
 

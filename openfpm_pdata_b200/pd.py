@@ -144,6 +144,8 @@ def lib():
             "pd_md_timers": ([vp, P(ctypes.c_double), P(ctypes.c_long)], ip),
             "pd_launch_count": ([], ctypes.c_ulonglong),
             "pd_empty_cache": ([], ip),
+            "pd_slab_halo": ([vp, lp, ip, ctypes.c_double, ctypes.c_double, vp, vp, P(ctypes.c_long),
+                              P(ctypes.c_long), vp], ip),
             "pd_set_cache_limit": ([lp, P(ctypes.c_long)], ip),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
@@ -209,6 +211,23 @@ def launch_count():
 def empty_cache():
     """Return the device blocks the library keeps for reuse to the driver."""
     check(lib().pd_empty_cache())
+
+
+def slab_halo(x, axis, lo_thr, hi_thr):
+    """Halo selection of a slab on a CUDA tensor of positions [n, 3] (float64):
+    (ascending indices with x[:, axis] < lo_thr, those with x[:, axis] >= hi_thr)
+    as int64 CUDA tensors, computed by the library."""
+    import torch
+    x = x.contiguous()
+    _check_tensor(x, np.float64)
+    n = x.shape[0]
+    lo = torch.empty(max(n, 1), dtype=torch.int32, device=x.device)
+    hi = torch.empty(max(n, 1), dtype=torch.int32, device=x.device)
+    a, b = ctypes.c_long(0), ctypes.c_long(0)
+    check(lib().pd_slab_halo(ctypes.c_void_p(x.data_ptr()), int(n), int(axis), float(lo_thr), float(hi_thr),
+                             ctypes.c_void_p(lo.data_ptr()), ctypes.c_void_p(hi.data_ptr()), ctypes.byref(a),
+                             ctypes.byref(b), None))
+    return lo[: a.value].to(torch.int64), hi[: b.value].to(torch.int64)
 
 
 def set_cache_limit(limit_bytes=-1):

@@ -93,3 +93,29 @@ def test_library_reads_and_writes_cuda_tensors():
     xl, _ = dp.map(xt)
     f1 = lj_forces_distributed(dp, xl)
     assert f1.is_cuda and np.array_equal(f1.cpu().numpy(), fh)
+
+
+def test_slab_halo_kernel_equals_masks():
+    """The library's halo selection (pd_slab_halo) gives the indices of the
+    tensor masks, in the same ascending order, for every rank of 2 and 3 slabs;
+    positions in host memory are refused before any kernel runs."""
+    import torch
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200 import pd
+    from openfpm_pdata_b200.decomp import SlabDecomposition
+    rng = np.random.default_rng(4)
+    L = 30.0
+    x = rng.uniform(0, L, size=(200000, 3))
+    xc, xg = torch.from_numpy(x), torch.from_numpy(x).cuda()
+    for P in (2, 3):
+        dec = SlabDecomposition(np.zeros(3), np.full(3, L), (1, 1, 1), 2.5, P, axis=1)
+        for r in range(P):
+            host = dec.halo_sends(r, xc)
+            dev = dec.halo_sends(r, xg)
+            assert [(d, s) for d, _, s in host] == [(d, s) for d, _, s in dev]
+            for (_, ih, _), (_, idv, _) in zip(host, dev):
+                assert idv.is_cuda and torch.equal(ih, idv.cpu())
+    n0, n1 = pd.ctypes.c_long(0), pd.ctypes.c_long(0)
+    rc = pd.lib().pd_slab_halo(x.ctypes.data_as(pd.ctypes.c_void_p), x.shape[0], 0, 1.0, 2.0, None, None,
+                               pd.ctypes.byref(n0), pd.ctypes.byref(n1), None)
+    assert rc == -1  # PD_EINVAL
