@@ -220,3 +220,28 @@ def test_single_rank_is_the_whole_box():
     assert xh.shape[0] == 0
     lo, hi, bc = dec.local_box(0)
     assert np.array_equal(bc, [1, 1, 1]) and hi[0] == L
+
+
+def test_rows_pack_every_property_type_exactly():
+    # positions and properties of any of the packed types and shapes travel as
+    # float64 rows and come back bit for bit; other types are refused
+    import torch
+    sys.path.insert(0, ROOT)
+    from openfpm_pdata_b200.decomp import _pack, _unpack
+    rng = np.random.default_rng(3)
+    n = 257
+    x = torch.from_numpy(rng.normal(size=(n, 3)))
+    props = [torch.from_numpy(rng.normal(size=n).astype(np.float32)),
+             torch.from_numpy(rng.integers(-2 ** 31, 2 ** 31 - 1, size=(n, 2), dtype=np.int64).astype(np.int32)),
+             torch.from_numpy(rng.normal(size=(n, 3, 3))),
+             torch.zeros((n, 0), dtype=torch.float64)]
+    rows, meta = _pack(x, props)
+    assert rows.dtype == torch.float64 and rows.shape == (n, 3 + 1 + 2 + 9 + 0)
+    x2, p2 = _unpack(rows, meta)
+    assert torch.equal(x2, x)
+    for a, b in zip(props, p2):
+        assert a.dtype == b.dtype and a.shape == b.shape and torch.equal(a, b)
+    x0, p0 = _unpack(_pack(x[:0], [p[:0] for p in props])[0], meta)
+    assert x0.shape == (0, 3) and [p.shape[0] for p in p0] == [0, 0, 0, 0]
+    with pytest.raises(TypeError):
+        _pack(x, [torch.zeros(n, dtype=torch.int64)])
