@@ -59,6 +59,14 @@ def test_bad_arguments_rejected_without_gpu():
     assert L.pd_srv_submit(None, ctypes.c_long(10), ctypes.c_double(10.0), None, None, 5, ctypes.byref(t)) == -1
     assert L.pd_srv_result(None, ctypes.c_long(0), None, None, None) == -1
     assert L.pd_srv_release(None, ctypes.c_long(0)) == -1
+    # the slab halo selection refuses positions that are not in device memory
+    import numpy as np
+    x = np.zeros((4, 3))
+    a, b = ctypes.c_long(0), ctypes.c_long(0)
+    assert L.pd_slab_halo(x.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(4), 0, ctypes.c_double(1.0),
+                          ctypes.c_double(2.0), None, None, ctypes.byref(a), ctypes.byref(b), None) == -1
+    assert L.pd_slab_halo(None, ctypes.c_long(4), 0, ctypes.c_double(1.0), ctypes.c_double(2.0), None, None,
+                          ctypes.byref(a), ctypes.byref(b), None) == -1
 
 
 def test_package_fails_loudly_without_library(tmp_path, monkeypatch):
