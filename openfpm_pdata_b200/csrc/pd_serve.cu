@@ -967,9 +967,9 @@ struct SrvReq {
 
 // Copies of the submitted arrays into pinned memory: one core copies at about
 // 6 GB/s, so a submission of a megabyte or more is cut into pieces of at least
-// 512 KB that the caller and up to three workers copy.  The workers start at
-// the first such submission and live as long as the server; if they cannot be
-// started the caller copies everything.
+// 512 KB that the caller and up to three workers (no more than the cores beside
+// the caller's) copy.  The workers start at the first such submission and live
+// as long as the server; if they cannot be started the caller copies everything.
 struct CopyJob {
     char* dst;
     const char* src;
@@ -1026,7 +1026,9 @@ struct CopyPool {
         if (!tried) {
             tried = true;
             try {
-                for (int k = 0; k < 3; ++k) workers.emplace_back([this] { worker(); });
+                const unsigned hw = std::thread::hardware_concurrency();
+                const int nw = hw == 0 ? 3 : (int)std::min(3u, hw > 1 ? hw - 1 : 0u);
+                for (int k = 0; k < nw; ++k) workers.emplace_back([this] { worker(); });
             } catch (const std::system_error&) {
             }
         }
