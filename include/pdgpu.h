@@ -286,7 +286,8 @@ int pd_celllist_destroy(pd_cl cl);
  * counting sort (stable), and with PD_CL_GPU_REORDER a coalesced reorder of the
  * positions / the properties in prop_mask into cell order. */
 int pd_celllist_update(pd_vd h, pd_cl cl, unsigned long prop_mask, void* stream);
-/* restoreOrder<prp...>(cl) -- vector_dist.hpp:3042-3049 */
+/* restoreOrder<prp...>(cl) -- vector_dist.hpp:3042-3049: positions, the properties
+ * in prop_mask and every property the update reordered return to the original order */
 int pd_restore_order(pd_vd h, pd_cl cl, unsigned long prop_mask, void* stream);
 int pd_celllist_view(pd_cl cl, pd_cl_view_t* out);
 /* download: cell_start[ncells+1], sorted_ids[n] (NULL to skip either) */
@@ -297,9 +298,9 @@ int pd_celllist_get(pd_cl cl, int* cell_start, int* sorted_ids, void* stream);
 int pd_test_force(pd_vd h, pd_cl cl, int in_prop, int out_prop, int sorted, void* stream);
 
 /* No counterpart in the reference.  The counting sort of pd_celllist_update for
- * callers that cannot allocate device memory: code that runs while a CUDA graph
- * is being captured, hosts whose device memory belongs to their own pool, and
- * callers that must not let cudaMalloc/cudaFree synchronise the device.  It
+ * callers that cannot allocate device memory: plugins in hosts whose device
+ * memory belongs to the host's own pool, and callers that must not let
+ * cudaMalloc/cudaFree synchronise the device under running work.  It
  * calls no allocator; its only scratch is a fixed static device array (about
  * 8.4 MB, held on every GPU that loads the library until exit).  Inputs and
  * outputs are caller-owned device buffers: pos_xyz [n][3] in dtype, cell_start
@@ -308,9 +309,16 @@ int pd_test_force(pd_vd h, pd_cl cl, int in_prop, int out_prop, int sorted, void
  * padding layers).  Limits: n <= 524288 particles and gs0*gs1*gs2 <= 524288
  * cells, else PD_EINVAL.  The first call on each device looks up the scratch
  * address (cudaGetSymbolAddress) and should come before any stream capture.
- * All calls share the scratch: calls that overlap on the GPU race. */
+ * All calls share the scratch: calls that overlap on the GPU race.  The three
+ * buffers must be device memory of the current device (else PD_EINVAL, before
+ * any launch).  A NaN or out-of-grid position is clamped into a border cell, as
+ * pd_celllist_update does (which reports it as PD_EOVERFLOW); here the optional
+ * device word `status` (NULL to skip) is cleared and then receives
+ * PD_STATIC_OUT_OF_GRID, readable once the stream's work is done. */
+#define PD_STATIC_OUT_OF_GRID 1u
 int pd_celllist_build_static(int dtype, const void* pos_xyz, long n, const double* box_lo, const double* spacing,
-                             const int* gs, int pad, int* cell_start, int* sorted_ids, void* stream);
+                             const int* gs, int pad, int* cell_start, int* sorted_ids, unsigned int* status,
+                             void* stream);
 
 /* ---- Verlet list -------------------------------------------------------- */
 /* getVerlet(r_cut) -- vector_dist.hpp:1514-1547: full list of every domain particle

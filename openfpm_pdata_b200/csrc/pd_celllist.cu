@@ -97,36 +97,15 @@ __global__ void k_cl_scatter(long n_bound, const unsigned int* __restrict__ n_de
         out[start[cell_of[i]] + slot[i]] = (int)i;
 }
 
-// 4. stabilise: one warp per cell, rank of each member = number of smaller indices
-__global__ void k_cl_stabilise(long ncells, const unsigned int* __restrict__ start, const int* __restrict__ in,
-                               int* __restrict__ out) {
+// 4. stabilise: one warp per cell puts its members in ascending index order
+__global__ void __launch_bounds__(256) k_cl_stabilise(long ncells, const unsigned int* __restrict__ start,
+                                                      const int* __restrict__ in, int* __restrict__ out) {
+    __shared__ int cell_sort_buf[256 / 32][CELL_SORT_SMEM];
     long warp = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-    int lane = threadIdx.x & 31;
     for (long c = warp; c < ncells; c += nwarps) {
-        unsigned int s = start[c], e = start[c + 1];
-        unsigned int n = e - s;
-        if (n == 0) continue;
-        if (n == 1) {
-            if (lane == 0) out[s] = in[s];
-            continue;
-        }
-        if (n <= 32) {
-            int v = lane < (int)n ? in[s + lane] : 0x7fffffff;
-            unsigned int rank = 0;
-            for (int j = 0; j < (int)n; ++j) {
-                int o = __shfl_sync(0xffffffffu, v, j);
-                rank += (o < v) ? 1u : 0u;
-            }
-            if (lane < (int)n) out[s + rank] = v;
-        } else {
-            for (unsigned int a = lane; a < n; a += 32) {
-                int v = in[s + a];
-                unsigned int rank = 0;
-                for (unsigned int j = 0; j < n; ++j) rank += (in[s + j] < v) ? 1u : 0u;
-                out[s + rank] = v;
-            }
-        }
+        const unsigned int s = start[c], e = start[c + 1];
+        warp_cell_order(in + s, out + s, e - s, cell_sort_buf[threadIdx.x >> 5]);
     }
 }
 
@@ -387,8 +366,13 @@ int pd_restore_order(pd_vd h, pd_cl cl, unsigned long prop_mask, void* stream) {
     }
     cudaStream_t st = S(stream);
     bool wp = (cl->opt & PD_CL_GPU_REORDER_POSITION) != 0;
-    PD_TRY(permute(h, cl->sorted.as<int>(), cl->n_part, prop_mask, wp, true, true, st));
+    // the listed properties (written in cell order) and every property the update
+    // reordered return to the original order: the reference swaps its original
+    // arrays back, so a reordered property that is not listed keeps its original
+    // order (vector_dist.hpp:3042-3049)
+    PD_TRY(permute(h, cl->sorted.as<int>(), cl->n_part, prop_mask | cl->reordered_mask, wp, true, true, st));
     cl->reordered = false;
+    cl->reordered_mask = 0;
     return PD_OK;
 }
 

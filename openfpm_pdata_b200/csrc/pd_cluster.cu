@@ -29,6 +29,7 @@ namespace pd {
 static constexpr int CL_CTAS = 16;       // CTAs of the cluster (non-portable size; 8 where 16 cannot be placed)
 static constexpr int CL_THREADS = 1024;  // threads per CTA
 static constexpr long CL_MAXN = 65536;   // real particles handled by the cluster path
+static constexpr unsigned int CL_SORT_CAP = 256;  // shared ints per warp for ordering a crowded cell
 
 template <class T> struct ClArgs {
     typename V4<T>::type* pos;  // real [0, n), images [n, n + img_cap)
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_md_cluster(ClArgs<T> A) {
     cg::cluster_group cluster = cg::this_cluster();
     __shared__ BoxSet<T> B;
     __shared__ unsigned int wsum[32];
+    __shared__ int cell_sort_buf[32][CL_SORT_CAP];  // per warp: in-cell ordering of crowded cells
     for (int i = threadIdx.x; i < (int)(sizeof(BoxSet<T>) / 4); i += blockDim.x)
         reinterpret_cast<int*>(&B)[i] = reinterpret_cast<const int*>(A.boxes)[i];
     __syncthreads();
@@ -207,32 +209,19 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_md_cluster(ClArgs<T> A) {
         // 7. scatter to the unordered slot
         for (long k = gt; k < nt; k += GT) A.sorted_tmp[A.cstart[A.cell_of[k]] + A.slot[k]] = (int)k;
         cluster.sync();
-        // 8. in-cell order by index (one warp per cell)
+        // 8. in-cell order by index (one warp per cell), then the cell-ordered position copy
         {
             const long warp = gt >> 5, nw = GT >> 5;
             const int lane = threadIdx.x & 31;
             for (long c = warp; c < A.ncells; c += nw) {
                 const unsigned int b0 = A.cstart[c], e0 = A.cstart[c + 1], cn = e0 - b0;
-                if (cn <= 32) {
-                    const int v = lane < (int)cn ? A.sorted_tmp[b0 + lane] : 0x7fffffff;
-                    unsigned int rk = 0;
-                    for (int j = 0; j < (int)cn; ++j) rk += (__shfl_sync(0xffffffffu, v, j) < v) ? 1u : 0u;
-                    if (lane < (int)cn) {
-                        A.sorted[b0 + rk] = v;
-                        T4 r = ldc4(A.pos, v);
-                        r.w = idx_bits<T>(v);
-                        st4(A.pcs, b0 + rk, r);
-                    }
-                } else {
-                    for (unsigned int a = lane; a < cn; a += 32) {
-                        const int v = A.sorted_tmp[b0 + a];
-                        unsigned int rk = 0;
-                        for (unsigned int j = 0; j < cn; ++j) rk += (A.sorted_tmp[b0 + j] < v) ? 1u : 0u;
-                        A.sorted[b0 + rk] = v;
-                        T4 r = ldc4(A.pos, v);
-                        r.w = idx_bits<T>(v);
-                        st4(A.pcs, b0 + rk, r);
-                    }
+                warp_cell_order(A.sorted_tmp + b0, A.sorted + b0, cn, cell_sort_buf[threadIdx.x >> 5], CL_SORT_CAP);
+                __syncwarp();
+                for (unsigned int a = lane; a < cn; a += 32) {
+                    const int v = A.sorted[b0 + a];
+                    T4 r = ldc4(A.pos, v);
+                    r.w = idx_bits<T>(v);
+                    st4(A.pcs, b0 + a, r);
                 }
             }
         }

@@ -224,18 +224,18 @@ int pd_slab_halo(const double* x, long n, int axis, double lo_thr, double hi_thr
     *n_hi = 0;
     if (n == 0) return PD_OK;
     if (n >= (1L << 31)) return PD_EINVAL;
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, x) != cudaSuccess ||
-        (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
-        cudaGetLastError();
-        set_error("pd_slab_halo: positions must be in device memory");
-        return PD_EINVAL;
-    }
+    PD_TRY(check_device_ptr(x, "pd_slab_halo", "the positions"));
+    int dev = 0;
+    PD_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return PD_EINVAL;
     cudaStream_t st = S(stream);
-    // scratch of the calls (one at a time): flags, offsets, index lists, totals
+    // scratch of the calls on each device (one call at a time): flags, offsets,
+    // index lists, totals
     static std::mutex mu;
-    static Buf work, scratch;
+    static Buf work_dev[64], scratch_dev[64];
     std::lock_guard<std::mutex> lk(mu);
+    Buf& work = work_dev[dev];
+    Buf& scratch = scratch_dev[dev];
     PD_TRY(work.ensure(sizeof(unsigned int) * (6 * (size_t)n + 2)));
     unsigned int* f0 = work.as<unsigned int>();
     unsigned int *f1 = f0 + n, *o0 = f1 + n, *o1 = o0 + n, *l0 = o1 + n, *l1 = l0 + n, *tot = l1 + n;

@@ -31,6 +31,25 @@ void set_error(const char* fmt, ...) {
     g_err = buf;
 }
 
+int check_device_ptr(const void* p, const char* who, const char* what) {
+    int dev = -1;
+    cudaPointerAttributes at;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("%s: %s is not a pointer the CUDA runtime knows", who, what);
+        return PD_EINVAL;
+    }
+    if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) {
+        set_error("%s: %s must be device memory, not host memory", who, what);
+        return PD_EINVAL;
+    }
+    if (at.type == cudaMemoryTypeDevice && at.device != dev) {
+        set_error("%s: %s is memory of device %d, the current device is %d", who, what, at.device, dev);
+        return PD_EINVAL;
+    }
+    return PD_OK;
+}
+
 thread_local AllocCtx* g_alloc_ctx = nullptr;
 
 // Device allocations of the library.  Inside an AllocScope (the serving loop) they

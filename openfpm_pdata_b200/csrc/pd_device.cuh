@@ -82,6 +82,62 @@ __device__ __forceinline__ unsigned int warp_agg_inc(unsigned int* counter, unsi
     return base + __popc(lower);
 }
 
+// Stable order of one cell after the atomic-slot scatter: one warp writes the n
+// distinct indices in[0..n) to out[0..n) in ascending order.  n <= 32: each lane's
+// rank from shuffles; n <= cap: bitonic sort in `wbuf` (the warp's `cap` ints of
+// shared memory, a power of two); larger: each member's rank counted against
+// 32-wide chunks of the cell broadcast through shuffles.
+static constexpr unsigned int CELL_SORT_SMEM = 512;
+__device__ __forceinline__ void warp_cell_order(const int* __restrict__ in, int* __restrict__ out, unsigned int n,
+                                                int* wbuf, unsigned int cap = CELL_SORT_SMEM) {
+    const int lane = threadIdx.x & 31;
+    if (n == 0) return;
+    if (n == 1) {
+        if (lane == 0) out[0] = in[0];
+        return;
+    }
+    if (n <= 32) {
+        const int v = lane < (int)n ? in[lane] : 0x7fffffff;
+        unsigned int rank = 0;
+        for (int j = 0; j < (int)n; ++j) rank += (__shfl_sync(0xffffffffu, v, j) < v) ? 1u : 0u;
+        if (lane < (int)n) out[rank] = v;
+        return;
+    }
+    if (n <= cap) {
+        unsigned int P = 64;
+        while (P < n) P <<= 1;
+        for (unsigned int i = lane; i < P; i += 32) wbuf[i] = i < n ? in[i] : 0x7fffffff;
+        __syncwarp();
+        for (unsigned int k = 2; k <= P; k <<= 1)
+            for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+                for (unsigned int i = lane; i < P; i += 32) {
+                    const unsigned int o = i ^ j;
+                    if (o > i) {
+                        const int a = wbuf[i], b = wbuf[o];
+                        if ((a > b) == ((i & k) == 0)) {
+                            wbuf[i] = b;
+                            wbuf[o] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        for (unsigned int i = lane; i < n; i += 32) out[i] = wbuf[i];
+        __syncwarp();
+        return;
+    }
+    for (unsigned int a0 = 0; a0 < n; a0 += 32) {
+        const int v = a0 + lane < n ? in[a0 + lane] : 0x7fffffff;
+        unsigned int rank = 0;
+        for (unsigned int j0 = 0; j0 < n; j0 += 32) {
+            const int w = j0 + lane < n ? in[j0 + lane] : 0x7fffffff;
+            const int m = (int)min(32u, n - j0);
+            for (int j = 0; j < m; ++j) rank += (__shfl_sync(0xffffffffu, w, j) < v) ? 1u : 0u;
+        }
+        if (a0 + lane < n) out[rank] = v;
+    }
+}
+
 template <class T> __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -14,6 +14,9 @@
 namespace pd {
 
 void set_error(const char* fmt, ...);
+// PD_OK when p is device (or managed) memory of the current device; else PD_EINVAL
+// with a message naming `who` and `what`.  Neither allocates nor synchronises.
+int check_device_ptr(const void* p, const char* who, const char* what);
 
 #define PD_CUDA(call)                                                                                   \
     do {                                                                                                \
@@ -169,6 +172,7 @@ struct pd_cl_s {
     bool reordered = false;  // the vector holds cell-ordered data until restore_order
     unsigned long reordered_mask = 0;
     long epoch = -1;
+    double mq = 0;  // quantum of the precision form's offsets on this grid (mixed_set_quantum; 0: unset)
 };
 
 struct pd_vl_s {

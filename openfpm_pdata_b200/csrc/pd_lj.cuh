@@ -8,7 +8,25 @@ namespace pd {
 
 template <class T> struct LJP {
     T eps24, eps4, sig2, rc2;
+    // precision form only: squared distances in [rc2lo, rc2hi) lie within the FP32
+    // rounding of r2 from the cutoff and are decided again in FP64 against rc2d;
+    // pairs below rclose2 are evaluated in FP64 with the *d parameters
+    T rc2lo, rc2hi, rclose2;
+    double rc2d, eps24d, eps4d, sig2d;
 };
+
+// Cutoff decision of the precision form.  dx, dy, dz are exact (the offsets lie on
+// the quantum grid, see pd_mixed.cu), so r2 = fma(dz,dz, fma(dy,dy, dx*dx)) in FP32
+// carries only its own three roundings; outside the band it decides like FP64.  In
+// the band the same formula in FP64 (the FP32 products are exact there) decides.
+__device__ __forceinline__ bool in_cut_exact(float r2, float dx, float dy, float dz, const LJP<float>& P) {
+    bool in = r2 < P.rc2lo;
+    if (r2 >= P.rc2lo && r2 < P.rc2hi) {
+        const double x = dx, y = dy, z = dz;
+        in = fma(z, z, fma(y, y, x * x)) < P.rc2d;
+    }
+    return in;
+}
 
 // Reciprocal by Newton-Raphson refinement (Newton's method for f(y) = 1/y - x,
 // y' = y (2 - x y), written as e = 1 - x y, y' = y + y e; each step doubles the

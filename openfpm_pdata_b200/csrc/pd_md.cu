@@ -827,6 +827,7 @@ int pd_md_create(pd_vd h, const pd_lj_params_t* lj, const pd_md_params_t* mp, pd
         delete md;
         return r;
     }
+    if (md->mixed) mixed_set_quantum(md->vl->cl, mp->skin);
     md->nblk = force_blocks(h->n_real);
     if ((r = md->fpart.ensure(sizeof(double) * 2 * md->nblk)) != PD_OK ||
         (r = md->kpart.ensure(sizeof(double) * md->nblk)) != PD_OK ||
@@ -970,7 +971,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         PD_EV(0);
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
         if (fused && s > 0 && md->mixed) {
-            PD_TRY(mixed_kick_kick_drift(h, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+            PD_TRY(mixed_kick_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
                                          md->mp.dt, md->mp.mass, md->kpart.as<double>(), st));
             PD_TRY(md_energy(md, s - 1, st));
         } else if (fused && s > 0) {
@@ -988,7 +989,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             PD_TRY(sph_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
                                   md->mp.dt, st));
         else if (md->mixed)
-            PD_TRY(mixed_kick_drift(h, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+            PD_TRY(mixed_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
                                     md->mp.dt, st));
         else if (h->dtype == PD_F64)
             pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,

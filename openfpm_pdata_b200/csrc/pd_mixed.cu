@@ -8,7 +8,15 @@
 //   v, f   : FP32 properties of the vector.
 // A pair displacement is formed from the offsets and the cell difference
 // (dx = (o_i - o_j) + (c_i - c_j) * s), so its rounding error is set by the
-// offset magnitude (<= 1.5 s), not by the box size.  In a tile, staged records
+// offset magnitude (<= 1.5 s), not by the box size.  Offsets are kept on a grid
+// of quantum q = 2^e with every value of the pair loop below 2^24 q
+// (mixed_set_quantum): differences and cell shifts of grid values are then exact in
+// FP32, so a pair displacement equals the FP64 displacement of the represented
+// positions exactly, and r2 carries only its own roundings.  The cutoff is
+// decided in FP64 for the few pairs within that rounding of it (in_cut_exact).
+// Centres use the cell side rounded to the grid; an image offset is its source's
+// offset plus a constant of the rebuild, exact when the box length is a multiple
+// of q (else rounded to the grid once).  In a tile, staged records
 // are rewritten once in shared memory: y and z are shifted by the row's cell
 // difference to the tile's centre row (|.| <= 2.5 s) and w holds the record's
 // cell column in the tile, so the pair loop forms
@@ -23,6 +31,9 @@
 #include "pd_mixed_dev.cuh"
 #include "pd_tile.cuh"
 
+#include <algorithm>
+#include <cmath>
+
 namespace pd {
 
 // positions -> offsets from the cell centre (all n particles)
@@ -34,7 +45,7 @@ __global__ void k_x64_to_off(const double4* __restrict__ pos, long n, Grid<doubl
         unsigned int c = (unsigned int)G.cell(r.x, r.y, r.z, bad);
         double cx, cy, cz;
         C.centre(c, cx, cy, cz);
-        off[k] = make_float4((float)(r.x - cx), (float)(r.y - cy), (float)(r.z - cz), __uint_as_float(c));
+        off[k] = make_float4(C.qd(r.x - cx), C.qd(r.y - cy), C.qd(r.z - cz), __uint_as_float(c));
     }
     if (bad) atomicOr(err, ERR_CELL_RANGE);
 }
@@ -74,8 +85,8 @@ __global__ void k_image_k(const double4* __restrict__ pos, const float4* __restr
         double ci[3], cs[3];
         C.centre(__float_as_uint(off[n_real + k].w), ci[0], ci[1], ci[2]);
         C.centre(__float_as_uint(off[s].w), cs[0], cs[1], cs[2]);
-        K[k] = make_float4((float)((xi.x - ci[0]) - (xs.x - cs[0])), (float)((xi.y - ci[1]) - (xs.y - cs[1])),
-                           (float)((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
+        K[k] = make_float4(C.qd((xi.x - ci[0]) - (xs.x - cs[0])), C.qd((xi.y - ci[1]) - (xs.y - cs[1])),
+                           C.qd((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
     }
 }
 
@@ -94,7 +105,7 @@ __global__ void k_replay32(float4* __restrict__ off, long n_real, long m, const 
 // v += h f ; o += dt v ; largest |o - o_build|^2
 __global__ void __launch_bounds__(256) k_kick_drift32(float4* __restrict__ off, const float4* __restrict__ ob,
                                                       float* __restrict__ v, const float* __restrict__ f, long cap,
-                                                      long n, float half, float dt,
+                                                      long n, float half, float dt, CellGeom C,
                                                       unsigned long long* __restrict__ maxd2) {
     double mx = 0;
     for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
@@ -102,9 +113,9 @@ __global__ void __launch_bounds__(256) k_kick_drift32(float4* __restrict__ off, 
         float vx = v[i] + half * f[i];
         float vy = v[cap + i] + half * f[cap + i];
         float vz = v[2 * cap + i] + half * f[2 * cap + i];
-        o.x += dt * vx;
-        o.y += dt * vy;
-        o.z += dt * vz;
+        o.x = C.qf(o.x + dt * vx);
+        o.y = C.qf(o.y + dt * vy);
+        o.z = C.qf(o.z + dt * vz);
         v[i] = vx;
         v[cap + i] = vy;
         v[2 * cap + i] = vz;
@@ -122,7 +133,7 @@ __global__ void __launch_bounds__(256) k_kick_drift32(float4* __restrict__ off, 
 __global__ void __launch_bounds__(256) k_kick_kick_drift32(float4* __restrict__ off, const float4* __restrict__ ob,
                                                            float* __restrict__ v, const float* __restrict__ f,
                                                            long cap, long n, float half, float dt, double mass,
-                                                           unsigned long long* __restrict__ maxd2,
+                                                           CellGeom C, unsigned long long* __restrict__ maxd2,
                                                            double* __restrict__ part) {
     double mx = 0, ke = 0;
     for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
@@ -135,9 +146,9 @@ __global__ void __launch_bounds__(256) k_kick_kick_drift32(float4* __restrict__ 
         vy = vy + half * fy;
         vz = vz + half * fz;
         float4 o = off[i];
-        o.x += dt * vx;
-        o.y += dt * vy;
-        o.z += dt * vz;
+        o.x = C.qf(o.x + dt * vx);
+        o.y = C.qf(o.y + dt * vy);
+        o.z = C.qf(o.z + dt * vz);
         v[i] = vx;
         v[cap + i] = vy;
         v[2 * cap + i] = vz;
@@ -196,11 +207,23 @@ __global__ void __launch_bounds__(FBLOCK_T, 5) k_vtile_lj_mixed(const float4* __
 }
 
 // ---------------------------------------------------------------------------
-static CellGeom cell_geom(pd_cl cl) {
+double mixed_set_quantum(pd_cl cl, double skin) {
+    double s = 0;
+    for (int d = 0; d < 3; ++d) s = std::max(s, cl->spacing[d]);
+    int e = 0;
+    std::frexp(2.0 * s + (skin > 0 ? skin : 0.0), &e);  // 2^e > 2 s + skin
+    cl->mq = std::ldexp(1.0, e - 24);
+    return cl->mq;
+}
+
+CellGeom mixed_cell_geom(pd_cl cl) {
+    if (!(cl->mq > 0)) mixed_set_quantum(cl, 0.5 * cl->spacing[0]);  // a skin of half a cell bounds any list
     CellGeom C;
+    C.q = cl->mq;
+    C.iq = 1.0 / cl->mq;
     for (int d = 0; d < 3; ++d) {
         C.lo[d] = cl->box_lo[d];
-        C.sp[d] = cl->spacing[d];
+        C.sp[d] = std::rint(cl->spacing[d] * C.iq) * C.q;  // the cell side on the grid
         C.gs[d] = cl->gs[d];
     }
     C.pad = cl->pad;
@@ -218,7 +241,7 @@ int mixed_from_positions(pd_vd h, pd_cl cl, Buf& off, Buf& K, cudaStream_t st) {
         G.gs[d] = cl->gs[d];
     }
     G.pad = cl->pad;
-    CellGeom C = cell_geom(cl);
+    CellGeom C = mixed_cell_geom(cl);
     if (nt > 0)
         pd::launch(k_x64_to_off, grid_for(nt, 256), 256, 0, st, (const double4*)h->pos, nt, G, C, off.as<float4>(),
                    &h->ctrl->err);
@@ -232,7 +255,7 @@ int mixed_from_positions(pd_vd h, pd_cl cl, Buf& off, Buf& K, cudaStream_t st) {
 int mixed_to_positions(pd_vd h, pd_cl cl, const Buf& off, cudaStream_t st) {
     long n = h->n_real;
     if (n > 0)
-        pd::launch(k_off_to_x64, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n, cell_geom(cl),
+        pd::launch(k_off_to_x64, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n, mixed_cell_geom(cl),
                    (double4*)h->pos);
     PD_LAUNCH_CHECK();
     return PD_OK;
@@ -242,7 +265,7 @@ int mixed_to_positions_by_id(pd_vd h, pd_cl cl, const Buf& off, double* out, cud
     long n = h->n_real;
     if (n > 0)
         pd::launch(k_off_to_x64_by_id, grid_for(n, 256), 256, 0, st, (const float4*)off.as<float4>(), n,
-                   cell_geom(cl), (const int*)h->gid, out);
+                   mixed_cell_geom(cl), (const int*)h->gid, out);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
@@ -256,22 +279,23 @@ int mixed_replay(pd_vd h, Buf& off, const Buf& K, cudaStream_t st) {
     return PD_OK;
 }
 
-int mixed_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
-                     double dt, cudaStream_t st) {
+int mixed_kick_drift(pd_vd h, pd_cl cl, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk,
+                     double half, double dt, cudaStream_t st) {
     Prop& V = h->props[vel_prop];
     Prop& F = h->props[force_prop];
     pd::launch(k_kick_drift32, nblk, 256, 0, st, off.as<float4>(), (const float4*)ob.as<float4>(), (float*)V.d,
-               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, &h->ctrl->maxdisp2);
+               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, mixed_cell_geom(cl), &h->ctrl->maxdisp2);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
 
-int mixed_kick_kick_drift(pd_vd h, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk, double half,
-                          double dt, double mass, double* kpart, cudaStream_t st) {
+int mixed_kick_kick_drift(pd_vd h, pd_cl cl, Buf& off, const Buf& ob, int vel_prop, int force_prop, int nblk,
+                          double half, double dt, double mass, double* kpart, cudaStream_t st) {
     Prop& V = h->props[vel_prop];
     Prop& F = h->props[force_prop];
     pd::launch(k_kick_kick_drift32, nblk, 256, 0, st, off.as<float4>(), (const float4*)ob.as<float4>(), (float*)V.d,
-               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, mass, &h->ctrl->maxdisp2, kpart);
+               (const float*)F.d, h->cap, h->n_real, (float)half, (float)dt, mass, mixed_cell_geom(cl),
+               &h->ctrl->maxdisp2, kpart);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
@@ -300,6 +324,19 @@ static int launch_mixed(pd_vd h, const TileGeom& tg, long ntiles, const unsigned
     return PD_OK;
 }
 
+void mixed_cutoff(const pd_lj_params_t& lj, LJP<float>& P) {
+    const float rc = (float)lj.r_cut;
+    P.rc2 = rc * rc;
+    P.rc2d = lj.r_cut * lj.r_cut;
+    // |r2_f32 - r2| <= 3 u r2 (u = 2^-24) for exact dx, dy, dz: a band of 16 u r2 on each side
+    P.rc2lo = (float)(P.rc2d * (1.0 - std::ldexp(1.0, -20)));
+    P.rc2hi = (float)(P.rc2d * (1.0 + std::ldexp(1.0, -20)));
+    P.rclose2 = (float)(0.95 * 0.95 * lj.sigma * lj.sigma);
+    P.eps24d = 24.0 * lj.eps;
+    P.eps4d = 4.0 * lj.eps;
+    P.sig2d = lj.sigma * lj.sigma;
+}
+
 int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
              unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj,
              int force_prop, double* part, int P, cudaStream_t st) {
@@ -307,10 +344,10 @@ int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned 
     LP.eps24 = (float)(24.0 * lj.eps);
     LP.eps4 = (float)(4.0 * lj.eps);
     LP.sig2 = (float)(lj.sigma * lj.sigma);
-    float rc = (float)lj.r_cut;
-    LP.rc2 = rc * rc;
+    mixed_cutoff(lj, LP);
     float* f = (float*)h->props[force_prop].d;
-    float sx = (float)cl->spacing[0], sy = (float)cl->spacing[1], sz = (float)cl->spacing[2];
+    const CellGeom C = mixed_cell_geom(cl);
+    const float sx = (float)C.sp[0], sy = (float)C.sp[1], sz = (float)C.sp[2];  // exact: multiples of q
     if (P == 1) return launch_mixed<1>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
     if (P == 4) return launch_mixed<4>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
     return launch_mixed<2>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);

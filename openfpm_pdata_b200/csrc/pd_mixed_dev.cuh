@@ -17,10 +17,19 @@ struct TileShM {
     unsigned int segb[18][TXMAX + 3];
 };
 
-// cell centres of the grid
+// Cell centres of the precision form and the quantum of its offsets.  Centres are
+// lo + (i - pad + 1/2) * sp with sp the cell side rounded to a multiple of the
+// quantum q (a power of two, mixed_set_quantum in pd_mixed.cu); every offset is a
+// multiple of q below 2^24 q in magnitude, so the FP32 differences and the cell
+// shifts of the pair loop are exact (FP32 holds every multiple of q in that range).
 struct CellGeom {
     double lo[3], sp[3];
     int gs[3], pad;
+    double q, iq;  // quantum and its reciprocal (powers of two)
+    // an FP64 offset rounded to the nearest multiple of q (exact in FP32)
+    __device__ __forceinline__ float qd(double o) const { return (float)(rint(o * iq) * q); }
+    // an FP32 value rounded to the nearest multiple of q (scalings by powers of two are exact)
+    __device__ __forceinline__ float qf(float o) const { return rintf(o * (float)iq) * (float)q; }
     __device__ __forceinline__ void centre(unsigned int c, double& cx, double& cy, double& cz) const {
         int i0 = (int)(c % (unsigned)gs[0]);
         int i1 = (int)((c / (unsigned)gs[0]) % (unsigned)gs[1]);
@@ -30,6 +39,18 @@ struct CellGeom {
         cz = lo[2] + ((double)(i2 - pad) + 0.5) * sp[2];
     }
 };
+
+// host: the centres and quantum of the precision form on the grid of `cl`
+CellGeom mixed_cell_geom(pd_cl cl);
+// host: the cutoff of the precision form (FP32 threshold and FP64 re-decision band)
+void mixed_cutoff(const pd_lj_params_t& lj, LJP<float>& P);
+
+// Pairs closer than Pr.rclose2 (0.95 sigma: the repulsive wall, where a relative
+// rounding error of r2 grows about sevenfold in the force) are evaluated in FP64
+// from the exact FP32 displacement: up to MIXED_KDEF per thread and round of a
+// tile (more such contacts than that within one thread's share of a row stay in
+// FP32).
+static constexpr int MIXED_KDEF = 8;
 
 struct Kahan {
     float s, c;
@@ -143,6 +164,8 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
         }
         __syncthreads();
         const unsigned int base = S.oR[4] - S.cR[4][0];
+        // staged indices of the pairs a thread sets aside for FP64, column per thread
+        __shared__ unsigned short defer[MIXED_KDEF][FBLOCK_T];
         // rounds of the whole CTA over the tile's particles: P lanes per row while a
         // round is full, more lanes per row (up to a warp) in the last, partial round;
         // every thread takes part in every round (the shuffles need whole warps)
@@ -160,6 +183,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
             const float4 xi = sm[li];
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             Kahan kx = {0.f, 0.f}, ky = {0.f, 0.f}, kz = {0.f, 0.f}, ke = {0.f, 0.f}, kw = {0.f, 0.f};
+            int nd = 0;  // wall pairs set aside in defer[][threadIdx.x]
             const unsigned int* row = nbr + i;
             // row words read four iterations ahead (register shift ring) to cover the memory latency
             unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
@@ -181,16 +205,21 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                     const float dx = fmaf(xi.w - xq.w, sx, xi.x - xq.x);
                     const float dy = xi.y - xq.y, dz = xi.z - xq.z;
                     const float r2 = dist2(dx, dy, dz);
-                    // every pair through the same instructions; pairs outside select zero
-                    const bool in = r2 < Pr.rc2 && l != li;
-                    const float ir2 = recip(in ? r2 : 1.f);
+                    // every pair through the same instructions; pairs outside select zero;
+                    // pairs within FP32 rounding of the cutoff decided in FP64; pairs on the
+                    // repulsive wall set aside for FP64 (while this thread's list has room)
+                    const bool in = in_cut_exact(r2, dx, dy, dz, Pr) && l != li;
+                    const bool wall = in && r2 < Pr.rclose2 && nd < MIXED_KDEF;
+                    if (wall) defer[nd++][threadIdx.x] = (unsigned short)l;
+                    const bool in32 = in && !wall;
+                    const float ir2 = recip(in32 ? r2 : 1.f);
                     const float s2 = Pr.sig2 * ir2;
                     const float s6 = s2 * s2 * s2;
-                    const float ff = in ? Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f) : 0.f;
+                    const float ff = in32 ? Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f) : 0.f;
                     fx += ff * dx;
                     fy += ff * dy;
                     fz += ff * dz;
-                    e += in ? Pr.eps4 * s6 * (s6 - 1.f) : 0.f;
+                    e += in32 ? Pr.eps4 * s6 * (s6 - 1.f) : 0.f;
                     w += ff * r2;
                 }
                 kx.add(fx);
@@ -200,6 +229,23 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                 kw.add(w);
             }
             double Fx = kx.value(), Fy = ky.value(), Fz = kz.value(), Ee = ke.value(), Ww = kw.value();
+            // the set-aside wall pairs in FP64: the displacement is exact in FP32, so it
+            // converts exactly; r2 and the pair terms then carry FP64 rounding only
+            for (int k = 0; k < nd; ++k) {
+                const float4 xq = sm[defer[k][threadIdx.x]];
+                const double dx = fmaf(xi.w - xq.w, sx, xi.x - xq.x);
+                const double dy = xi.y - xq.y, dz = xi.z - xq.z;
+                const double r2 = dist2(dx, dy, dz);
+                const double ir2 = recip(r2);
+                const double s2 = Pr.sig2d * ir2;
+                const double s6 = s2 * s2 * s2;
+                const double ff = Pr.eps24d * ir2 * s6 * (2.0 * s6 - 1.0);
+                Fx += ff * dx;
+                Fy += ff * dy;
+                Fz += ff * dz;
+                Ee += Pr.eps4d * s6 * (s6 - 1.0);
+                Ww += ff * r2;
+            }
             for (unsigned int o = 1; o < q; o <<= 1) {
                 Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
                 Fy += __shfl_xor_sync(0xffffffffu, Fy, o);

@@ -1,12 +1,12 @@
 // pd_noalloc.cu -- cell-list counting sort that allocates no device memory.
 //
 // pd_celllist_update grows its scratch buffers with cudaMalloc on demand.  Some
-// callers cannot allow that: code running while a CUDA graph is being
-// captured (cudaMalloc is not capturable), real-time or plugin hosts whose
-// device memory is owned by a pool of the host application, and callers that
-// must not synchronise the device (cudaMalloc/cudaFree may).  For them this
-// entry point sorts particles into cells using a file-scope __device__ array
-// as its only scratch; the caller passes inputs and outputs.
+// callers cannot allow that: real-time or plugin hosts whose device memory is
+// owned by a pool of the host application (the plugin gets a budget, not the
+// allocator), and callers that must not let cudaMalloc/cudaFree synchronise the
+// device under running work.  For them this entry point sorts particles into
+// cells using a file-scope __device__ array as its only scratch; the caller
+// passes inputs and outputs.
 //
 // The scratch array is part of the library's device image: every GPU that
 // loads the library holds it (about 8.4 MB) until the process exits.  Its
@@ -15,7 +15,12 @@
 // should therefore come before any stream capture.  All calls share the one
 // array and it keeps the last call's contents (the counts are cleared on every
 // call), so calls that overlap on the GPU -- on different streams, or from
-// different host threads -- race and must be serialised by the caller.
+// different host threads -- race and must be serialised by the caller.  A
+// position that is NaN or outside the grid is clamped into a border cell, as in
+// pd_celllist_update; the optional caller-owned device word `status` is cleared
+// and then receives PD_STATIC_OUT_OF_GRID for such a call (read it after the
+// stream's work: nothing here synchronises).  Pointers are checked to be device
+// memory of the current device before any launch.
 #include <mutex>
 
 #include "pd_device.cuh"
@@ -69,7 +74,8 @@ __global__ void k_zero(unsigned int* a, long n) {
 
 template <class T>
 __global__ void k_hash_xyz(const T* __restrict__ xyz, long n, Grid<T> G, unsigned int* __restrict__ cnt,
-                           unsigned int* __restrict__ cell_of, unsigned int* __restrict__ slot) {
+                           unsigned int* __restrict__ cell_of, unsigned int* __restrict__ slot,
+                           unsigned int* __restrict__ status) {
     unsigned int bad = 0;
     for (long base = blockIdx.x * (long)blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         long i = base + threadIdx.x;
@@ -81,6 +87,7 @@ __global__ void k_hash_xyz(const T* __restrict__ xyz, long n, Grid<T> G, unsigne
             slot[i] = warp_agg_inc(cnt, c, act);
         }
     }
+    if (bad && status) atomicOr(status, PD_STATIC_OUT_OF_GRID);
 }
 
 // scan of m counts: per-block totals, exclusive scan of the totals in one block, apply
@@ -149,27 +156,22 @@ __global__ void k_scatter(long n, const unsigned int* __restrict__ cell_of, cons
         tmp[start[cell_of[i]] + slot[i]] = (unsigned int)i;
 }
 
-// one warp per cell: rank members by index (stable in-cell order)
-__global__ void k_stabilise(long ncells, const int* __restrict__ start, const unsigned int* __restrict__ in,
-                            int* __restrict__ out) {
+// one warp per cell: members in ascending index order (stable in-cell order)
+__global__ void __launch_bounds__(BLOCK) k_stabilise(long ncells, const int* __restrict__ start,
+                                                     const unsigned int* __restrict__ in, int* __restrict__ out) {
+    __shared__ int cell_sort_buf[BLOCK / 32][CELL_SORT_SMEM];
     long warp = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
     long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-    int lane = threadIdx.x & 31;
     for (long c = warp; c < ncells; c += nwarps) {
-        int s = start[c], e = start[c + 1];
-        int n = e - s;
-        for (int a = lane; a < n; a += 32) {
-            unsigned int v = in[s + a];
-            int rank = 0;
-            for (int j = 0; j < n; ++j) rank += in[s + j] < v ? 1 : 0;
-            out[s + rank] = (int)v;
-        }
+        const int s = start[c], e = start[c + 1];
+        warp_cell_order(reinterpret_cast<const int*>(in) + s, out + s, (unsigned int)(e - s),
+                        cell_sort_buf[threadIdx.x >> 5]);
     }
 }
 
 template <class T>
 static int run(const void* pos_xyz, long n, const double* box_lo, const double* spacing, const int* gs, int pad,
-               int* cell_start, int* sorted_ids, cudaStream_t st) {
+               int* cell_start, int* sorted_ids, unsigned int* status, cudaStream_t st) {
     unsigned int* S = nullptr;
     PD_TRY(scratch_address(&S));
     long ncells = (long)gs[0] * gs[1] * gs[2];
@@ -188,9 +190,10 @@ static int run(const void* pos_xyz, long n, const double* box_lo, const double* 
     long m = ncells + 1;
     long nb = (m + TILE - 1) / TILE;
     pd::launch(k_zero, grid_for(m, BLOCK), BLOCK, 0, st, cnt, m);
+    if (status) pd::launch(k_zero, 1, 32, 0, st, status, 1L);
     if (n > 0)
         pd::launch(k_hash_xyz<T>, grid_for(n, BLOCK), BLOCK, 0, st, static_cast<const T*>(pos_xyz), n, G, cnt,
-                   cell_of, slot);
+                   cell_of, slot, status);
     pd::launch(k_block_tot, (unsigned)nb, BLOCK, 0, st, (const unsigned int*)cnt, m, parts);
     pd::launch(k_tot_scan, 1, 32, 0, st, parts, nb);
     pd::launch(k_apply, (unsigned)nb, BLOCK, 0, st, (const unsigned int*)cnt, m, (const unsigned int*)parts,
@@ -213,7 +216,8 @@ using namespace pd;
 extern "C" {
 
 int pd_celllist_build_static(int dtype, const void* pos_xyz, long n, const double* box_lo, const double* spacing,
-                             const int* gs, int pad, int* cell_start, int* sorted_ids, void* stream) {
+                             const int* gs, int pad, int* cell_start, int* sorted_ids, unsigned int* status,
+                             void* stream) {
     if ((dtype != PD_F32 && dtype != PD_F64) || n < 0 || !box_lo || !spacing || !gs || !cell_start ||
         (n > 0 && (!pos_xyz || !sorted_ids)) || pad < 0) {
         set_error("pd_celllist_build_static: invalid argument");
@@ -231,10 +235,18 @@ int pd_celllist_build_static(int dtype, const void* pos_xyz, long n, const doubl
                   n, ncells, noalloc::MAX_PART, noalloc::MAX_CELLS);
         return PD_EINVAL;
     }
+    // device memory of the current device only: a host pointer would reach the kernels
+    static const char* who = "pd_celllist_build_static";
+    PD_TRY(check_device_ptr(cell_start, who, "cell_start"));
+    if (n > 0) {
+        PD_TRY(check_device_ptr(pos_xyz, who, "pos_xyz"));
+        PD_TRY(check_device_ptr(sorted_ids, who, "sorted_ids"));
+    }
+    if (status) PD_TRY(check_device_ptr(status, who, "status"));
     cudaStream_t st = S(stream);
     if (dtype == PD_F64)
-        return noalloc::run<double>(pos_xyz, n, box_lo, spacing, gs, pad, cell_start, sorted_ids, st);
-    return noalloc::run<float>(pos_xyz, n, box_lo, spacing, gs, pad, cell_start, sorted_ids, st);
+        return noalloc::run<double>(pos_xyz, n, box_lo, spacing, gs, pad, cell_start, sorted_ids, status, st);
+    return noalloc::run<float>(pos_xyz, n, box_lo, spacing, gs, pad, cell_start, sorted_ids, status, st);
 }
 
 }  // extern "C"

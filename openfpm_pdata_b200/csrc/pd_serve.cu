@@ -262,9 +262,9 @@ __global__ void __launch_bounds__(CHUNK) k_b_kick_drift(const SysDesc* __restric
             float vx = d.v[i] + half * d.f[i];
             float vy = d.v[cap + i] + half * d.f[cap + i];
             float vz = d.v[2 * cap + i] + half * d.f[2 * cap + i];
-            o.x += dt * vx;
-            o.y += dt * vy;
-            o.z += dt * vz;
+            o.x = d.C.qf(o.x + dt * vx);
+            o.y = d.C.qf(o.y + dt * vy);
+            o.z = d.C.qf(o.z + dt * vz);
             d.v[i] = vx;
             d.v[cap + i] = vy;
             d.v[2 * cap + i] = vz;
@@ -590,36 +590,18 @@ __global__ void __launch_bounds__(CHUNK) k_rb_scatter(const SysDesc* __restrict_
     RB_END
 }
 
-// stable order inside every cell: one warp per cell ranks its members by index
+// stable order inside every cell: one warp per cell orders its members by index
 template <int IMG>
 __global__ void __launch_bounds__(CHUNK) k_rb_stabilise(const SysDesc* __restrict__ D, const RbWork* __restrict__ W) {
+    __shared__ int cell_sort_buf[CHUNK / 32][CELL_SORT_SMEM];
     RB_LOOP(K_W)
     const long cell = c * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
     if (cell < d.ncell) {
         const unsigned int* start = IMG ? d.csI : d.csR;
         const int* in = d.sorted_tmp;
         int* out = d.sorted;
         const unsigned int s0 = start[cell], e0 = start[cell + 1];
-        const unsigned int n = e0 - s0;
-        if (n == 1) {
-            if (lane == 0) out[s0] = in[s0];
-        } else if (n > 1 && n <= 32) {
-            int v = lane < (int)n ? in[s0 + lane] : 0x7fffffff;
-            unsigned int rk = 0;
-            for (int j = 0; j < (int)n; ++j) {
-                int o = __shfl_sync(0xffffffffu, v, j);
-                rk += (o < v) ? 1u : 0u;
-            }
-            if (lane < (int)n) out[s0 + rk] = v;
-        } else if (n > 32) {
-            for (unsigned int a = lane; a < n; a += 32) {
-                int v = in[s0 + a];
-                unsigned int rk = 0;
-                for (unsigned int j = 0; j < n; ++j) rk += (in[s0 + j] < v) ? 1u : 0u;
-                out[s0 + rk] = v;
-            }
-        }
+        warp_cell_order(in + s0, out + s0, e0 - s0, cell_sort_buf[threadIdx.x >> 5]);
     }
     RB_END
 }
@@ -766,7 +748,7 @@ __global__ void __launch_bounds__(CHUNK) k_rb_offsets(const SysDesc* __restrict_
         unsigned int cc = (unsigned int)d.G.cell(r.x, r.y, r.z, bad);
         double cx, cy, cz;
         d.C.centre(cc, cx, cy, cz);
-        d.off[k] = make_float4((float)(r.x - cx), (float)(r.y - cy), (float)(r.z - cz), __uint_as_float(cc));
+        d.off[k] = make_float4(d.C.qd(r.x - cx), d.C.qd(r.y - cy), d.C.qd(r.z - cz), __uint_as_float(cc));
     }
     if (bad) atomicOr(d.err, ERR_CELL_RANGE);
     RB_END
@@ -786,8 +768,8 @@ __global__ void __launch_bounds__(CHUNK) k_rb_image_k(const SysDesc* __restrict_
         double ci[3], cs[3];
         d.C.centre(__float_as_uint(d.off[n + m].w), ci[0], ci[1], ci[2]);
         d.C.centre(__float_as_uint(d.off[s].w), cs[0], cs[1], cs[2]);
-        d.offK[m] = make_float4((float)((xi.x - ci[0]) - (xs.x - cs[0])), (float)((xi.y - ci[1]) - (xs.y - cs[1])),
-                                (float)((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
+        d.offK[m] = make_float4(d.C.qd((xi.x - ci[0]) - (xs.x - cs[0])), d.C.qd((xi.y - ci[1]) - (xs.y - cs[1])),
+                                d.C.qd((xi.z - ci[2]) - (xs.z - cs[2])), 0.f);
     }
     RB_END
 }
@@ -1151,12 +1133,9 @@ static void fill_desc(pd_srv s, SrvReq* r, SysDesc& d) {
         d.G.lo[k] = cl->box_lo[k];
         d.G.sp[k] = cl->spacing[k];
         d.G.gs[k] = cl->gs[k];
-        d.C.lo[k] = cl->box_lo[k];
-        d.C.sp[k] = cl->spacing[k];
-        d.C.gs[k] = cl->gs[k];
     }
     d.G.pad = cl->pad;
-    d.C.pad = cl->pad;
+    d.C = mixed_cell_geom(cl);
     d.L = r->L;
     d.tg = md->tg;
     d.csR = md->csR.as<unsigned int>();
@@ -1165,9 +1144,9 @@ static void fill_desc(pd_srv s, SrvReq* r, SysDesc& d) {
     d.nn = md->tnn.as<int>();
     d.tstride = md->tstride;
     d.max_nn = md->tmax_nn;
-    d.sx = (float)cl->spacing[0];
-    d.sy = (float)cl->spacing[1];
-    d.sz = (float)cl->spacing[2];
+    d.sx = (float)d.C.sp[0];  // exact: multiples of the quantum
+    d.sy = (float)d.C.sp[1];
+    d.sz = (float)d.C.sp[2];
     const double rl = md->vl->r_cut;
     const double band = fp32_band(h, rl);
     d.lo_thr = (float)(rl * rl - band);
@@ -1253,8 +1232,7 @@ static int capture_graph(pd_srv s, int lk) {
     P.eps24 = (float)(24.0 * s->lj.eps);
     P.eps4 = (float)(4.0 * s->lj.eps);
     P.sig2 = (float)(s->lj.sigma * s->lj.sigma);
-    float rc = (float)s->lj.r_cut;
-    P.rc2 = rc * rc;
+    mixed_cutoff(s->lj, P);
     PD_CUDA(cudaFuncSetAttribute(k_b_force, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
     PD_CUDA(cudaFuncSetAttribute(k_rb_build<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BSMEM));
     PD_CUDA(cudaFuncSetAttribute(k_b_force_ovf, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
@@ -1384,6 +1362,7 @@ static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
         PD_CUDA(cudaMemsetAsync(h->ctrl, 0, sizeof(Ctrl), s->as));
         memset(h->ctrl_h, 0, sizeof(Ctrl));
         PD_TRY(cl_geometry(md->vl->cl, h, rl, 1.013, 1));
+        mixed_set_quantum(md->vl->cl, s->skin);
         md->ready = false;
         md->steps = 0;
         md->builds = 0;

@@ -148,7 +148,7 @@ def lib():
                               P(ctypes.c_long), vp], ip),
             "pd_set_cache_limit": ([lp, P(ctypes.c_long)], ip),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
-            "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp], ip),
+            "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
             "pd_sph_create": ([vp, P(SPHParams), P(MDParams), P(vp)], ip),
             "pd_srv_create": ([lp, ip, P(LJParams), ctypes.c_double, ctypes.c_double, P(vp)], ip),

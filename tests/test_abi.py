@@ -67,6 +67,16 @@ def test_bad_arguments_rejected_without_gpu():
                           ctypes.c_double(2.0), None, None, ctypes.byref(a), ctypes.byref(b), None) == -1
     assert L.pd_slab_halo(None, ctypes.c_long(4), 0, ctypes.c_double(1.0), ctypes.c_double(2.0), None, None,
                           ctypes.byref(a), ctypes.byref(b), None) == -1
+    # the no-allocation cell-list build refuses host buffers before any launch
+    cs = np.zeros(1001, np.int32)
+    so = np.zeros(4, np.int32)
+    box_lo = (ctypes.c_double * 3)(0, 0, 0)
+    sp = (ctypes.c_double * 3)(0.1, 0.1, 0.1)
+    gs = (ctypes.c_int * 3)(10, 10, 10)
+    assert L.pd_celllist_build_static(pd.PD_F64, x.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(4), box_lo, sp,
+                                      gs, 1, cs.ctypes.data_as(ctypes.c_void_p), so.ctypes.data_as(ctypes.c_void_p),
+                                      None, None) == -1
+    assert b"pd_celllist_build_static" in L.pd_last_error()
 
 
 def test_package_fails_loudly_without_library(tmp_path, monkeypatch):
