@@ -657,15 +657,18 @@ def main():
 
     value = replica_value(world, n, a.steps, ms)
     # roofline of the dominant kernel (Verlet-list LJ force): algorithmic bytes per launch
-    # = N * (32 B position record + 4 B row length + 4 B * mean row + 24 B force)
+    # = N * (position + 4 B row length + row entries + force): the FP64 tiled kernel stages
+    # 24-byte (x, y) / z copies, 2-byte entries; the precision form 16-byte offsets, FP32 forces
     f_ms, f_cnt = timers["force"]
     f_avg_s = f_ms / max(f_cnt, 1) / 1000.0
     # tiled rows: 2-byte entries, the position record is staged once per tile (counted once);
     # mixed form: 16-byte FP32 offset records and FP32 forces
     if mixed:
         alg_bytes = n * (16 + 4 + 2 * mean_nn + 12)
+    elif a.tiles:
+        alg_bytes = n * (24 + 4 + 2 * mean_nn + 24)
     else:
-        alg_bytes = n * (32 + 4 + (2 if a.tiles else 4) * mean_nn + 24)
+        alg_bytes = n * (32 + 4 + 4 * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
     # secondary roofline of the FP64 pair kernel (its arithmetic, not HBM, is the
@@ -677,7 +680,7 @@ def main():
     in_cut = 4.18879 * R_CUT ** 3 * rho
     flops = n * (8 * mean_nn + 29 * in_cut)
     fma_peak = pd.measure_fma_rate(pd.PD_F32 if mixed else pd.PD_F64)
-    kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_f64" if a.tiles else "k_lj_verlet_f64")
+    kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_xyz" if a.tiles else "k_lj_verlet_f64")
     traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
 
     out = {
@@ -688,7 +691,7 @@ def main():
         "verlet_list": {"rebuilds_in_timed_region": builds, "mean_row": round(mean_nn, 2), "max_row": max_nn},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "kernel": "k_vtile_lj_mixed" if mixed else ("k_vtile_lj<double>" if a.tiles else
+                     "kernel": "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_xyz (FP64)" if a.tiles else
                                                                   "k_lj_verlet<double>"),
                      "peak_kind": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": f_avg_s * 1000.0,

@@ -413,6 +413,48 @@ int pd_srv_completed(pd_srv s, long* tickets, int cap, int* n);
    batched step graphs (launch to completion), retirement */
 int pd_srv_timers(pd_srv s, double ms[4]);
 
+/* ---- slab decomposition over ranks (one sub-domain per rank) -------------
+ * The reference decomposes the box into sub-domains (Decomposition/
+ * CartDecomposition.hpp), sends every particle to the sub-domain owning it
+ * (map, vector_dist_comm.hpp:1957-2014) and copies to each neighbouring
+ * sub-domain the particles in its ghost (ghost_get, vector_dist_comm.hpp:
+ * 1398-1596), over MPI.  Here a sub-domain is the slab r of `nslabs` along
+ * `axis` (rank r owns [lo + r w, lo + (r + 1) w), w = (hi - lo) / nslabs, the
+ * last slab closed at hi); each rank's vector holds its slab, created with the
+ * split axis NON_PERIODIC (its own periodic images cover the other axes).  The
+ * library labels, packs and unpacks on the device; the caller moves the packed
+ * rows between ranks (an all-to-all of NCCL, MPI, or any transport): rows to
+ * rank d are contiguous, ranks ascending, send_counts[d] of them.  A row is
+ * pd_slab_row_bytes bytes: the position in the vector's type, then the
+ * properties of prop_mask in their own types (int32 stays int32). */
+typedef struct {
+    int axis;      /* split axis 0..2 */
+    int nslabs;    /* slabs = ranks */
+    int periodic;  /* the global box is periodic along the axis */
+    double lo, hi; /* the global box along the axis */
+    double ghost;  /* halo width (<= the slab width) */
+} pd_slab_t;
+/* map, labelling: positions wrapped (the split axis by the global box when
+ * periodic, the other axes by the vector's box), the owner of every real particle
+ * found, the rows grouped by destination rank (ascending index within a rank);
+ * send_counts[nslabs] (host) receives the rows per rank.  Synchronises. */
+int pd_slab_map_label(pd_vd h, const pd_slab_t* s, long* send_counts, void* stream);
+/* ghost_get, labelling for rank `rank`: every real particle and local periodic
+ * image within `ghost` of the slab's lower face goes to the lower neighbour,
+ * within `ghost` of the upper face to the upper one, shifted by the box length
+ * across a periodic face; nothing for one slab.  Synchronises. */
+int pd_slab_halo_label(pd_vd h, const pd_slab_t* s, int rank, long* send_counts, void* stream);
+/* bytes of one packed row for the properties in prop_mask (a multiple of 8) */
+int pd_slab_row_bytes(pd_vd h, unsigned long prop_mask, long* bytes);
+/* the rows of the last labelling into `send` (device memory, room for cap_rows rows) */
+int pd_slab_pack(pd_vd h, unsigned long prop_mask, void* send, long cap_rows, void* stream);
+/* map, unpacking: the vector's particles become the n_recv received rows (ghosts
+ * dropped; ids 0..n_recv-1; properties not in prop_mask zeroed) */
+int pd_slab_map_unpack(pd_vd h, unsigned long prop_mask, const void* recv, long n_recv, void* stream);
+/* ghost_get, unpacking: the n_recv received rows are appended as ghosts after the
+ * vector's local periodic images (id -1); a later ghost_get or map drops them */
+int pd_slab_halo_unpack(pd_vd h, unsigned long prop_mask, const void* recv, long n_recv, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

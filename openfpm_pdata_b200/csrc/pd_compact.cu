@@ -10,8 +10,8 @@
 // particles and the flipped mark (:366-372).
 //
 // The scatter writes all columns of one particle in one thread (a column table
-// passed by value), into one scratch block; one device-to-device copy per column
-// then brings the compacted columns back, so the arrays keep their addresses.
+// passed by value) straight into new storage of the same capacity, which replaces
+// the old; the vector's epoch moves on, so views taken before are stale.
 //
 // get_indexes_by_type<prp, functor>: flag p < end whose property satisfies the
 // comparison (mark_indexes :414-423), scan, and write p at its scan offset
@@ -86,8 +86,6 @@ __global__ void k_fill_indexes(const unsigned int* __restrict__ flag, const unsi
         if (flag[i]) ids[off[i]] = (unsigned int)i;
 }
 
-static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
-
 // halo flags of a slab: x[i][axis] below the lower threshold, at or above the upper
 __global__ void k_slab_mark(const double* __restrict__ x, long n, int axis, double lo_thr, double hi_thr,
                             unsigned int* __restrict__ f0, unsigned int* __restrict__ f1) {
@@ -126,43 +124,65 @@ int pd_remove_marked(pd_vd h, int prop, void* stream) {
     }
     PD_LAUNCH_CHECK();
     PD_TRY(scan_u32(keep, off, n, &h->ctrl->n_keep, h->scan_scratch, st));
-    PD_CUDA(cudaMemcpyAsync(&h->ctrl_h->n_keep, &h->ctrl->n_keep, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-    PD_CUDA(cudaStreamSynchronize(st));
-    const long k = h->ctrl_h->n_keep;
-    if (k == n) return PD_OK;  // nothing marked: the particles stay, the mark stays flipped
-    if (k > 0) {
-        // columns: positions, global ids, every component of every property
-        struct Col {
-            unsigned char* a;
-            int w;
-        };
-        std::vector<Col> cols;
-        cols.push_back({(unsigned char*)h->pos, h->pos_bytes});
-        cols.push_back({(unsigned char*)h->gid, (int)sizeof(int)});
-        for (auto& P : h->props)
-            for (int c = 0; c < P.ncomp; ++c) cols.push_back({(unsigned char*)P.d + (size_t)c * h->cap * P.esize, P.esize});
-        for (size_t c0 = 0; c0 < cols.size(); c0 += CMAXC) {
-            const size_t c1 = std::min(cols.size(), c0 + (size_t)CMAXC);
-            size_t bytes = 0;
-            for (size_t c = c0; c < c1; ++c) bytes += align_up((size_t)k * cols[c].w);
-            PD_TRY(h->tmp.ensure(bytes));
-            ColSet C;
-            memset(&C, 0, sizeof(C));
-            C.nc = (int)(c1 - c0);
-            size_t o = 0;
-            for (size_t c = c0; c < c1; ++c) {
-                C.src[c - c0] = cols[c].a;
-                C.dst[c - c0] = h->tmp.as<unsigned char>() + o;
-                C.wsize[c - c0] = cols[c].w;
-                o += align_up((size_t)k * cols[c].w);
-            }
-            pd::launch(k_compact_scatter, g, 256, 0, st, C, n, (const unsigned int*)keep, (const unsigned int*)off);
-            PD_LAUNCH_CHECK();
-            for (int c = 0; c < C.nc; ++c)
-                PD_CUDA(cudaMemcpyAsync((void*)C.src[c], C.dst[c], (size_t)k * C.wsize[c], cudaMemcpyDeviceToDevice,
-                                        st));
+    // the kept particles go straight into new storage of the same capacity, which
+    // then replaces the old (the reference swaps its compacted vectors in,
+    // vector_dist_cuda_funcs.cuh:405-418); after the first call the storage comes
+    // from the library's block cache.  The scatter needs no count on the host, so
+    // flip, scan and scatter run back to back and the call synchronises once.
+    void* np = nullptr;
+    int* ng = nullptr;
+    std::vector<char*> nprops;
+    PD_TRY(alloc_storage(h, h->cap, &np, &ng, nprops));
+    struct Col {
+        const unsigned char* s;
+        unsigned char* d;
+        int w;
+    };
+    std::vector<Col> cols;
+    cols.push_back({(const unsigned char*)h->pos, (unsigned char*)np, h->pos_bytes});
+    cols.push_back({(const unsigned char*)h->gid, (unsigned char*)ng, (int)sizeof(int)});
+    for (size_t p = 0; p < h->props.size(); ++p) {
+        const Prop& P = h->props[p];
+        for (int c = 0; c < P.ncomp; ++c) {
+            const size_t o = (size_t)c * h->cap * P.esize;
+            cols.push_back({(const unsigned char*)P.d + o, (unsigned char*)nprops[p] + o, P.esize});
         }
     }
+    int rc = PD_OK;
+    for (size_t c0 = 0; c0 < cols.size() && rc == PD_OK; c0 += CMAXC) {
+        const size_t c1 = std::min(cols.size(), c0 + (size_t)CMAXC);
+        ColSet C;
+        memset(&C, 0, sizeof(C));
+        C.nc = (int)(c1 - c0);
+        for (size_t c = c0; c < c1; ++c) {
+            C.src[c - c0] = cols[c].s;
+            C.dst[c - c0] = cols[c].d;
+            C.wsize[c - c0] = cols[c].w;
+        }
+        pd::launch(k_compact_scatter, g, 256, 0, st, C, n, (const unsigned int*)keep, (const unsigned int*)off);
+        if (cudaGetLastError() != cudaSuccess) rc = PD_ECUDA;
+    }
+    if (rc == PD_OK && cudaMemcpyAsync(&h->ctrl_h->n_keep, &h->ctrl->n_keep, sizeof(unsigned int),
+                                       cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        rc = PD_ECUDA;
+    // the old storage returns to the cache only after the scatter has read it
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = PD_ECUDA;
+    if (rc != PD_OK) {
+        free_storage(np, ng, nprops);
+        set_error("remove_marked: the compaction kernels failed");
+        return rc;
+    }
+    const long k = h->ctrl_h->n_keep;
+    if (k == n) {  // nothing marked: the particles stay, the mark stays flipped
+        free_storage(np, ng, nprops);
+        return PD_OK;
+    }
+    std::vector<char*> old;
+    for (auto& P : h->props) old.push_back(P.d);
+    free_storage(h->pos, h->gid, old);
+    h->pos = np;
+    h->gid = ng;
+    for (size_t p = 0; p < h->props.size(); ++p) h->props[p].d = nprops[p];
     h->n_real = h->n_total = k;
     h->n_img = 0;
     h->img_valid = false;

@@ -331,33 +331,44 @@ __global__ void k_iota(int* g, long off, long n) {
 }
 
 // grow every per-particle array to hold `need` particles, keeping [0, n_total)
+int alloc_storage(pd_vd h, long cap, void** pos, int** gid, std::vector<char*>& props) {
+    *pos = nullptr;
+    *gid = nullptr;
+    props.assign(h->props.size(), nullptr);
+    bool ok = dev_alloc(pos, (size_t)cap * h->pos_bytes) == cudaSuccess &&
+              dev_alloc((void**)gid, sizeof(int) * cap) == cudaSuccess;
+    for (size_t p = 0; ok && p < h->props.size(); ++p)
+        ok = dev_alloc((void**)&props[p], (size_t)h->props[p].esize * h->props[p].ncomp * cap) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        free_storage(*pos, *gid, props);
+        *pos = nullptr;
+        *gid = nullptr;
+        set_error("cudaMalloc failed for the storage of %ld particles", cap);
+        return PD_ENOMEM;
+    }
+    return PD_OK;
+}
+
+void free_storage(void* pos, int* gid, const std::vector<char*>& props) {
+    dev_free(pos);
+    dev_free(gid);
+    for (char* p : props) dev_free(p);
+}
+
 int ensure_capacity(pd_vd h, long need, cudaStream_t st) {
     if (need <= h->cap) return PD_OK;
     long ncap = need + need / 4 + 1024;
     void* np = nullptr;
-    PD_CUDA(dev_alloc(&np, (size_t)ncap * h->pos_bytes));
     int* ng = nullptr;
-    if (dev_alloc((void**)&ng, sizeof(int) * ncap) != cudaSuccess) {
-        dev_free(np);
-        cudaGetLastError();
-        set_error("cudaMalloc failed growing to %ld particles", ncap);
-        return PD_ENOMEM;
-    }
+    std::vector<char*> nprops;
+    PD_TRY(alloc_storage(h, ncap, &np, &ng, nprops));
     if (h->pos && h->n_total) {
         PD_CUDA(cudaMemcpyAsync(np, h->pos, (size_t)h->n_total * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
         PD_CUDA(cudaMemcpyAsync(ng, h->gid, sizeof(int) * h->n_total, cudaMemcpyDeviceToDevice, st));
     }
-    std::vector<char*> nprops(h->props.size(), nullptr);
     for (size_t p = 0; p < h->props.size(); ++p) {
         Prop& P = h->props[p];
-        if (dev_alloc((void**)&nprops[p], (size_t)P.esize * P.ncomp * ncap) != cudaSuccess) {
-            cudaGetLastError();
-            for (size_t q = 0; q < p; ++q) dev_free(nprops[q]);
-            dev_free(np);
-            dev_free(ng);
-            set_error("cudaMalloc failed growing property %zu to %ld particles", p, ncap);
-            return PD_ENOMEM;
-        }
         if (P.d && h->n_total)
             for (int c = 0; c < P.ncomp; ++c)
                 PD_CUDA(cudaMemcpyAsync(nprops[p] + (size_t)c * ncap * P.esize, P.d + (size_t)c * h->cap * P.esize,

@@ -154,6 +154,15 @@ struct pd_vd_s {
     pd::Ctrl* ctrl_h = nullptr;  // pinned host mirror
     pd::Buf scan_scratch, tmp, tmp2, red;
     long epoch = 0;
+    // slab decomposition (pd_slab.cu): the rows of the last labelling, in send
+    // order (slot of each row, shift code of each halo row), and the halo
+    // received last (from slot halo_base on, while the epoch is halo_epoch)
+    pd::Buf slab_idx, slab_shift, slab_flag, slab_off, slab_tot;
+    long slab_rows = 0;
+    int slab_kind = 0;  // 0 none, 1 map, 2 halo
+    double slab_L = 0;
+    int slab_axis = 0;
+    long halo_base = 0, halo_epoch = -1;
 };
 
 struct pd_cl_s {
@@ -191,6 +200,10 @@ struct pd_vl_s {
 // internal host API shared between translation units
 namespace pd {
 int ensure_capacity(pd_vd h, long need, cudaStream_t st);
+// storage of `cap` particles in the vector's layout (positions, ids, every property);
+// PD_ENOMEM (nothing held) on failure
+int alloc_storage(pd_vd h, long cap, void** pos, int** gid, std::vector<char*>& props);
+void free_storage(void* pos, int* gid, const std::vector<char*>& props);
 int set_ctrl_n_img(pd_vd h, long n_img, cudaStream_t st);
 int read_ctrl(pd_vd h, cudaStream_t st);
 int cl_geometry(pd_cl cl, pd_vd h, double r_cut, double enlarge, int nn_box);

@@ -211,7 +211,8 @@ template <class T>
 __global__ void __launch_bounds__(FBLOCK) k_kick_drift(typename V4<T>::type* __restrict__ pos,
                                                        const typename V4<T>::type* __restrict__ xb, T* __restrict__ v,
                                                        const T* __restrict__ f, long cap, long n, T half, T dt,
-                                                       unsigned long long* __restrict__ maxd2) {
+                                                       unsigned long long* __restrict__ maxd2, T* __restrict__ sxy,
+                                                       T* __restrict__ sz) {
     double mx = 0;
     for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
         typename V4<T>::type x = ld4(pos, i);
@@ -225,6 +226,11 @@ __global__ void __launch_bounds__(FBLOCK) k_kick_drift(typename V4<T>::type* __r
         v[cap + i] = vy;
         v[2 * cap + i] = vz;
         st4(pos, i, x);
+        if (sxy) {  // the pair kernel's staging copies
+            sxy[2 * i] = x.x;
+            sxy[2 * i + 1] = x.y;
+            sz[i] = x.z;
+        }
         typename V4<T>::type b = ld4(xb, i);
         T dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
         mx = fmax(mx, (double)dist2(dx, dy, dz));
@@ -243,7 +249,8 @@ __global__ void __launch_bounds__(FBLOCK) k_kick_kick_drift(typename V4<T>::type
                                                             T* __restrict__ v, const T* __restrict__ f, long cap, long n,
                                                             T half, T dt, double mass,
                                                             unsigned long long* __restrict__ maxd2,
-                                                            double* __restrict__ part) {
+                                                            double* __restrict__ part, T* __restrict__ sxy,
+                                                            T* __restrict__ sz) {
     double ke = 0, mx = 0;
     for (long i = blockIdx.x * (long)FBLOCK + threadIdx.x; i < n; i += (long)gridDim.x * FBLOCK) {
         const T fx = f[i], fy = f[cap + i], fz = f[2 * cap + i];
@@ -262,6 +269,11 @@ __global__ void __launch_bounds__(FBLOCK) k_kick_kick_drift(typename V4<T>::type
         v[cap + i] = vy;
         v[2 * cap + i] = vz;
         st4(pos, i, x);
+        if (sxy) {  // the pair kernel's staging copies
+            sxy[2 * i] = x.x;
+            sxy[2 * i + 1] = x.y;
+            sz[i] = x.z;
+        }
         typename V4<T>::type b = ld4(xb, i);
         T dx = x.x - b.x, dy = x.y - b.y, dz = x.z - b.z;
         mx = fmax(mx, (double)dist2(dx, dy, dz));
@@ -387,7 +399,7 @@ __global__ void k_energy_idx(const double* __restrict__ fpart, int nbf, const do
 namespace pd {
 
 template <class T> static LJP<T> ljp(const pd_lj_params_t& lj) {
-    LJP<T> P;
+    LJP<T> P{};
     P.eps24 = (T)(24.0 * lj.eps);
     P.eps4 = (T)(4.0 * lj.eps);
     P.sig2 = (T)(lj.sigma * lj.sigma);
@@ -531,6 +543,12 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
 }
 
 // wrap, sort the real particles into cell order, periodic images, neighbour structure
+// the FP64 tiled pair kernel reads (x, y) / z copies of the positions, refreshed by
+// the rebuild, the drift (real particles) and the image replay
+static bool md_split(pd_md md) {
+    return md->physics == 0 && !md->mixed && md->tiles_active && !md->mp.use_cell_list && md->h->dtype == PD_F64;
+}
+
 int md_rebuild(pd_md md, cudaStream_t st) {
     pd_vd h = md->h;
     if (md->mixed && md->off_valid) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));
@@ -568,6 +586,7 @@ int md_rebuild(pd_md md, cudaStream_t st) {
         } else {
             if (!md->tiles_active) PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
             PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
+            if (md_split(md)) PD_TRY(tile_split(h, md->sxy, md->sz, 0, h->n_total, st));
         }
     }
     h->epoch++;
@@ -586,7 +605,7 @@ int md_forces(pd_md md, cudaStream_t st) {
     if (md->tiles_active)
         return tile_lj(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                        md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop, md->tpart.as<double>(), true,
-                       md->tile_p, st);
+                       md->tile_p, md->sxy, md->sz, st);
     return lj_launch(md->h, md->mp.use_cell_list ? nullptr : md->vl, md->mp.use_cell_list ? md->cl : nullptr, md->lj,
                      md->mp.force_prop, md->fpart.as<double>(), md->nblk, st);
 }
@@ -612,7 +631,7 @@ static int md_step_cl(pd_md md, cudaStream_t st, long img_cap) {
     const T half = (T)(0.5 * md->mp.dt / md->mp.mass);
     PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
     pd::launch(k_kick_drift<T>, md->nblk, FBLOCK, 0, st, (T4*)h->pos, md->xb.as<T4>(), (T*)V.d, (const T*)F.d, h->cap,
-               n, half, (T)md->mp.dt, &h->ctrl->maxdisp2);
+               n, half, (T)md->mp.dt, &h->ctrl->maxdisp2, (T*)nullptr, (T*)nullptr);
     PD_LAUNCH_CHECK();
     h->n_total = n;
     h->img_valid = false;
@@ -900,6 +919,8 @@ int pd_md_destroy(pd_md md) {
     md->tnn.release();
     md->tpart.release();
     md->pos32.release();
+    md->sxy.release();
+    md->sz.release();
     md->off.release();
     md->offb.release();
     md->offK.release();
@@ -968,6 +989,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     if (md->timing) PD_CUDA(cudaEventRecord(md->evp[6 * (size_t)s + (k)], st))
     for (int s = 0; s < steps; ++s) {
         unsigned int rebuilt = 0;
+        const bool split = md_split(md);  // the drift also refreshes the pair kernel's staging copies
         PD_EV(0);
         PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
         if (fused && s > 0 && md->mixed) {
@@ -978,11 +1000,13 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             if (h->dtype == PD_F64)
                 pd::launch(k_kick_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos,
                            (const double4*)md->xb.as<double4>(), (double*)V.d, (const double*)F.d, h->cap, n, half,
-                           md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>());
+                           md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), split ? md->sxy.as<double>() : nullptr,
+                           split ? md->sz.as<double>() : nullptr);
             else
                 pd::launch(k_kick_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos,
                            (const float4*)md->xb.as<float4>(), (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
-                           (float)md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>());
+                           (float)md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), (float*)nullptr,
+                           (float*)nullptr);
             PD_LAUNCH_CHECK();
             PD_TRY(md_energy(md, s - 1, st));
         } else if (md->physics == 1)
@@ -994,11 +1018,13 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         else if (h->dtype == PD_F64)
             pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,
                                                               (const double*)F.d, h->cap, n, half, md->mp.dt,
-                                                              &h->ctrl->maxdisp2);
+                                                              &h->ctrl->maxdisp2, split ? md->sxy.as<double>() : nullptr,
+                                                              split ? md->sz.as<double>() : nullptr);
         else
             pd::launch(k_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos, md->xb.as<float4>(), (float*)V.d,
                                                              (const float*)F.d, h->cap, n, (float)half,
-                                                             (float)md->mp.dt, &h->ctrl->maxdisp2);
+                                                             (float)md->mp.dt, &h->ctrl->maxdisp2, (float*)nullptr,
+                                                             (float*)nullptr);
         PD_LAUNCH_CHECK();
         PD_EV(1);
         bool rb = md->mp.skin <= 0 || md->mp.use_cell_list;
@@ -1018,6 +1044,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             PD_TRY(mixed_replay(h, md->off, md->offK, st));
         } else {
             PD_TRY(ghost_replay(h, 0ul, true, nullptr, h->n_img, st));
+            if (split) PD_TRY(tile_split(h, md->sxy, md->sz, h->n_real, h->n_img, st));
         }
         PD_EV(3);
         PD_TRY(md_forces(md, st));

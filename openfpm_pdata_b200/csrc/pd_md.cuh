@@ -26,6 +26,7 @@ struct pd_md_s {
     long tstride = 0;
     int tmax_nn = 0;
     pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
+    pd::Buf sxy, sz;  // FP64 tiled path: the pair kernel's (x, y) / z copies of the positions
     // precision form: FP32 cell-local offsets (all particles), their value at the
     // last build (real particles) and the constant parts of the image offsets
     int physics = 0;  // 0: Lennard-Jones, 1: WCSPH

@@ -340,7 +340,7 @@ void mixed_cutoff(const pd_lj_params_t& lj, LJP<float>& P) {
 int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
              unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj,
              int force_prop, double* part, int P, cudaStream_t st) {
-    LJP<float> LP;
+    LJP<float> LP{};
     LP.eps24 = (float)(24.0 * lj.eps);
     LP.eps4 = (float)(4.0 * lj.eps);
     LP.sig2 = (float)(lj.sigma * lj.sigma);

@@ -1228,7 +1228,7 @@ static constexpr int GRAPH_KERNELS = 32;  // kernel nodes per step of the step g
 // the step graphs: 2^lk velocity-Verlet steps of every active system per launch
 static int capture_graph(pd_srv s, int lk) {
     float half = (float)(0.5 * s->dt / 1.0), dt = (float)s->dt;
-    LJP<float> P;
+    LJP<float> P{};
     P.eps24 = (float)(24.0 * s->lj.eps);
     P.eps4 = (float)(4.0 * s->lj.eps);
     P.sig2 = (float)(s->lj.sigma * s->lj.sigma);

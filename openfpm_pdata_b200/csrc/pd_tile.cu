@@ -227,6 +227,128 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
     }
 }
 
+// The same pair loop on split staging: (x, y) as 16-byte records through the bulk
+// copies and z as 8-byte values loaded by the CTA (their ranges need not start on
+// a 16-byte boundary), 24 bytes a record instead of 32; (x, y) records of
+// consecutive slots fall on all eight 16-byte bank groups.
+template <bool ENERGY, int P, int MINB>
+__global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* __restrict__ xy,
+                                                           const double* __restrict__ zz, long n_real, TileGeom tg,
+                                                           const unsigned int* __restrict__ csR,
+                                                           const unsigned int* __restrict__ csI, unsigned int cap,
+                                                           const unsigned int* __restrict__ nbr,
+                                                           const int* __restrict__ nn, long stride, LJP<double> Pr,
+                                                           double* __restrict__ f, long fcap,
+                                                           double* __restrict__ part, unsigned int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tile_raw[];
+    double2* sxy = reinterpret_cast<double2*>(tile_raw);
+    double* sz = reinterpret_cast<double*>(tile_raw + (size_t)cap * sizeof(double2));
+    __shared__ TileSh S;
+    tile_layout(tg, blockIdx.x, csR, csI, S);
+    const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    double pe = 0, vir = 0;
+    bool staged = ib != ie && tile_stage<float>(reinterpret_cast<const float4*>(xy),
+                                                reinterpret_cast<const float4*>(xy + n_real), S,
+                                                reinterpret_cast<float4*>(sxy), cap, err);
+    if (staged) {
+        const int nc = S.ncol - 1;
+        for (int r = 0; r < 9; ++r) {
+            const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
+            for (unsigned int k = threadIdx.x; k < lr; k += blockDim.x) sz[S.oR[r] + k] = __ldg(zz + S.cR[r][0] + k);
+            for (unsigned int k = threadIdx.x; k < li; k += blockDim.x)
+                sz[S.oI[r] + k] = __ldg(zz + n_real + S.cI[r][0] + k);
+        }
+        __syncthreads();
+        const unsigned int base = S.oR[4] - S.cR[4][0];
+        unsigned int first = ib;
+        while (first < ie) {
+            const unsigned int left = ie - first;
+            unsigned int q = P;
+            while (q < 32u && left * (q << 1) <= (unsigned int)FBLOCK_T) q <<= 1;
+            const unsigned int cnt = min(left, (unsigned int)FBLOCK_T / q);
+            const int sub = (int)(threadIdx.x % q);
+            const bool active = threadIdx.x / q < cnt;
+            const unsigned int i = first + (active ? threadIdx.x / q : 0u);
+            const unsigned int li = base + i;
+            const double2 xyi = sxy[li];
+            const double zi = sz[li];
+            const int words = active ? (nn[i] + 1) >> 1 : 0;
+            const int Q = (int)q;
+            double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
+            const unsigned int* row = nbr + i;
+            unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
+            unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+            unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+            unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
+#pragma unroll 2
+            for (int k = sub; k < words; k += Q) {
+                const unsigned int pair = q0;
+                q0 = q1;
+                q1 = q2;
+                q2 = q3;
+                q3 = k + 4 * Q < words ? __ldg(row + (long)(k + 4 * Q) * stride) : 0u;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
+                    const double2 xyq = sxy[l];
+                    const double dx = xyi.x - xyq.x, dy = xyi.y - xyq.y, dz = zi - sz[l];
+                    const double r2 = dist2(dx, dy, dz);
+                    const bool in = r2 < Pr.rc2 && l != li;
+                    const double ir2 = recip(in ? r2 : 1.0);
+                    const double s2 = Pr.sig2 * ir2;
+                    const double s6 = s2 * s2 * s2;
+                    const double ff = in ? Pr.eps24 * ir2 * s6 * (2.0 * s6 - 1.0) : 0.0;
+                    fx += ff * dx;
+                    fy += ff * dy;
+                    fz += ff * dz;
+                    if (ENERGY) {
+                        e += in ? Pr.eps4 * s6 * (s6 - 1.0) : 0.0;
+                        w += ff * r2;
+                    }
+                }
+            }
+            for (unsigned int o = 1; o < q; o <<= 1) {
+                fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                if (ENERGY) {
+                    e += __shfl_xor_sync(0xffffffffu, e, o);
+                    w += __shfl_xor_sync(0xffffffffu, w, o);
+                }
+            }
+            if (active && sub == 0) {
+                f[i] = fx;
+                f[fcap + i] = fy;
+                f[2 * fcap + i] = fz;
+                if (ENERGY) {
+                    pe += 0.5 * e;
+                    vir += 0.5 * w;
+                }
+            }
+            first += cnt;
+        }
+    }
+    if (ENERGY) {
+        pe = block_sum<double, FBLOCK_T>(pe);
+        vir = block_sum<double, FBLOCK_T>(vir);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = pe;
+            part[2 * blockIdx.x + 1] = vir;
+        }
+    }
+}
+
+// (x, y) and z of the slots [first, first + n) from the 32-byte records
+__global__ void k_split_xyz(const double4* __restrict__ pos, long first, long n, double2* __restrict__ xy,
+                            double* __restrict__ zz) {
+    for (long k = first + blockIdx.x * (long)blockDim.x + threadIdx.x; k < first + n;
+         k += (long)gridDim.x * blockDim.x) {
+        const double4 r = ld4(pos, k);
+        xy[k] = make_double2(r.x, r.y);
+        zz[k] = r.z;
+    }
+}
+
 // tile-local rows -> global particle indices (for checks and downloads)
 __global__ void __launch_bounds__(TBLOCK) k_vtile_translate(long n_real, TileGeom tg,
                                                             const unsigned int* __restrict__ csR,
@@ -389,23 +511,67 @@ int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR
     return PD_EOVERFLOW;
 }
 
-template <class T, bool E, int P>
-static int launch_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
-                       unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<T>& LP, T* f,
-                       double* part, int smem, cudaStream_t st) {
-    PD_TRY(allow_smem(k_vtile_lj<T, E, P>, smem));
-    pd::launch(k_vtile_lj<T, E, P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
-               (const typename V4<T>::type*)h->pos, h->n_real, tg, csR, csI, cap, nbr.as<unsigned int>(),
-               nn.as<int>(), stride, LP, f, h->cap, part, &h->ctrl->err);
+int tile_split(pd_vd h, Buf& sxy, Buf& sz, long first, long n, cudaStream_t st) {
+    const size_t cap = (size_t)(h->cap > 0 ? h->cap : 1);
+    PD_TRY(sxy.ensure(cap * sizeof(double2)));
+    PD_TRY(sz.ensure(cap * sizeof(double)));
+    if (n <= 0) return PD_OK;
+    pd::launch(k_split_xyz, grid_for(n, 256), 256, 0, st, (const double4*)h->pos, first, n, sxy.as<double2>(),
+               sz.as<double>());
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
 
+template <bool E, int P, int MINB>
+static int launch_lj_xyz(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                         unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<double>& LP, double* f,
+                         double* part, const Buf& sxy, const Buf& sz, cudaStream_t st) {
+    if (!sxy.p || !sz.p) {
+        set_error("tile_lj: the FP64 staging copies were not made");
+        return PD_ESTATE;
+    }
+    int smem = (int)(cap * 24);
+    if (smem < 32) smem = 32;
+    PD_TRY(allow_smem(k_vtile_lj_xyz<E, P, MINB>, smem));
+    pd::launch(k_vtile_lj_xyz<E, P, MINB>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
+               (const double2*)sxy.as<double2>(), (const double*)sz.as<double>(), h->n_real, tg, csR, csI, cap,
+               nbr.as<unsigned int>(), nn.as<int>(), stride, LP, f, h->cap, part, &h->ctrl->err);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+// FP32 storage: the 16-byte records
+template <class T, bool E, int P>
+struct LjLaunch {
+    static int run(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                   unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<T>& LP, T* f, double* part,
+                   const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+        (void)sxy;
+        (void)sz;
+        PD_TRY(allow_smem(k_vtile_lj<T, E, P>, smem));
+        pd::launch(k_vtile_lj<T, E, P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
+                   (const typename V4<T>::type*)h->pos, h->n_real, tg, csR, csI, cap, nbr.as<unsigned int>(),
+                   nn.as<int>(), stride, LP, f, h->cap, part, &h->ctrl->err);
+        PD_LAUNCH_CHECK();
+        return PD_OK;
+    }
+};
+// FP64: the split staging (k_vtile_lj_xyz, at most 64 registers: four CTAs per SM)
+template <bool E, int P>
+struct LjLaunch<double, E, P> {
+    static int run(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                   unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<double>& LP, double* f,
+                   double* part, const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+        (void)smem;
+        return launch_lj_xyz<E, P, 4>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, st);
+    }
+};
+
 template <class T>
 static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                      unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, T* f,
-                     double* part, bool energy, int P, int smem, cudaStream_t st) {
-    LJP<T> LP;
+                     double* part, bool energy, int P, const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+    LJP<T> LP{};
     LP.eps24 = (T)(24.0 * lj.eps);
     LP.eps4 = (T)(4.0 * lj.eps);
     LP.sig2 = (T)(lj.sigma * lj.sigma);
@@ -413,7 +579,7 @@ static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned in
     LP.rc2 = rc * rc;
 #define PD_LJ_CASE(E, PP)                                                                                         \
     if (energy == E && P == PP)                                                                                   \
-        return launch_lj_t<T, E, PP>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, smem, st);
+        return LjLaunch<T, E, PP>::run(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, smem, st);
     PD_LJ_CASE(true, 1)
     PD_LJ_CASE(true, 2)
     PD_LJ_CASE(true, 4)
@@ -427,15 +593,15 @@ static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned in
 
 int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
             unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
-            double* part, bool energy, int P, cudaStream_t st) {
+            double* part, bool energy, int P, const Buf& sxy, const Buf& sz, cudaStream_t st) {
     Prop& F = h->props[force_prop];
     int smem = (int)(cap * h->pos_bytes);
     if (smem < 16) smem = 16;
     if (h->dtype == PD_F64)
         return tile_lj_t<double>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (double*)F.d, part, energy, P,
-                                 smem, st);
-    return tile_lj_t<float>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (float*)F.d, part, energy, P, smem,
-                            st);
+                                 sxy, sz, smem, st);
+    return tile_lj_t<float>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (float*)F.d, part, energy, P, sxy,
+                            sz, smem, st);
 }
 
 int tile_translate(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,

@@ -22,9 +22,13 @@ double fp32_band(pd_vd h, double r);  // FP64/FP32 staging of the pair kernel fi
 int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                unsigned int cap, double r_list, Buf& pos32, Buf& nbr, Buf& nn, long& stride, int& max_nn,
                cudaStream_t st);
+// The FP64 pair kernel stages (x, y) and z from copies of the positions: those of
+// the slots [first, first + n) refreshed from the records (room for the vector's capacity)
+int tile_split(pd_vd h, Buf& sxy, Buf& sz, long first, long n, cudaStream_t st);
+// LJ forces from the tiled rows (FP64: from the staging copies sxy / sz, which must be current)
 int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
             unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
-            double* part, bool energy, int P, cudaStream_t st);
+            double* part, bool energy, int P, const Buf& sxy, const Buf& sz, cudaStream_t st);
 int tile_translate(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                    const Buf& nbr, const Buf& nn, long stride, int max_nn, int* out_dev, cudaStream_t st);
 

@@ -28,6 +28,7 @@ RED_ADD, RED_MAX = 1, 2
 PUT_ADD, PUT_MAX, PUT_REPLACE = 1, 2, 3
 CMP_EQ, CMP_NE, CMP_LT, CMP_LE, CMP_GT, CMP_GE = range(6)
 VTK_WRITER, CSV_WRITER, FORMAT_BINARY = 0, 1, 2
+PD_STATIC_OUT_OF_GRID = 1  # status of pd_celllist_build_static: a position outside the grid
 
 _NP = {PD_F32: np.float32, PD_F64: np.float64, PD_I32: np.int32, PD_U32: np.uint32, PD_I64: np.int64}
 _CODES = {-1: "PD_EINVAL", -2: "PD_ENOMEM", -3: "PD_ECUDA", -4: "PD_ESTALE", -5: "PD_ETIMEOUT",
@@ -69,6 +70,12 @@ class SPHParams(ctypes.Structure):
     _fields_ = [("h", ctypes.c_double), ("mass", ctypes.c_double), ("c0", ctypes.c_double),
                 ("rho0", ctypes.c_double), ("alpha", ctypes.c_double), ("gz", ctypes.c_double),
                 ("rho_prop", ctypes.c_int), ("drho_prop", ctypes.c_int), ("type_prop", ctypes.c_int)]
+
+
+class SlabT(ctypes.Structure):
+    """pd_slab_t: slab r of nslabs along `axis` is [lo + r w, lo + (r+1) w), w = (hi - lo) / nslabs."""
+    _fields_ = [("axis", ctypes.c_int), ("nslabs", ctypes.c_int), ("periodic", ctypes.c_int),
+                ("lo", ctypes.c_double), ("hi", ctypes.c_double), ("ghost", ctypes.c_double)]
 
 
 class MDParams(ctypes.Structure):
@@ -149,6 +156,12 @@ def lib():
             "pd_set_cache_limit": ([lp, P(ctypes.c_long)], ip),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp, vp], ip),
+            "pd_slab_map_label": ([vp, P(SlabT), P(ctypes.c_long), vp], ip),
+            "pd_slab_halo_label": ([vp, P(SlabT), ip, P(ctypes.c_long), vp], ip),
+            "pd_slab_row_bytes": ([vp, ctypes.c_ulong, P(ctypes.c_long)], ip),
+            "pd_slab_pack": ([vp, ctypes.c_ulong, vp, lp, vp], ip),
+            "pd_slab_map_unpack": ([vp, ctypes.c_ulong, vp, lp, vp], ip),
+            "pd_slab_halo_unpack": ([vp, ctypes.c_ulong, vp, lp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
             "pd_sph_create": ([vp, P(SPHParams), P(MDParams), P(vp)], ip),
             "pd_srv_create": ([lp, ip, P(LJParams), ctypes.c_double, ctypes.c_double, P(vp)], ip),
@@ -372,9 +385,17 @@ class VectorDist:
         x = np.ascontiguousarray(x, dtype=self.dtype).reshape(-1, 3)
         check(lib().pd_h2d_pos(self.h, _ptr(x), int(offset), int(x.shape[0]), None))
 
-    def deviceToHostPos(self, offset=0, count=None, with_ghost=True, out=None):
-        """positions [n][3]; `out` (e.g. pinned memory) receives them when given"""
+    def deviceToHostPos(self, offset=0, count=None, with_ghost=True, out=None, device=False):
+        """positions [n][3]; `out` (e.g. pinned memory) receives them when given;
+        device=True returns a CUDA tensor (copied on the GPU)"""
         n = (self.size_local_with_ghost() if with_ghost else self.size_local()) - offset if count is None else count
+        if device:
+            import torch
+            t = torch.empty((max(n, 0), 3), dtype=torch.float64 if self.dtype == np.float64 else torch.float32,
+                            device="cuda")
+            if n:
+                check(lib().pd_d2h_pos(self.h, ctypes.c_void_p(t.data_ptr()), int(offset), int(n), None))
+            return t
         if out is None:
             out = np.zeros((n, 3), self.dtype)
         elif out.dtype != self.dtype or not out.flags.c_contiguous or out.size < 3 * n:
@@ -384,7 +405,18 @@ class VectorDist:
         return out
 
     def hostToDeviceProp(self, p, a, offset=0):
+        """property p from [n] or [n][ncomp] host data, or from a CUDA tensor of the
+        property's type (transposed on the GPU, no host round trip)"""
         t, nc = self.props[p]
+        if _is_cuda_tensor(a):
+            import torch
+            want = getattr(torch, np.dtype(_NP[t]).name)
+            if a.dtype != want:
+                raise TypeError(f"hostToDeviceProp: a {want} tensor is expected, got {a.dtype}")
+            cm = a.reshape(-1, nc).t().contiguous()
+            check(lib().pd_h2d_prop(self.h, int(p), ctypes.c_void_p(cm.data_ptr()), int(offset), int(cm.shape[1]),
+                                    None))
+            return
         a = np.asarray(a, dtype=_NP[t]).reshape(-1, nc)
         cm = np.ascontiguousarray(a.T)
         check(lib().pd_h2d_prop(self.h, int(p), _ptr(cm), int(offset), int(a.shape[0]), None))
@@ -430,6 +462,39 @@ class VectorDist:
         out = np.zeros(max(n, 1), np.int64)
         check(lib().pd_d2h_gid(self.h, _ptr(out), 0, int(n), None))
         return out[:n]
+
+    # -- slab decomposition over ranks (pd_slab_*): label, pack, (transport), unpack
+    def slab_map_label(self, slab):
+        """map labelling: the rows per destination rank (a list)."""
+        c = (ctypes.c_long * slab.nslabs)()
+        check(lib().pd_slab_map_label(self.h, ctypes.byref(slab), c, None))
+        return list(c)
+
+    def slab_halo_label(self, slab, rank):
+        """ghost_get labelling of `rank`: the halo rows per destination rank (a list)."""
+        c = (ctypes.c_long * slab.nslabs)()
+        check(lib().pd_slab_halo_label(self.h, ctypes.byref(slab), int(rank), c, None))
+        return list(c)
+
+    def slab_row_bytes(self, mask):
+        b = ctypes.c_long(0)
+        check(lib().pd_slab_row_bytes(self.h, ctypes.c_ulong(mask), ctypes.byref(b)))
+        return b.value
+
+    def slab_pack(self, mask, rows):
+        """the labelled rows packed into a new CUDA uint8 tensor [rows * row_bytes]"""
+        import torch
+        out = torch.empty(max(rows * self.slab_row_bytes(mask), 1), dtype=torch.uint8, device="cuda")
+        check(lib().pd_slab_pack(self.h, ctypes.c_ulong(mask), ctypes.c_void_p(out.data_ptr()), int(rows), None))
+        return out[: rows * self.slab_row_bytes(mask)]
+
+    def slab_map_unpack(self, mask, recv, n):
+        check(lib().pd_slab_map_unpack(self.h, ctypes.c_ulong(mask), ctypes.c_void_p(recv.data_ptr() if n else 0),
+                                       int(n), None))
+
+    def slab_halo_unpack(self, mask, recv, n):
+        check(lib().pd_slab_halo_unpack(self.h, ctypes.c_ulong(mask), ctypes.c_void_p(recv.data_ptr() if n else 0),
+                                        int(n), None))
 
     # -- reference API
     def map(self, opt=RUN_ON_DEVICE):

@@ -43,7 +43,8 @@ def test_c1_config_exact(pd, orc):
     l0 = pd.launch_count()
     E = md.run(100)
     launches = pd.launch_count() - l0
-    assert launches <= 8, launches  # the whole run in the cluster kernel, not ~28 kernels a step
+    # the first build, then all 100 steps in the cluster kernel: not the ~28 kernels of a graph step
+    assert launches < 50, launches
     xo, vo, Eo = orc.md_lj(x, v, lo, hi, bc, 2.5, 2.5, 0.0, 1.0, 1.0, 0.005, 1.0, 100)
     np.testing.assert_allclose(E[:, :3], Eo[1:, :3], rtol=1e-9, atol=1e-9)
     gid = vd.gid(with_ghost=False)
