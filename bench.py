@@ -540,7 +540,8 @@ def form_serving(pd, torch, n_systems=600, steps=50, slots=128, seed=6, loads=(0
             "note": "Poisson value = particle-steps of that phase / (last completion - first arrival), ramp-up and "
                     "drain included; vs_isolated = that value / the isolated sequential throughput; "
                     "systems_vs_capacity = systems completed per second / the capacity phase's systems per second",
-            "tuned_tile_width_by_log2_size": {str(k): v for k, v in tuned.items()},
+            "tuned_shape_by_log2_size": {str(k): {"tile_width": v[0], "lanes_per_particle": v[1], "cta_threads": v[2]}
+                                         for k, v in tuned.items()},
             "host_ms": {"capacity_phase": tm_cap, "total": tm_all, "ticks": st_all["ticks"],
                         "rebuilds": st_all["rebuilds"]}}
 

@@ -372,6 +372,8 @@ int pd_md_set_timing(pd_md md, int on);
  * global-index rows; tx = cells per tile along x (0 = from the mean occupancy),
  * threads_per_particle = 1, 2 or 4 lanes sharing one row (0 = 2) */
 int pd_md_set_tiles(pd_md md, int on, int tx, int threads_per_particle);
+/* threads per CTA (256 or 128) of the precision form's pair kernel (no reference counterpart) */
+int pd_md_set_block(pd_md md, int threads);
 /* the driver's Verlet rows as CSR of global particle indices (current storage
  * order: real particles then images); *tiled tells which structure is active */
 int pd_md_verlet_get(pd_md md, int* counts, int* idx, long idx_cap, int* tiled);
@@ -391,8 +393,13 @@ typedef struct pd_srv_s* pd_srv;
 int pd_srv_create(long hbm_budget_bytes, int max_slots, const pd_lj_params_t* lj, double dt, double skin,
                   pd_srv* out);
 int pd_srv_destroy(pd_srv s);
-/* autotune != 0: tile width chosen per size bucket by timing; else the fixed tx */
-int pd_srv_set_tuning(pd_srv s, int autotune, int tx);
+/* autotune != 0: the force kernel's launch shape (tile width, lanes per particle
+ * 1/2/4, threads per CTA 256/128) chosen per size bucket (floor(log2 N)) by timing
+ * the single-system kernel on the first system of the bucket; else the fixed shape
+ * (tx 0: the width from the occupancy) */
+int pd_srv_set_tuning(pd_srv s, int autotune, int tx, int lanes, int block);
+/* the shape of one size bucket set by the caller (used as if tuned, with or without autotune) */
+int pd_srv_set_shape(pd_srv s, int bucket, int tx, int lanes, int block);
 /* queue a system: n particles in a periodic cube of side `box`, host AoS x, v */
 int pd_srv_submit(pd_srv s, long n, double box, const double* x_host, const double* v_host, int steps,
                   long* ticket);
@@ -404,8 +411,8 @@ int pd_srv_state(pd_srv s, long ticket, int* state);
 int pd_srv_result(pd_srv s, long ticket, double* x_out, double* E_out, double* times);
 int pd_srv_release(pd_srv s, long ticket);
 int pd_srv_stats(pd_srv s, long* particle_steps, long* systems_done, long* ticks, long* rebuilds, double* tune_ms);
-/* autotuner table: size bucket (floor(log2 N)) -> tile width */
-int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int cap, int* n);
+/* autotuner table: size bucket (floor(log2 N)) -> tile width, lanes per particle, threads per CTA */
+int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int* lanes, int* blocks, int cap, int* n);
 /* tickets finished (done or failed) since the last call, oldest first, at most
    `cap`; the rest stay for the next call */
 int pd_srv_completed(pd_srv s, long* tickets, int cap, int* n);

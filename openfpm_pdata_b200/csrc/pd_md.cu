@@ -601,7 +601,7 @@ int md_forces(pd_md md, cudaStream_t st) {
     if (md->mixed)
         return mixed_lj(md->h, md->vl->cl, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(),
                         md->tcap, md->off, md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop,
-                        md->tpart.as<double>(), md->tile_p, st);
+                        md->tpart.as<double>(), md->tile_p, md->tile_block, st);
     if (md->tiles_active)
         return tile_lj(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                        md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop, md->tpart.as<double>(), true,
@@ -1161,6 +1161,12 @@ int pd_md_set_tiles(pd_md md, int on, int tx, int threads_per_particle) {
     md->tile_tx = tx;
     md->tile_p = p;
     md->ready = false;  // rebuild with the new structure at the next run
+    return PD_OK;
+}
+
+int pd_md_set_block(pd_md md, int threads) {
+    if (!md || (threads != FBLOCK_T && threads != FBLOCK_T / 2)) return PD_EINVAL;
+    md->tile_block = threads;
     return PD_OK;
 }
 

@@ -19,6 +19,7 @@ struct pd_md_s {
     bool use_tiles = true;
     int tile_tx = 0;  // cells per tile along x (0: from the mean occupancy)
     int tile_p = 2;   // threads per domain particle in the pair kernel
+    int tile_block = pd::FBLOCK_T;  // threads per CTA of the precision form's pair kernel
     bool tiles_active = false;
     pd::TileGeom tg;
     long ntiles = 0;

@@ -179,8 +179,8 @@ __global__ void __launch_bounds__(256) k_kick32(float* __restrict__ v, const flo
     if (threadIdx.x == 0) part[blockIdx.x] = ke;
 }
 
-template <int P>
-__global__ void __launch_bounds__(FBLOCK_T, 5) k_vtile_lj_mixed(const float4* __restrict__ off, long n_real,
+template <int P, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 5 * FBLOCK_T / BLOCK) k_vtile_lj_mixed(const float4* __restrict__ off, long n_real,
                                                              TileGeom tg, const unsigned int* __restrict__ csR,
                                                              const unsigned int* __restrict__ csI, unsigned int cap,
                                                              const unsigned int* __restrict__ nbr,
@@ -196,10 +196,10 @@ __global__ void __launch_bounds__(FBLOCK_T, 5) k_vtile_lj_mixed(const float4* __
     __syncthreads();
     unsigned int uses = 0;
     double pe = 0, vir = 0;
-    mixed_tile<P>(blockIdx.x, off, n_real, tg, csR, csI, cap, nbr, nn, stride, sx, sy, sz, Pr, f, fcap, err, sm, S,
-                  &bar, uses, pe, vir);
-    pe = block_sum<double, FBLOCK_T>(pe);
-    vir = block_sum<double, FBLOCK_T>(vir);
+    mixed_tile<P, BLOCK>(blockIdx.x, off, n_real, tg, csR, csI, cap, nbr, nn, stride, sx, sy, sz, Pr, f, fcap, err, sm,
+                         S, &bar, uses, pe, vir);
+    pe = block_sum<double, BLOCK>(pe);
+    vir = block_sum<double, BLOCK>(vir);
     if (threadIdx.x == 0) {
         part[2 * blockIdx.x] = pe;
         part[2 * blockIdx.x + 1] = vir;
@@ -310,14 +310,14 @@ int mixed_kick(pd_vd h, int vel_prop, int force_prop, int nblk, double half, dou
     return PD_OK;
 }
 
-template <int P>
+template <int P, int BLOCK>
 static int launch_mixed(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                         unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, float sx,
                         float sy, float sz, const LJP<float>& LP, float* f, double* part, cudaStream_t st) {
     int smem = (int)(cap * sizeof(float4));
     if (smem < 16) smem = 16;
-    PD_CUDA(cudaFuncSetAttribute(k_vtile_lj_mixed<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    pd::launch(k_vtile_lj_mixed<P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st, (const float4*)off.as<float4>(),
+    PD_CUDA(cudaFuncSetAttribute(k_vtile_lj_mixed<P, BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    pd::launch(k_vtile_lj_mixed<P, BLOCK>, (unsigned)ntiles, BLOCK, (size_t)smem, st, (const float4*)off.as<float4>(),
                h->n_real, tg, csR, csI, cap, (const unsigned int*)nbr.as<unsigned int>(), (const int*)nn.as<int>(),
                stride, sx, sy, sz, LP, f, h->cap, part, &h->ctrl->err);
     PD_LAUNCH_CHECK();
@@ -339,7 +339,7 @@ void mixed_cutoff(const pd_lj_params_t& lj, LJP<float>& P) {
 
 int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
              unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj,
-             int force_prop, double* part, int P, cudaStream_t st) {
+             int force_prop, double* part, int P, int block, cudaStream_t st) {
     LJP<float> LP{};
     LP.eps24 = (float)(24.0 * lj.eps);
     LP.eps4 = (float)(4.0 * lj.eps);
@@ -348,9 +348,18 @@ int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned 
     float* f = (float*)h->props[force_prop].d;
     const CellGeom C = mixed_cell_geom(cl);
     const float sx = (float)C.sp[0], sy = (float)C.sp[1], sz = (float)C.sp[2];  // exact: multiples of q
-    if (P == 1) return launch_mixed<1>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
-    if (P == 4) return launch_mixed<4>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
-    return launch_mixed<2>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
+#define PD_MIXED_CASE(PP, BB)                                                                                   \
+    if (P == PP && block == BB)                                                                                 \
+        return launch_mixed<PP, BB>(h, tg, ntiles, csR, csI, cap, off, nbr, nn, stride, sx, sy, sz, LP, f, part, st);
+    PD_MIXED_CASE(1, FBLOCK_T)
+    PD_MIXED_CASE(2, FBLOCK_T)
+    PD_MIXED_CASE(4, FBLOCK_T)
+    PD_MIXED_CASE(1, FBLOCK_T / 2)
+    PD_MIXED_CASE(2, FBLOCK_T / 2)
+    PD_MIXED_CASE(4, FBLOCK_T / 2)
+#undef PD_MIXED_CASE
+    set_error("precision form: lanes per particle 1, 2 or 4 and CTAs of %d or %d threads", FBLOCK_T, FBLOCK_T / 2);
+    return PD_EINVAL;
 }
 
 }  // namespace pd

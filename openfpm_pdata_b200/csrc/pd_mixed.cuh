@@ -23,6 +23,6 @@ int mixed_kick(pd_vd h, int vel_prop, int force_prop, int nblk, double half, dou
                cudaStream_t st);
 int mixed_lj(pd_vd h, pd_cl cl, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
              unsigned int cap, const Buf& off, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj,
-             int force_prop, double* part, int P, cudaStream_t st);
+             int force_prop, double* part, int P, int block, cudaStream_t st);
 
 }  // namespace pd

@@ -64,13 +64,14 @@ struct Kahan {
 };
 
 // One tile of the mixed-form LJ kernel, shared by the single-system kernel and
-// the batched persistent kernels of the serving loop.  The mbarrier `bar` is
+// the batched persistent kernels of the serving loop; P lanes per particle, CTAs
+// of BLOCK threads.  The mbarrier `bar` is
 // initialised by the caller; `uses` counts its completed phases (the parity of
 // the next wait).  Adds the thread's partial potential energy and virial to
 // pe / vir.  A tile whose staging exceeds `cap` sets ERR_TILE_CAP, or, with an
 // overflow list, is appended to it (item `ovf_item`) for a kernel with more
 // shared memory; the return value is then true (nothing computed).
-template <int P>
+template <int P, int BLOCK = FBLOCK_T>
 __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__ off, long n_real, const TileGeom& tg,
                                            const unsigned int* __restrict__ csR,
                                            const unsigned int* __restrict__ csI, unsigned int cap,
@@ -149,7 +150,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
     if (ok) {
         // rewrite the staged records: y/z relative to the centre row, w = cell column
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int sg = warp; sg < 18; sg += FBLOCK_T / 32) {
+        for (int sg = warp; sg < 18; sg += BLOCK / 32) {
             const int r = sg >> 1;
             const float shy = (float)(r % 3 - 1) * sy, shz = (float)(r / 3 - 1) * sz;
             for (unsigned int k = S.segb[sg][0] + lane; k < S.segb[sg][ncol - 1]; k += 32) {
@@ -165,7 +166,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
         __syncthreads();
         const unsigned int base = S.oR[4] - S.cR[4][0];
         // staged indices of the pairs a thread sets aside for FP64, column per thread
-        __shared__ unsigned short defer[MIXED_KDEF][FBLOCK_T];
+        __shared__ unsigned short defer[MIXED_KDEF][BLOCK];
         // rounds of the whole CTA over the tile's particles: P lanes per row while a
         // round is full, more lanes per row (up to a warp) in the last, partial round;
         // every thread takes part in every round (the shuffles need whole warps)
@@ -173,8 +174,8 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
         while (first < ie) {
             const unsigned int left = ie - first;
             unsigned int q = P;
-            while (q < 32u && left * (q << 1) <= (unsigned int)FBLOCK_T) q <<= 1;
-            const unsigned int cnt = min(left, (unsigned int)FBLOCK_T / q);
+            while (q < 32u && left * (q << 1) <= (unsigned int)BLOCK) q <<= 1;
+            const unsigned int cnt = min(left, (unsigned int)BLOCK / q);
             const int sub = (int)(threadIdx.x % q);
             const int Q = (int)q;
             const bool active = threadIdx.x / q < cnt;

@@ -59,7 +59,6 @@
 
 namespace pd {
 
-static constexpr int SRV_P = 2;                       // lanes per particle in the batched force kernel
 static constexpr int SRV_SMEM = 48 * 1024;            // staging bytes per tile CTA (fixed: graph-invariant)
 static constexpr unsigned SRV_CAP = SRV_SMEM / 16;    // staged FP32 records per tile
 static constexpr int SRV_BSMEM = 24 * 1024;           // staging bytes per CTA of the batched list build (one z-layer)
@@ -104,6 +103,7 @@ struct SysDesc {
     float sx, sy, sz;
     float lo_thr, hi_thr;
     double r2;
+    int lanes, block;  // the force kernel's lanes per particle and CTA size for this system (tuned per size)
     const BoxSet<double>* boxes;
     const double* shifts;
     // build scratch
@@ -135,14 +135,22 @@ struct SysDesc {
     int slot;
 };
 
+// the force kernel's launch shapes: lanes per particle 1, 2, 4 x CTAs of FBLOCK_T, FBLOCK_T / 2
+static constexpr int NSHAPE = 6;
+__host__ __device__ constexpr int shape_group(int lanes, int block) {
+    return (lanes == 1 ? 0 : (lanes == 2 ? 1 : 2)) + (block == FBLOCK_T ? 0 : 3);
+}
+
 struct BatchHdr {
     int nsys;
     int pad0;
     long tot_tiles, tot_chunks, tot_img;
-    unsigned int tile_ctr;   // work queue of the force kernel
     unsigned int ovf_force;  // tiles deferred to the large-staging kernels
     unsigned int ovf_build;
-    unsigned int pad1;
+    // force-kernel groups (shape_group: lanes per particle x CTA size): the
+    // descriptors list the groups in order, group k's tiles are [grp[k], grp[k+1])
+    long grp[NSHAPE + 1];
+    unsigned int grp_ctr[NSHAPE];  // work queue of each group's persistent kernel
 };
 
 // compacted work of the systems flagged for a rebuild this step
@@ -323,36 +331,57 @@ __global__ void __launch_bounds__(CHUNK) k_b_replay(const SysDesc* __restrict__ 
     }
 }
 
-__global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict__ D, BatchHdr* __restrict__ B,
-                                                      LJP<float> Pr, double* __restrict__ tpart,
-                                                      long* __restrict__ ovf) {
+// one tile of system d with its tuned lanes per particle (the overflow kernels)
+template <int BLOCK>
+__device__ __forceinline__ void b_force_tile_any(const SysDesc& d, long t, unsigned int cap, const LJP<float>& Pr,
+                                                 float4* sm, TileShM& S, unsigned long long* bar, unsigned int& uses,
+                                                 double& pe, double& vir) {
+    if (d.lanes == 1)
+        mixed_tile<1, BLOCK>(t, d.off, d.n_real, d.tg, d.csR, d.csI, cap, d.nbr, d.nn, d.tstride, d.sx, d.sy, d.sz, Pr,
+                             d.f, d.cap, d.err, sm, S, bar, uses, pe, vir);
+    else if (d.lanes == 4)
+        mixed_tile<4, BLOCK>(t, d.off, d.n_real, d.tg, d.csR, d.csI, cap, d.nbr, d.nn, d.tstride, d.sx, d.sy, d.sz, Pr,
+                             d.f, d.cap, d.err, sm, S, bar, uses, pe, vir);
+    else
+        mixed_tile<2, BLOCK>(t, d.off, d.n_real, d.tg, d.csR, d.csI, cap, d.nbr, d.nn, d.tstride, d.sx, d.sy, d.sz, Pr,
+                             d.f, d.cap, d.err, sm, S, bar, uses, pe, vir);
+}
+
+// Persistent force kernel of one shape group (LANES lanes per particle, CTAs of
+// BLOCK threads): the tiles [grp[k], grp[k+1]) of the systems of that shape.
+template <int LANES, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_b_force(const SysDesc* __restrict__ D, BatchHdr* __restrict__ B,
+                                                   LJP<float> Pr, double* __restrict__ tpart,
+                                                   long* __restrict__ ovf) {
     extern __shared__ __align__(128) unsigned char tile_raw[];
     float4* sm = reinterpret_cast<float4*>(tile_raw);
     __shared__ TileShM S;
     __shared__ unsigned long long bar;
     __shared__ long cur;
+    constexpr int G = shape_group(LANES, BLOCK);
+    const long first = B->grp[G], tot = B->grp[G + 1];
+    if (first >= tot) return;  // no system of this shape in the batch
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     unsigned int uses = 0;
     const int nsys = B->nsys;
-    const long tot = B->tot_tiles;
     for (;;) {
         // generic-proxy accesses of the previous tile are ordered before the next bulk copies
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0) cur = (long)atomicAdd(&B->tile_ctr, 1u);
+        if (threadIdx.x == 0) cur = first + (long)atomicAdd(&B->grp_ctr[G], 1u);
         __syncthreads();
         const long g = cur;
         if (g >= tot) break;
         const int s = find_sys(D, nsys, g, 0);
         const SysDesc& d = D[s];
         double pe = 0, vir = 0;
-        if (mixed_tile<SRV_P>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_CAP, d.nbr, d.nn, d.tstride,
-                              d.sx, d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir, &B->ovf_force, ovf,
-                              g))
+        if (mixed_tile<LANES, BLOCK>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_CAP, d.nbr, d.nn,
+                                     d.tstride, d.sx, d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir,
+                                     &B->ovf_force, ovf, g))
             continue;  // deferred to k_b_force_ovf
-        pe = block_sum<double, FBLOCK_T>(pe);
-        vir = block_sum<double, FBLOCK_T>(vir);
+        pe = block_sum<double, BLOCK>(pe);
+        vir = block_sum<double, BLOCK>(vir);
         if (threadIdx.x == 0) {
             const long slot = d.tpart_base + (g - d.tile_base);
             tpart[2 * slot] = pe;
@@ -361,10 +390,12 @@ __global__ void __launch_bounds__(FBLOCK_T) k_b_force(const SysDesc* __restrict_
     }
 }
 
-// tiles whose staging exceeds SRV_CAP, with SRV_BIG of shared memory
-__global__ void __launch_bounds__(FBLOCK_T) k_b_force_ovf(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
-                                                          LJP<float> Pr, double* __restrict__ tpart,
-                                                          const long* __restrict__ ovf) {
+// tiles whose staging exceeds SRV_CAP, with SRV_BIG of shared memory (each CTA size
+// takes the tiles of its systems)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_b_force_ovf(const SysDesc* __restrict__ D, const BatchHdr* __restrict__ B,
+                                                       LJP<float> Pr, double* __restrict__ tpart,
+                                                       const long* __restrict__ ovf) {
     extern __shared__ __align__(128) unsigned char tile_raw[];
     float4* sm = reinterpret_cast<float4*>(tile_raw);
     __shared__ TileShM S;
@@ -375,16 +406,16 @@ __global__ void __launch_bounds__(FBLOCK_T) k_b_force_ovf(const SysDesc* __restr
     const int nsys = B->nsys;
     const long tot = B->ovf_force;
     for (long q = blockIdx.x; q < tot; q += gridDim.x) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
         const long g = ovf[q];
         const int s = find_sys(D, nsys, g, 0);
         const SysDesc& d = D[s];
+        if (d.block != BLOCK) continue;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
         double pe = 0, vir = 0;
-        mixed_tile<SRV_P>(g - d.tile_base, d.off, d.n_real, d.tg, d.csR, d.csI, SRV_BIG_CAP, d.nbr, d.nn, d.tstride,
-                          d.sx, d.sy, d.sz, Pr, d.f, d.cap, d.err, sm, S, &bar, uses, pe, vir);
-        pe = block_sum<double, FBLOCK_T>(pe);
-        vir = block_sum<double, FBLOCK_T>(vir);
+        b_force_tile_any<BLOCK>(d, g - d.tile_base, SRV_BIG_CAP, Pr, sm, S, &bar, uses, pe, vir);
+        pe = block_sum<double, BLOCK>(pe);
+        vir = block_sum<double, BLOCK>(vir);
         if (threadIdx.x == 0) {
             const long slot = d.tpart_base + (g - d.tile_base);
             tpart[2 * slot] = pe;
@@ -840,6 +871,12 @@ __global__ void k_srv_iota(int* __restrict__ g, long n) {
 using namespace pd;
 
 // ---------------------------------------------------------------------------
+// launch shape of a system's force kernel: tile width (cells along x), lanes per
+// particle, threads per CTA
+struct SrvShape {
+    int tx, lanes, block;
+};
+
 struct SrvSlot {
     pd_vd h = nullptr;
     pd_md md = nullptr;
@@ -1081,10 +1118,10 @@ struct pd_srv_s {
     bool adm_pending = false;
     cudaGraphExec_t gstep[4] = {nullptr, nullptr, nullptr, nullptr};  // 1, 2, 4, 8 steps per launch
     bool dirty = true;
-    // autotuner: size bucket -> tile width
+    // autotuner: size bucket -> tile width, lanes per particle, CTA size of the force kernel
     bool autotune = true;
-    int fixed_tx = 0;
-    std::map<int, int> tuned;
+    SrvShape fixed{0, 2, pd::FBLOCK_T};
+    std::map<int, SrvShape> tuned;
     // statistics
     long particle_steps = 0, systems_done = 0, steps_run = 0, rebuilds = 0;
     double tune_ms = 0;
@@ -1144,6 +1181,8 @@ static void fill_desc(pd_srv s, SrvReq* r, SysDesc& d) {
     d.nn = md->tnn.as<int>();
     d.tstride = md->tstride;
     d.max_nn = md->tmax_nn;
+    d.lanes = md->tile_p;
+    d.block = md->tile_block;
     d.sx = (float)d.C.sp[0];  // exact: multiples of the quantum
     d.sy = (float)d.C.sp[1];
     d.sz = (float)d.C.sp[2];
@@ -1193,9 +1232,19 @@ static int upload_tables(pd_srv s) {
     int ns = (int)s->active.size();
     s->hdesc.resize(ns);
     long tb = 0, cb = 0, ib = 0, tp = 0, kp = 0;
+    // the systems in order of their force kernel's shape group (each group's tiles
+    // contiguous), in admission order within a group
+    std::vector<SrvReq*> order;
+    for (int grp = 0; grp < NSHAPE; ++grp)
+        for (SrvReq* r : s->active) {
+            const pd_md m = s->slots[r->slot].md;
+            if (shape_group(m->tile_p, m->tile_block) == grp) order.push_back(r);
+        }
+    for (int grp = 0; grp <= NSHAPE; ++grp) s->hhdr.grp[grp] = 0;
     for (int k = 0; k < ns; ++k) {
         SysDesc& d = s->hdesc[k];
-        fill_desc(s, s->active[k], d);
+        fill_desc(s, order[k], d);
+        for (int grp = shape_group(d.lanes, d.block) + 1; grp <= NSHAPE; ++grp) s->hhdr.grp[grp] = tb + d.ntiles;
         d.tile_base = tb;
         d.chunk_base = cb;
         d.img_base = ib;
@@ -1215,7 +1264,7 @@ static int upload_tables(pd_srv s) {
     s->hhdr.tot_tiles = tb;
     s->hhdr.tot_chunks = cb;
     s->hhdr.tot_img = ib;
-    s->hhdr.tile_ctr = 0;
+    for (int grp = 0; grp < NSHAPE; ++grp) s->hhdr.grp_ctr[grp] = 0;
     if (ns) PD_CUDA(cudaMemcpyAsync(s->desc.p, s->hdesc.data(), sizeof(SysDesc) * ns, cudaMemcpyHostToDevice, s->st));
     PD_CUDA(cudaMemcpyAsync(s->hdr.p, &s->hhdr, sizeof(BatchHdr), cudaMemcpyHostToDevice, s->st));
     PD_CUDA(cudaStreamSynchronize(s->st));  // host staging vectors are reused
@@ -1223,7 +1272,7 @@ static int upload_tables(pd_srv s) {
     return PD_OK;
 }
 
-static constexpr int GRAPH_KERNELS = 32;  // kernel nodes per step of the step graphs
+static constexpr int GRAPH_KERNELS = 38;  // kernel nodes per step of the step graphs
 
 // the step graphs: 2^lk velocity-Verlet steps of every active system per launch
 static int capture_graph(pd_srv s, int lk) {
@@ -1233,16 +1282,26 @@ static int capture_graph(pd_srv s, int lk) {
     P.eps4 = (float)(4.0 * s->lj.eps);
     P.sig2 = (float)(s->lj.sigma * s->lj.sigma);
     mixed_cutoff(s->lj, P);
-    PD_CUDA(cudaFuncSetAttribute(k_b_force, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
+#define PD_SRV_FORCE_ATTR(L, BL) \
+    PD_CUDA(cudaFuncSetAttribute(k_b_force<L, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_SMEM));
+    PD_SRV_FORCE_ATTR(1, FBLOCK_T)
+    PD_SRV_FORCE_ATTR(2, FBLOCK_T)
+    PD_SRV_FORCE_ATTR(4, FBLOCK_T)
+    PD_SRV_FORCE_ATTR(1, FBLOCK_T / 2)
+    PD_SRV_FORCE_ATTR(2, FBLOCK_T / 2)
+    PD_SRV_FORCE_ATTR(4, FBLOCK_T / 2)
+#undef PD_SRV_FORCE_ATTR
     PD_CUDA(cudaFuncSetAttribute(k_rb_build<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BSMEM));
-    PD_CUDA(cudaFuncSetAttribute(k_b_force_ovf, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
+    PD_CUDA(cudaFuncSetAttribute(k_b_force_ovf<FBLOCK_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
+    PD_CUDA(cudaFuncSetAttribute(k_b_force_ovf<FBLOCK_T / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
     PD_CUDA(cudaFuncSetAttribute(k_rb_build<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_BIG));
-    int sms = 148, dev = 0, per = 1, perb = 1;
+    int sms = 148, dev = 0, per = 1, per2 = 1, perb = 1;
     PD_CUDA(cudaGetDevice(&dev));
     PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_force, FBLOCK_T, SRV_SMEM));
+    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_force<2, FBLOCK_T>, FBLOCK_T, SRV_SMEM));
+    PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_b_force<2, FBLOCK_T / 2>, FBLOCK_T / 2, SRV_SMEM));
     PD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_rb_build<0>, TBLOCK, SRV_BSMEM));
-    const int gf = sms * std::max(per, 1), gb = sms * std::max(perb, 1), gc = sms * 8;
+    const int gf = sms * std::max(per, 1), gf2 = sms * std::max(per2, 1), gb = sms * std::max(perb, 1), gc = sms * 8;
     const SysDesc* D = s->desc.as<SysDesc>();
     BatchHdr* B = s->hdr.as<BatchHdr>();
     RbWork* W = s->work.as<RbWork>();
@@ -1256,7 +1315,8 @@ static int capture_graph(pd_srv s, int lk) {
     PD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int step = 0; step < (1 << lk); ++step) {
     cudaMemsetAsync(md2, 0, sizeof(unsigned long long) * M, st);
-    cudaMemsetAsync(&B->tile_ctr, 0, 3 * sizeof(unsigned int), st);  // tile_ctr, ovf_force, ovf_build
+    cudaMemsetAsync(&B->ovf_force, 0, 2 * sizeof(unsigned int), st);  // ovf_force, ovf_build
+    cudaMemsetAsync(B->grp_ctr, 0, sizeof(B->grp_ctr), st);
     unsigned int* ph = s->phase.as<unsigned int>();
     k_b_kick_drift<<<gc, CHUNK, 0, st>>>(D, B, half, dt, md2, ph);
     k_b_decide<<<1, 1024, 0, st>>>(D, B, md2, lim2, always, fl, ph, W);
@@ -1288,8 +1348,16 @@ static int capture_graph(pd_srv s, int lk) {
     k_rb_build<1><<<sms, TBLOCK, SRV_BIG, st>>>(D, W, B, s->ovf_b.as<long>(), s->nnmax.as<unsigned int>());
     // step of every system
     k_b_replay<<<gc, CHUNK, 0, st>>>(D, B, fl);
-    k_b_force<<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
-    k_b_force_ovf<<<sms, FBLOCK_T, SRV_BIG, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    // one persistent force kernel per shape group (a group without systems returns at once)
+    k_b_force<1, FBLOCK_T><<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force<2, FBLOCK_T><<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force<4, FBLOCK_T><<<gf, FBLOCK_T, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force<1, FBLOCK_T / 2><<<gf2, FBLOCK_T / 2, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force<2, FBLOCK_T / 2><<<gf2, FBLOCK_T / 2, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force<4, FBLOCK_T / 2><<<gf2, FBLOCK_T / 2, SRV_SMEM, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force_ovf<FBLOCK_T><<<sms, FBLOCK_T, SRV_BIG, st>>>(D, B, P, s->tpart.as<double>(), s->ovf_f.as<long>());
+    k_b_force_ovf<FBLOCK_T / 2><<<sms, FBLOCK_T / 2, SRV_BIG, st>>>(D, B, P, s->tpart.as<double>(),
+                                                                   s->ovf_f.as<long>());
     k_b_kick<<<gc, CHUNK, 0, st>>>(D, B, half, s->kpart.as<double>(), ph);
     k_b_energy<<<M, 256, 0, st>>>(D, B, s->tpart.as<double>(), s->kpart.as<double>(), fl, ph);
     }
@@ -1332,7 +1400,7 @@ static int slot_capacity(pd_vd h, long need) {
 }
 
 // (re)initialise a slot's containers for a system of n particles in a box of side L
-static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
+static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, const SrvShape& shape) {
     const double rl = s->lj.r_cut + s->skin;
     if (!sl.h) {
         double lo[3] = {0, 0, 0}, hi[3] = {r->L, r->L, r->L};
@@ -1374,7 +1442,9 @@ static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, int tx) {
         PD_TRY(md->kpart.ensure(sizeof(double) * md->nblk));
         PD_TRY(md->xb.ensure((size_t)r->n * h->pos_bytes));
     }
-    sl.md->tile_tx = tx;
+    sl.md->tile_tx = shape.tx;
+    sl.md->tile_p = shape.lanes;
+    sl.md->tile_block = shape.block;
     // capacities for the batched rebuilds, reserved before the first build so that
     // the buffers it fills are not reallocated afterwards
     sl.img_cap = (long)(1.3 * image_estimate(r->n, r->L, rl)) + 2048;
@@ -1571,12 +1641,13 @@ static int load_state(pd_srv s, SrvSlot& sl, SrvReq* r) {
 
 static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r);
 
-// time the single-system force for candidate tile widths on a throw-away copy of
-// the system (so the admitted system starts from the submitted state); keep the fastest
+// time the single-system force for candidate shapes (tile width x lanes per particle
+// x CTA size) on a throw-away copy of the system (so the admitted system starts from
+// the submitted state); keep the fastest
 static int autotune_tx(pd_srv s, SrvReq* r) {
     AllocScope scope(s->as, s->pool);
     SrvSlot tmp;
-    int rc = slot_reset(s, tmp, r, 0);
+    int rc = slot_reset(s, tmp, r, SrvShape{0, 2, FBLOCK_T});
     if (rc == PD_OK) rc = load_state(s, tmp, r);
     if (rc == PD_OK) rc = autotune_tx_on(s, tmp, r);
     cudaStreamSynchronize(s->as);
@@ -1584,39 +1655,77 @@ static int autotune_tx(pd_srv s, SrvReq* r) {
     return rc;
 }
 
-static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
-    static const int cand[] = {5, 7, 9, 12};
-    cudaEvent_t a, b;
-    PD_CUDA(cudaEventCreate(&a));
-    PD_CUDA(cudaEventCreate(&b));
-    int best = 0;
-    float best_ms = 1e30f;
-    double t0 = now_s(s);
-    for (int tx : cand) {
+// the force time of the slot's system for its current shape (three launches after a warm one)
+static int time_forces(pd_srv s, SrvSlot& sl, cudaEvent_t a, cudaEvent_t b, float& ms) {
+    PD_TRY(md_forces(sl.md, s->as));
+    PD_CUDA(cudaEventRecord(a, s->as));
+    for (int k = 0; k < 3; ++k) PD_TRY(md_forces(sl.md, s->as));
+    PD_CUDA(cudaEventRecord(b, s->as));
+    PD_CUDA(cudaEventSynchronize(b));
+    PD_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return PD_OK;
+}
+
+// two stages: the tile width with 2 lanes and CTAs of FBLOCK_T, then lanes per
+// particle x CTA size at that width (systems of at least two tiles per SM)
+static int autotune_shape(pd_srv s, SrvSlot& sl, SrvReq* r, cudaEvent_t a, cudaEvent_t b) {
+    static const int cand_tx[] = {5, 7, 9, 12};
+    static const int cand_lanes[] = {1, 2, 4};
+    static const int cand_block[] = {FBLOCK_T, FBLOCK_T / 2};
+    SrvShape best{0, 2, FBLOCK_T};
+    float best_ms = 1e30f, ms = 0;
+    sl.md->tile_p = 2;
+    sl.md->tile_block = FBLOCK_T;
+    for (int tx : cand_tx) {
         sl.md->tile_tx = tx;
-        int rc = md_rebuild(sl.md, s->as);
-        if (rc != PD_OK || !sl.md->tiles_active || sl.md->tcap > SRV_BIG_CAP) continue;
-        PD_TRY(md_forces(sl.md, s->as));  // warm
-        PD_CUDA(cudaEventRecord(a, s->as));
-        for (int k = 0; k < 3; ++k) PD_TRY(md_forces(sl.md, s->as));
-        PD_CUDA(cudaEventRecord(b, s->as));
-        PD_CUDA(cudaEventSynchronize(b));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
+        if (md_rebuild(sl.md, s->as) != PD_OK || !sl.md->tiles_active || sl.md->tcap > SRV_BIG_CAP) continue;
+        PD_TRY(time_forces(s, sl, a, b, ms));
         if (ms < best_ms) {
             best_ms = ms;
-            best = tx;
+            best.tx = tx;
         }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    s->tune_ms += 1000.0 * (now_s(s) - t0);
-    if (best == 0) {
+    if (best.tx == 0) {
         set_error("serving: no tile width fits the batched kernel's shared memory");
         return PD_EOVERFLOW;
     }
+    sl.md->tile_tx = best.tx;
+    PD_TRY(md_rebuild(sl.md, s->as));
+    // Lanes and CTA size only for systems of at least two tiles per SM: the timing
+    // of a smaller system's single launch measures its latency, not the throughput
+    // it gets among the batch's tiles.  Another shape must beat the default by 10 %.
+    int sms = 148, dev = 0;
+    PD_CUDA(cudaGetDevice(&dev));
+    PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (sl.md->ntiles >= 2L * sms) {
+        const float base_ms = best_ms;
+        for (int lanes : cand_lanes)
+            for (int block : cand_block) {
+                if (lanes == 2 && block == FBLOCK_T) continue;  // timed in the first stage
+                sl.md->tile_p = lanes;
+                sl.md->tile_block = block;
+                PD_TRY(time_forces(s, sl, a, b, ms));
+                if (ms < best_ms && ms < 0.9f * base_ms) {
+                    best_ms = ms;
+                    best.lanes = lanes;
+                    best.block = block;
+                }
+            }
+    }
     s->tuned[r->bucket] = best;
     return PD_OK;
+}
+
+static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
+    cudaEvent_t a, b;
+    PD_CUDA(cudaEventCreate(&a));
+    PD_CUDA(cudaEventCreate(&b));
+    const double t0 = now_s(s);
+    const int rc = autotune_shape(s, sl, r, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    s->tune_ms += 1000.0 * (now_s(s) - t0);
+    return rc;
 }
 
 // Admission is host-side setup only: geometry, tile plan and capacities of the
@@ -1625,10 +1734,13 @@ static int autotune_tx_on(pd_srv s, SrvSlot& sl, SrvReq* r) {
 static int admit_one(pd_srv s, SrvReq* r, int slot) {
     r->slot = slot;
     r->bucket = (int)std::floor(std::log2((double)std::max(r->n, 1L)));
+    // the bucket's shape: set by the caller or tuned before, else tuned now, else the fixed one
     if (s->autotune && !s->tuned.count(r->bucket)) PD_TRY(autotune_tx(s, r));
+    const auto it = s->tuned.find(r->bucket);
+    const SrvShape shape = it != s->tuned.end() ? it->second : s->fixed;
     SrvSlot& sl = s->slots[slot];
     const double t0 = now_s(s);
-    PD_TRY(slot_reset(s, sl, r, s->autotune ? s->tuned[r->bucket] : s->fixed_tx));
+    PD_TRY(slot_reset(s, sl, r, shape));
     s->ms[1] += 1e3 * (now_s(s) - t0);
     pd_md md = sl.md;
     pd_cl cl = md->vl->cl;
@@ -1872,10 +1984,20 @@ int pd_srv_destroy(pd_srv s) {
     return PD_OK;
 }
 
-int pd_srv_set_tuning(pd_srv s, int autotune, int tx) {
-    if (!s || tx < 0 || tx > TXMAX) return PD_EINVAL;
+int pd_srv_set_tuning(pd_srv s, int autotune, int tx, int lanes, int block) {
+    if (!s || tx < 0 || tx > TXMAX || (lanes != 1 && lanes != 2 && lanes != 4) ||
+        (block != FBLOCK_T && block != FBLOCK_T / 2))
+        return PD_EINVAL;
     s->autotune = autotune != 0;
-    s->fixed_tx = tx;
+    s->fixed = SrvShape{tx, lanes, block};
+    return PD_OK;
+}
+
+int pd_srv_set_shape(pd_srv s, int bucket, int tx, int lanes, int block) {
+    if (!s || bucket < 0 || tx < 1 || tx > TXMAX || (lanes != 1 && lanes != 2 && lanes != 4) ||
+        (block != FBLOCK_T && block != FBLOCK_T / 2))
+        return PD_EINVAL;
+    s->tuned[bucket] = SrvShape{tx, lanes, block};
     return PD_OK;
 }
 
@@ -2079,13 +2201,15 @@ int pd_srv_timers(pd_srv s, double ms[4]) {
     return PD_OK;
 }
 
-int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int cap, int* n) {
+int pd_srv_tuned(pd_srv s, int* buckets, int* widths, int* lanes, int* blocks, int cap, int* n) {
     if (!s || !n) return PD_EINVAL;
     int k = 0;
     for (auto& kv : s->tuned) {
         if (k < cap) {
             if (buckets) buckets[k] = kv.first;
-            if (widths) widths[k] = kv.second;
+            if (widths) widths[k] = kv.second.tx;
+            if (lanes) lanes[k] = kv.second.lanes;
+            if (blocks) blocks[k] = kv.second.block;
         }
         ++k;
     }

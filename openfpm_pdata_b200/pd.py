@@ -163,10 +163,12 @@ def lib():
             "pd_slab_map_unpack": ([vp, ctypes.c_ulong, vp, lp, vp], ip),
             "pd_slab_halo_unpack": ([vp, ctypes.c_ulong, vp, lp, vp], ip),
             "pd_md_set_tiles": ([vp, ip, ip, ip], ip),
+            "pd_md_set_block": ([vp, ip], ip),
             "pd_sph_create": ([vp, P(SPHParams), P(MDParams), P(vp)], ip),
             "pd_srv_create": ([lp, ip, P(LJParams), ctypes.c_double, ctypes.c_double, P(vp)], ip),
             "pd_srv_destroy": ([vp], ip),
-            "pd_srv_set_tuning": ([vp, ip, ip], ip),
+            "pd_srv_set_tuning": ([vp, ip, ip, ip, ip], ip),
+            "pd_srv_set_shape": ([vp, ip, ip, ip, ip], ip),
             "pd_srv_submit": ([vp, lp, ctypes.c_double, vp, vp, ip, P(ctypes.c_long)], ip),
             "pd_srv_tick": ([vp, P(ctypes.c_int), P(ctypes.c_int)], ip),
             "pd_srv_state": ([vp, lp, P(ctypes.c_int)], ip),
@@ -174,7 +176,7 @@ def lib():
             "pd_srv_release": ([vp, lp], ip),
             "pd_srv_stats": ([vp, P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long),
                               P(ctypes.c_double)], ip),
-            "pd_srv_tuned": ([vp, vp, vp, ip, P(ctypes.c_int)], ip),
+            "pd_srv_tuned": ([vp, vp, vp, vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_srv_timers": ([vp, vp], ip),
             "pd_srv_completed": ([vp, vp, ip, P(ctypes.c_int)], ip),
             "pd_gen_clustered": ([lp, ctypes.c_double, ip, ctypes.c_double, ctypes.c_double, ctypes.c_ulong, ip, vp,
@@ -656,6 +658,10 @@ class MD:
     def set_tiles(self, on=True, tx=0, threads_per_particle=0):
         check(lib().pd_md_set_tiles(self.h, int(bool(on)), int(tx), int(threads_per_particle)))
 
+    def set_block(self, threads):
+        """Threads per CTA (256 or 128) of the precision form's pair kernel."""
+        check(lib().pd_md_set_block(self.h, int(threads)))
+
     def verlet(self):
         """(offsets, idx, tiled) of the driver's current Verlet rows (global indices)."""
         n = self.vd.size_local()
@@ -705,14 +711,18 @@ class Server:
     QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
 
     def __init__(self, hbm_budget_bytes, max_slots=64, dt=0.005, skin=0.3, eps=1.0, sigma=1.0, r_cut=2.5,
-                 autotune=True, tx=0):
+                 autotune=True, tx=0, lanes=2, block=256):
         self.lj = LJParams(eps, sigma, r_cut)
         h = ctypes.c_void_p()
         check(lib().pd_srv_create(int(hbm_budget_bytes), int(max_slots), ctypes.byref(self.lj), float(dt),
                                   float(skin), ctypes.byref(h)))
         self.h = h
         self.info = {}
-        check(lib().pd_srv_set_tuning(self.h, int(bool(autotune)), int(tx)))
+        check(lib().pd_srv_set_tuning(self.h, int(bool(autotune)), int(tx), int(lanes), int(block)))
+
+    def set_shape(self, bucket, tx, lanes, block):
+        """The force kernel's launch shape for systems of size bucket floor(log2 N)."""
+        check(lib().pd_srv_set_shape(self.h, int(bucket), int(tx), int(lanes), int(block)))
 
     def submit(self, x, v, box, steps):
         x = np.ascontiguousarray(x, np.float64)
@@ -766,11 +776,12 @@ class Server:
         return out[: n.value].tolist()
 
     def tuned(self):
-        b = np.zeros(64, np.int32)
-        w = np.zeros(64, np.int32)
+        """size bucket -> (tile width, lanes per particle, threads per CTA) of the force kernel"""
+        b, w, l, k = (np.zeros(64, np.int32) for _ in range(4))
         n = ctypes.c_int(0)
-        check(lib().pd_srv_tuned(self.h, _ptr(b), _ptr(w), 64, ctypes.byref(n)))
-        return dict(zip(b[:n.value].tolist(), w[:n.value].tolist()))
+        check(lib().pd_srv_tuned(self.h, _ptr(b), _ptr(w), _ptr(l), _ptr(k), 64, ctypes.byref(n)))
+        m = n.value
+        return {int(b[i]): (int(w[i]), int(l[i]), int(k[i])) for i in range(m)}
 
     def run_until_done(self, tickets, max_ticks=100000):
         for _ in range(max_ticks):

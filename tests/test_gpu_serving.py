@@ -24,8 +24,10 @@ def _sys(n, seed):
     return workloads.serving_system(n, density=0.8, seed=seed)
 
 
-def _serve(pd, systems, steps=20, autotune=False, tx=5, budget=8 << 30, slots=16):
+def _serve(pd, systems, steps=20, autotune=False, tx=5, budget=8 << 30, slots=16, shapes=None):
     srv = pd.Server(budget, max_slots=slots, dt=0.005, skin=0.3, autotune=autotune, tx=tx)
+    for bucket, shape in (shapes or {}).items():
+        srv.set_shape(bucket, *shape)
     tickets = [srv.submit(x, v, L, steps) for (x, v, L) in systems]
     srv.run_until_done(tickets)
     out = [srv.result(t) for t in tickets]
@@ -84,6 +86,39 @@ def test_served_matches_single_driver_and_oracle(pd, orc):
     tot = Es[:, 0] + Es[:, 1]
     toto = Eo[1:, 0] + Eo[1:, 1]
     assert np.max(np.abs(tot - toto) / np.abs(toto)) < 2e-5
+
+
+@pytest.mark.parametrize("lanes,block", [(1, 128), (4, 256), (2, 128)])
+def test_served_shape_matches_single_driver(pd, lanes, block):
+    """Every launch shape of the batched force kernel (lanes per particle, CTA size)
+    gives the single-system driver's trajectory with the same shape, bit for bit."""
+    x, v, L = _sys(6000, 3)
+    bucket = int(np.floor(np.log2(6000)))
+    (xs, Es, _), = _serve(pd, [(x, v, L)], steps=15, autotune=True, shapes={bucket: (5, lanes, block)})[0]
+    assert _serve.last.tuned()[bucket] == (5, lanes, block)
+    vd = pd.VectorDist(x.shape[0], np.zeros(3), np.full(3, L), np.ones(3, np.int32), 2.8, dtype=np.float64,
+                       props=[(pd.PD_F32, 3), (pd.PD_F32, 3)])
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3, precision=pd.PREC_MIXED)
+    md.set_tiles(True, tx=5, threads_per_particle=lanes)
+    md.set_block(block)
+    E1 = md.run(15)
+    np.testing.assert_allclose(Es[:, :3], E1[:, :3], rtol=1e-12, atol=1e-12)
+    x1 = np.zeros_like(x)
+    x1[vd.gid(with_ghost=False)] = vd.deviceToHostPos(with_ghost=False)
+    assert np.array_equal(x1, xs)
+
+
+def test_mixed_shapes_alone_equals_in_mix(pd):
+    """Systems of different size buckets with different shapes (both CTA sizes, all
+    lane counts) in one batch: each result equals the system served alone."""
+    systems = [_sys(n, 50 + k) for k, n in enumerate([700, 3000, 9000, 20000])]
+    shapes = {9: (5, 1, 128), 11: (7, 4, 256), 13: (9, 2, 128), 14: (5, 2, 256)}
+    mix, _ = _serve(pd, systems, shapes=shapes)
+    for k, s in enumerate(systems):
+        (xa, Ea, _), = _serve(pd, [s], shapes=shapes)[0]
+        assert np.array_equal(Ea, mix[k][1]) and np.array_equal(xa, mix[k][0])
 
 
 def test_admission_by_budget(pd):
