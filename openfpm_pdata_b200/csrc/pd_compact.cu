@@ -2,10 +2,11 @@
 // (Vector/cuda/vector_dist_cuda_funcs.cuh:313-481).
 //
 // remove_marked<prp>: the mark property is flipped in place (x -> x == 0, the
-// reference's destructive step, flip_one_to_zero :313-321), the flipped flags are
-// scanned, and every kept particle (mark 0 before the flip) is scattered, in
-// order, with its position, global id and all properties (copy_new_to_old_by_scan
-// :295-311).  The ghosts are dropped: the vector then holds the kept particles
+// reference's destructive step, flip_one_to_zero :313-321) while each tile counts
+// its kept particles, the tile counts are scanned, and every kept particle (mark
+// 0 before the flip) is scattered, in order, with its position, global id and all
+// properties (copy_new_to_old_by_scan :295-311), its rank within the tile from
+// warp ballots.  The ghosts are dropped: the vector then holds the kept particles
 // only (setGhostMarker(kept), :406).  When nothing is marked the vector keeps its
 // particles and the flipped mark (:366-372).
 //
@@ -32,21 +33,34 @@ struct ColSet {
     int wsize[CMAXC];  // bytes per element: 4, 8, 16 or 32
 };
 
+// compaction tiles: CT_BLOCK threads, CT_ITEMS passes of CT_BLOCK consecutive particles
+static constexpr int CT_BLOCK = 512;
+static constexpr int CT_ITEMS = 8;
+static constexpr long CT_TILE = (long)CT_BLOCK * CT_ITEMS;
+
+// the mark flipped in place (x -> x == 0), a keep byte per particle and the
+// tile's count of kept particles
 template <class E>
-__global__ void k_flip_mark(E* __restrict__ m, long n, unsigned int* __restrict__ keep) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const bool k = (m[i] == E(0));
-        m[i] = k ? E(1) : E(0);
-        keep[i] = k ? 1u : 0u;
+__global__ void __launch_bounds__(CT_BLOCK) k_flip_mark(E* __restrict__ m, long n, unsigned char* __restrict__ keep,
+                                                        unsigned int* __restrict__ part) {
+    const long base = (long)blockIdx.x * CT_TILE;
+    unsigned int cnt = 0;
+    for (int k = 0; k < CT_ITEMS; ++k) {
+        const long i = base + (long)k * CT_BLOCK + threadIdx.x;
+        if (i < n) {
+            const bool kp = (m[i] == E(0));
+            m[i] = kp ? E(1) : E(0);
+            keep[i] = kp ? 1 : 0;
+            cnt += kp ? 1u : 0u;
+        }
     }
+    cnt = block_sum<unsigned int, CT_BLOCK>(cnt);
+    if (threadIdx.x == 0) part[blockIdx.x] = cnt;
 }
 
-__global__ void k_compact_scatter(ColSet C, long n, const unsigned int* __restrict__ keep,
-                                  const unsigned int* __restrict__ off) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        if (!keep[i]) continue;
-        const long d = off[i];
-        for (int c = 0; c < C.nc; ++c) {
+// one column element moved from slot i to slot d
+__device__ __forceinline__ void move_cols(const ColSet& C, long i, long d) {
+    for (int c = 0; c < C.nc; ++c) {
             switch (C.wsize[c]) {
                 case 4: ((unsigned int*)C.dst[c])[d] = ((const unsigned int*)C.src[c])[i]; break;
                 case 8: ((unsigned long long*)C.dst[c])[d] = ((const unsigned long long*)C.src[c])[i]; break;
@@ -58,7 +72,35 @@ __global__ void k_compact_scatter(ColSet C, long n, const unsigned int* __restri
                     t[1] = s[1];
                 }
             }
+    }
+}
+
+// every kept particle of the tile to its slot: the tile's base from the scanned
+// counts, the rank within the tile from warp ballots (kept particles keep their order)
+__global__ void __launch_bounds__(CT_BLOCK) k_compact_scatter(ColSet C, long n, const unsigned char* __restrict__ keep,
+                                                              const unsigned int* __restrict__ part) {
+    __shared__ unsigned int wcnt[CT_BLOCK / 32];
+    __shared__ unsigned int carry;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long base = (long)blockIdx.x * CT_TILE;
+    if (threadIdx.x == 0) carry = part[blockIdx.x];
+    __syncthreads();
+    for (int k = 0; k < CT_ITEMS; ++k) {
+        const long i = base + (long)k * CT_BLOCK + threadIdx.x;
+        const bool kp = i < n && keep[i];
+        const unsigned int bal = __ballot_sync(0xffffffffu, kp);
+        if (lane == 0) wcnt[w] = __popc(bal);
+        __syncthreads();
+        unsigned int before = 0, tot = 0;
+        for (int q = 0; q < CT_BLOCK / 32; ++q) {
+            const unsigned int c = wcnt[q];
+            before += q < w ? c : 0u;
+            tot += c;
         }
+        if (kp) move_cols(C, i, (long)carry + before + __popc(bal & ((1u << lane) - 1u)));
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
     }
 }
 
@@ -109,21 +151,22 @@ int pd_remove_marked(pd_vd h, int prop, void* stream) {
     const long n = h->n_real;
     if (n == 0) return PD_OK;
     if (n >= (1L << 32)) return PD_EINVAL;
-    // flags and offsets
-    PD_TRY(h->tmp2.ensure(sizeof(unsigned int) * 2 * (size_t)n));
-    unsigned int* keep = h->tmp2.as<unsigned int>();
-    unsigned int* off = keep + n;
-    const unsigned g = grid_for(n, 256);
+    // keep bytes and the per-tile counts (scanned in place); the total to n_keep
+    const long nt = (n + CT_TILE - 1) / CT_TILE;
+    PD_TRY(h->tmp2.ensure((size_t)n + sizeof(unsigned int) * (size_t)nt + 16));
+    unsigned char* keep = h->tmp2.as<unsigned char>();
+    unsigned int* part = reinterpret_cast<unsigned int*>(keep + (((size_t)n + 15) & ~(size_t)15));
+    const unsigned g = (unsigned)nt;
     switch (M.type) {
-        case PD_F64: pd::launch(k_flip_mark<double>, g, 256, 0, st, (double*)M.d, n, keep); break;
-        case PD_F32: pd::launch(k_flip_mark<float>, g, 256, 0, st, (float*)M.d, n, keep); break;
-        case PD_I32: pd::launch(k_flip_mark<int>, g, 256, 0, st, (int*)M.d, n, keep); break;
-        case PD_U32: pd::launch(k_flip_mark<unsigned int>, g, 256, 0, st, (unsigned int*)M.d, n, keep); break;
-        case PD_I64: pd::launch(k_flip_mark<long long>, g, 256, 0, st, (long long*)M.d, n, keep); break;
+        case PD_F64: pd::launch(k_flip_mark<double>, g, CT_BLOCK, 0, st, (double*)M.d, n, keep, part); break;
+        case PD_F32: pd::launch(k_flip_mark<float>, g, CT_BLOCK, 0, st, (float*)M.d, n, keep, part); break;
+        case PD_I32: pd::launch(k_flip_mark<int>, g, CT_BLOCK, 0, st, (int*)M.d, n, keep, part); break;
+        case PD_U32: pd::launch(k_flip_mark<unsigned int>, g, CT_BLOCK, 0, st, (unsigned int*)M.d, n, keep, part); break;
+        case PD_I64: pd::launch(k_flip_mark<long long>, g, CT_BLOCK, 0, st, (long long*)M.d, n, keep, part); break;
         default: return PD_EINVAL;
     }
     PD_LAUNCH_CHECK();
-    PD_TRY(scan_u32(keep, off, n, &h->ctrl->n_keep, h->scan_scratch, st));
+    PD_TRY(scan_partials(part, nt, &h->ctrl->n_keep, st));
     // the kept particles go straight into new storage of the same capacity, which
     // then replaces the old (the reference swaps its compacted vectors in,
     // vector_dist_cuda_funcs.cuh:405-418); after the first call the storage comes
@@ -159,7 +202,7 @@ int pd_remove_marked(pd_vd h, int prop, void* stream) {
             C.dst[c - c0] = cols[c].d;
             C.wsize[c - c0] = cols[c].w;
         }
-        pd::launch(k_compact_scatter, g, 256, 0, st, C, n, (const unsigned int*)keep, (const unsigned int*)off);
+        pd::launch(k_compact_scatter, g, CT_BLOCK, 0, st, C, n, (const unsigned char*)keep, (const unsigned int*)part);
         if (cudaGetLastError() != cudaSuccess) rc = PD_ECUDA;
     }
     if (rc == PD_OK && cudaMemcpyAsync(&h->ctrl_h->n_keep, &h->ctrl->n_keep, sizeof(unsigned int),

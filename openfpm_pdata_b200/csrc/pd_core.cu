@@ -284,6 +284,13 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_apply(const unsigned int* _
     }
 }
 
+int scan_partials(unsigned int* part, long nb, unsigned int* total_dev, cudaStream_t st) {
+    if (nb <= 0) return PD_OK;
+    pd::launch(k_scan_partials, 1, 1024, 0, st, part, nb, total_dev);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
 int scan_u32(const unsigned int* in, unsigned int* out, long n, unsigned int* total_dev, Buf& scratch,
              cudaStream_t st) {
     if (n <= 0) {

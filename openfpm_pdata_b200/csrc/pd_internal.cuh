@@ -102,6 +102,8 @@ inline int type_size(int t) {
     }
 }
 
+// exclusive scan, in place, of nb per-block partial counts (one block); the total to *total_dev
+int scan_partials(unsigned int* part, long nb, unsigned int* total_dev, cudaStream_t st);
 // exclusive scan of n uint32 values (in may equal out); writes the total to *total_dev
 int scan_u32(const unsigned int* in, unsigned int* out, long n, unsigned int* total_dev, Buf& scratch,
              cudaStream_t st);
