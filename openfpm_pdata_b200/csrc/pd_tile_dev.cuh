@@ -136,6 +136,51 @@ __device__ __forceinline__ void tile_segb(const TileSh& S, unsigned int (*segb)[
     }
 }
 
+// Row entries of particle i (global index; FP32 copy x) from the staged candidates
+// [qb, qe), staging indices, candidate q at sm[q - base].  Candidates go in chunks
+// of up to 32: the test of a chunk only shifts the sign of d2 - lo_thr (surely in)
+// and of d2 - hi_thr (possibly in) into two masks, the first candidate ending in
+// the highest bit (fl(a - b) < 0 exactly when a < b for finite a, b); the few band
+// candidates are then decided exactly and the accepted ones appended in ascending
+// q, so the row is the one of the candidate-by-candidate walk.  c counts the row's
+// entries, pend holds the first half of an unfinished word.
+template <class T>
+__device__ __forceinline__ void seg_rows(const float4* __restrict__ sm, unsigned int base, unsigned int qb,
+                                         unsigned int qe, const float4 x, unsigned int i,
+                                         const typename V4<T>::type* __restrict__ pos, T r2, float lo_thr,
+                                         float hi_thr, unsigned int* __restrict__ out, long stride, int max_nn,
+                                         int& c, unsigned int& pend) {
+#pragma unroll 1
+    for (unsigned int q0 = qb; q0 < qe; q0 += 32) {
+        const unsigned int n = min(32u, qe - q0);
+        const float4* c4 = sm + (q0 - base);
+        unsigned int m = 0, h = 0;
+#pragma unroll 4
+        for (unsigned int k = 0; k < n; ++k) {
+            const float4 xq = c4[k];
+            const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
+            m = __funnelshift_l(__float_as_uint(d2 - lo_thr), m, 1);
+            h = __funnelshift_l(__float_as_uint(d2 - hi_thr), h, 1);
+        }
+        // bit n-1-k stands for candidate q0 + k
+        unsigned int band = h & ~m;
+        while (band) {
+            const int b = 31 - __clz(band);
+            band ^= 1u << b;
+            if (exact_in<T>(pos, i, __float_as_int(c4[n - 1 - b].w), r2)) m |= 1u << b;
+        }
+        while (m) {
+            const int b = 31 - __clz(m);
+            m ^= 1u << b;
+            const unsigned int q = q0 + n - 1 - (unsigned int)b;
+            const bool odd = (c & 1) != 0;
+            if (odd && c < max_nn) out[(long)(c >> 1) * stride] = pend | (q << 16);
+            pend = odd ? pend : q;
+            ++c;
+        }
+    }
+}
+
 // List build of one staged tile.  The candidates are staged as FP32 copies; d2
 // in FP32 decides every pair farther than `band` from r^2 (|d2_f32 - d2_exact| <
 // band by the error bound computed on the host), the few inside the band are
@@ -159,21 +204,9 @@ __device__ __forceinline__ void tile_rows(const TileSh& S, const unsigned int (*
         unsigned int pend = 0;
         unsigned int* out = nbr + i;
 #pragma unroll 1
-        for (int sg = 0; sg < 18; ++sg) {
-            const unsigned int qe = segb[sg][j + 2];
-#pragma unroll 4
-            for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
-                const float4 xq = sm[q];
-                const float d2 = dist2(xi.x - xq.x, xi.y - xq.y, xi.z - xq.z);
-                // accept without a divergent branch (the rare band candidates aside)
-                bool acc = d2 < lo_thr;
-                if (!acc && d2 < hi_thr) acc = exact_in<T>(pos, i, __float_as_int(xq.w), r2);
-                const bool odd = (cnt & 1) != 0;
-                if (acc && odd && cnt < max_nn) out[(long)(cnt >> 1) * stride] = pend | (q << 16);
-                pend = (acc && !odd) ? q : pend;
-                cnt += acc ? 1 : 0;
-            }
-        }
+        for (int sg = 0; sg < 18; ++sg)
+            seg_rows<T>(sm, 0, segb[sg][j - 1], segb[sg][j + 2], xi, i, pos, r2, lo_thr, hi_thr, out, stride, max_nn,
+                        cnt, pend);
         // odd rows end with the particle itself, which the pair kernel skips
         if ((cnt & 1) && cnt < max_nn) out[(long)(cnt >> 1) * stride] = pend | ((self_base + i) << 16);
         if (cnt > max_nn) {
@@ -258,22 +291,9 @@ __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned
             unsigned int pd_ = pend[m];
             unsigned int* out = nbr + i;
 #pragma unroll 1
-            for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg) {
-                const unsigned int qe = segb[sg][j + 2];
-#pragma unroll 4
-                for (unsigned int q = segb[sg][j - 1]; q < qe; ++q) {
-                    const float4 xq = sm[q - base];
-                    const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
-                    // accept without a divergent branch (the rare band candidates aside):
-                    // the pending half-word and the count by selects, the word store predicated
-                    bool acc = d2 < lo_thr;
-                    if (!acc && d2 < hi_thr) acc = exact_in<T>(pos, i, __float_as_int(xq.w), r2);
-                    const bool odd = (c & 1) != 0;
-                    if (acc && odd && c < max_nn) out[(long)(c >> 1) * stride] = pd_ | (q << 16);
-                    pd_ = (acc && !odd) ? q : pd_;
-                    c += acc ? 1 : 0;
-                }
-            }
+            for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg)
+                seg_rows<T>(sm, base, segb[sg][j - 1], segb[sg][j + 2], x, i, pos, r2, lo_thr, hi_thr, out, stride,
+                            max_nn, c, pd_);
             cnt[m] = c;
             pend[m] = pd_;
         }
