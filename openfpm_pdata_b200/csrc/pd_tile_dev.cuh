@@ -136,14 +136,40 @@ __device__ __forceinline__ void tile_segb(const TileSh& S, unsigned int (*segb)[
     }
 }
 
+// Accept masks of one chunk of n <= 32 staged candidates (c4[0..n)) for the
+// particle at x: the sign of d2 - lo_thr (surely in) and of d2 - hi_thr (possibly
+// in) shifted in, the first candidate ending in the highest bit: bit n-1-k stands
+// for c4[k] (fl(a - b) < 0 exactly when a < b for finite a, b).  The few band
+// candidates are decided exactly in the position type.
+template <class T>
+__device__ __forceinline__ unsigned int chunk_mask(const float4* __restrict__ c4, unsigned int n, const float4 x,
+                                                   unsigned int i, const typename V4<T>::type* __restrict__ pos,
+                                                   T r2, float lo_thr, float hi_thr) {
+    unsigned int m = 0, h = 0;
+#pragma unroll 4
+    for (unsigned int k = 0; k < n; ++k) {
+        const float4 xq = c4[k];
+        const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
+        m = __funnelshift_l(__float_as_uint(d2 - lo_thr), m, 1);
+        h = __funnelshift_l(__float_as_uint(d2 - hi_thr), h, 1);
+    }
+    unsigned int band = h & ~m;
+    while (band) {
+        const int b = 31 - __clz(band);
+        band ^= 1u << b;
+        if (exact_in<T>(pos, i, __float_as_int(c4[n - 1 - b].w), r2)) m |= 1u << b;
+    }
+    return m;
+}
+
 // Row entries of particle i (global index; FP32 copy x) from the staged candidates
-// [qb, qe), staging indices, candidate q at sm[q - base].  Candidates go in chunks
-// of up to 32: the test of a chunk only shifts the sign of d2 - lo_thr (surely in)
-// and of d2 - hi_thr (possibly in) into two masks, the first candidate ending in
-// the highest bit (fl(a - b) < 0 exactly when a < b for finite a, b); the few band
-// candidates are then decided exactly and the accepted ones appended in ascending
-// q, so the row is the one of the candidate-by-candidate walk.  c counts the row's
-// entries, pend holds the first half of an unfinished word.
+// [qb, qe), staging indices, candidate q at sm[q - base], appended in ascending q
+// (the entries of the candidate-by-candidate walk, in its order).  Up to three
+// chunks of 32 are tested into masks first; their accepted candidates then leave
+// as one stream, two entries (one 32-bit word) at a time, so a lane's loop runs
+// about half its accept count rather than the sum of the chunks' largest counts
+// over the warp.  c counts the row's entries, pend holds the first half of an
+// unfinished word.
 template <class T>
 __device__ __forceinline__ void seg_rows(const float4* __restrict__ sm, unsigned int base, unsigned int qb,
                                          unsigned int qe, const float4 x, unsigned int i,
@@ -151,31 +177,41 @@ __device__ __forceinline__ void seg_rows(const float4* __restrict__ sm, unsigned
                                          float hi_thr, unsigned int* __restrict__ out, long stride, int max_nn,
                                          int& c, unsigned int& pend) {
 #pragma unroll 1
-    for (unsigned int q0 = qb; q0 < qe; q0 += 32) {
-        const unsigned int n = min(32u, qe - q0);
+    for (unsigned int q0 = qb; q0 < qe; q0 += 96) {
+        const unsigned int n = min(96u, qe - q0);
+        const unsigned int na = min(32u, n), nb = min(32u, n - na), nc = n - na - nb;
         const float4* c4 = sm + (q0 - base);
-        unsigned int m = 0, h = 0;
-#pragma unroll 4
-        for (unsigned int k = 0; k < n; ++k) {
-            const float4 xq = c4[k];
-            const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
-            m = __funnelshift_l(__float_as_uint(d2 - lo_thr), m, 1);
-            h = __funnelshift_l(__float_as_uint(d2 - hi_thr), h, 1);
+        unsigned int ma = chunk_mask<T>(c4, na, x, i, pos, r2, lo_thr, hi_thr);
+        unsigned int mb = chunk_mask<T>(c4 + 32, nb, x, i, pos, r2, lo_thr, hi_thr);
+        unsigned int mc = chunk_mask<T>(c4 + 64, nc, x, i, pos, r2, lo_thr, hi_thr);
+        // candidate of bit b of a mask: qt - 31 + clz position, qt = last q of the chunk
+        unsigned int qa = q0 + na - 32, qb_ = q0 + 32 + nb - 32, qc = q0 + 64 + nc - 32;
+        int rem = __popc(ma) + __popc(mb) + __popc(mc);
+        if (rem == 0) continue;
+        // the stream: ma first; an emptied mask takes the next one's place
+        if (ma == 0) { ma = mb; qa = qb_; mb = mc; qb_ = qc; mc = 0; }
+        if (ma == 0) { ma = mb; qa = qb_; mb = 0; }
+        if (mb == 0) { mb = mc; qb_ = qc; mc = 0; }
+        auto next = [&]() -> unsigned int {
+            const int z = __clz(ma);
+            const unsigned int q = qa + (unsigned int)z;
+            ma ^= 0x80000000u >> z;
+            if (ma == 0) { ma = mb; qa = qb_; mb = mc; qb_ = qc; mc = 0; }
+            return q;
+        };
+        if (c & 1) {  // complete the pending word
+            const unsigned int q = next();
+            if (c < max_nn) out[(long)(c >> 1) * stride] = pend | (q << 16);
+            ++c;
+            --rem;
         }
-        // bit n-1-k stands for candidate q0 + k
-        unsigned int band = h & ~m;
-        while (band) {
-            const int b = 31 - __clz(band);
-            band ^= 1u << b;
-            if (exact_in<T>(pos, i, __float_as_int(c4[n - 1 - b].w), r2)) m |= 1u << b;
+        for (; rem >= 2; rem -= 2, c += 2) {
+            const unsigned int q1 = next();
+            const unsigned int q2 = next();
+            if (c < max_nn) out[(long)(c >> 1) * stride] = q1 | (q2 << 16);
         }
-        while (m) {
-            const int b = 31 - __clz(m);
-            m ^= 1u << b;
-            const unsigned int q = q0 + n - 1 - (unsigned int)b;
-            const bool odd = (c & 1) != 0;
-            if (odd && c < max_nn) out[(long)(c >> 1) * stride] = pend | (q << 16);
-            pend = odd ? pend : q;
+        if (rem) {
+            pend = next();
             ++c;
         }
     }
