@@ -247,18 +247,41 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
     tile_layout(tg, blockIdx.x, csR, csI, S);
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     double pe = 0, vir = 0;
-    bool staged = ib != ie && tile_stage<float>(reinterpret_cast<const float4*>(xy),
-                                                reinterpret_cast<const float4*>(xy + n_real), S,
-                                                reinterpret_cast<float4*>(sxy), cap, err);
-    if (staged) {
-        const int nc = S.ncol - 1;
-        for (int r = 0; r < 9; ++r) {
-            const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
-            for (unsigned int k = threadIdx.x; k < lr; k += blockDim.x) sz[S.oR[r] + k] = __ldg(zz + S.cR[r][0] + k);
-            for (unsigned int k = threadIdx.x; k < li; k += blockDim.x)
-                sz[S.oI[r] + k] = __ldg(zz + n_real + S.cI[r][0] + k);
+    // (x, y) by bulk copies; the CTA loads z while they are in flight
+    bool staged = false;
+    if (ib != ie) {
+        if (S.total > cap) {
+            if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+        } else {
+            const int nc = S.ncol - 1;
+            if (threadIdx.x == 0) {
+                mbar_init(&S.bar, 1);
+                mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(double2));
+                for (int r = 0; r < 9; ++r) {
+                    const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
+                    if (lr) bulk_g2s(sxy + S.oR[r], xy + S.cR[r][0], lr * (unsigned int)sizeof(double2), &S.bar);
+                    if (li)
+                        bulk_g2s(sxy + S.oI[r], xy + n_real + S.cI[r][0], li * (unsigned int)sizeof(double2), &S.bar);
+                }
+            }
+            for (int r = 0; r < 9; ++r) {
+                const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
+                for (unsigned int k = threadIdx.x; k < lr; k += blockDim.x)
+                    sz[S.oR[r] + k] = __ldg(zz + S.cR[r][0] + k);
+                for (unsigned int k = threadIdx.x; k < li; k += blockDim.x)
+                    sz[S.oI[r] + k] = __ldg(zz + n_real + S.cI[r][0] + k);
+            }
+            // every thread waits on the barrier only after thread 0 initialised it
+            __syncthreads();
+            bool ok = mbar_wait_bounded(&S.bar, 0, 1u << 24);
+            if (!ok) {
+                atomicOr(err, ERR_TIMEOUT);
+                mbar_wait_bounded(&S.bar, 0, 1u << 24);  // let copies in flight land before the CTA exits
+            }
+            staged = __syncthreads_and(ok ? 1 : 0) != 0;
         }
-        __syncthreads();
+    }
+    if (staged) {
         const unsigned int base = S.oR[4] - S.cR[4][0];
         unsigned int first = ib;
         while (first < ie) {
@@ -276,6 +299,26 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             const int Q = (int)q;
             double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             const unsigned int* row = nbr + i;
+            // one pair (rows hold the particle itself, as the reference's full list
+            // does): outside the cutoff or self, s6 is zero and with it the force,
+            // energy and virial terms -- one select instead of three
+            auto pair_term = [&](unsigned int l) {
+                const double2 xyq = sxy[l];
+                const double dx = xyi.x - xyq.x, dy = xyi.y - xyq.y, dz = zi - sz[l];
+                const double r2 = dist2(dx, dy, dz);
+                const bool in = r2 < Pr.rc2 && l != li;
+                const double ir2 = recip(in ? r2 : 1.0);
+                const double s2 = Pr.sig2 * ir2;
+                const double s6 = in ? s2 * s2 * s2 : 0.0;
+                const double ff = ir2 * s6 * fma(2.0 * Pr.eps24, s6, -Pr.eps24);  // 24 eps (2 s12 - s6) / r2
+                fx = fma(ff, dx, fx);
+                fy = fma(ff, dy, fy);
+                fz = fma(ff, dz, fz);
+                if (ENERGY) {
+                    e = fma(s6, fma(Pr.eps4, s6, -Pr.eps4), e);  // 4 eps (s12 - s6)
+                    w = fma(ff, r2, w);
+                }
+            };
             unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
             unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
             unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
@@ -287,25 +330,8 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
                 q1 = q2;
                 q2 = q3;
                 q3 = k + 4 * Q < words ? __ldg(row + (long)(k + 4 * Q) * stride) : 0u;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const unsigned int l = h ? (pair >> 16) : (pair & 0xffffu);
-                    const double2 xyq = sxy[l];
-                    const double dx = xyi.x - xyq.x, dy = xyi.y - xyq.y, dz = zi - sz[l];
-                    const double r2 = dist2(dx, dy, dz);
-                    const bool in = r2 < Pr.rc2 && l != li;
-                    const double ir2 = recip(in ? r2 : 1.0);
-                    const double s2 = Pr.sig2 * ir2;
-                    const double s6 = s2 * s2 * s2;
-                    const double ff = in ? Pr.eps24 * ir2 * s6 * (2.0 * s6 - 1.0) : 0.0;
-                    fx += ff * dx;
-                    fy += ff * dy;
-                    fz += ff * dz;
-                    if (ENERGY) {
-                        e += in ? Pr.eps4 * s6 * (s6 - 1.0) : 0.0;
-                        w += ff * r2;
-                    }
-                }
+                pair_term(pair & 0xffffu);
+                pair_term(pair >> 16);
             }
             for (unsigned int o = 1; o < q; o <<= 1) {
                 fx += __shfl_xor_sync(0xffffffffu, fx, o);
