@@ -58,49 +58,72 @@ __global__ void __launch_bounds__(CT_BLOCK) k_flip_mark(E* __restrict__ m, long 
     if (threadIdx.x == 0) part[blockIdx.x] = cnt;
 }
 
-// one column element moved from slot i to slot d
-__device__ __forceinline__ void move_cols(const ColSet& C, long i, long d) {
-    for (int c = 0; c < C.nc; ++c) {
-            switch (C.wsize[c]) {
-                case 4: ((unsigned int*)C.dst[c])[d] = ((const unsigned int*)C.src[c])[i]; break;
-                case 8: ((unsigned long long*)C.dst[c])[d] = ((const unsigned long long*)C.src[c])[i]; break;
-                case 16: ((uint4*)C.dst[c])[d] = ((const uint4*)C.src[c])[i]; break;
-                default: {
-                    const uint4* s = (const uint4*)C.src[c] + 2 * i;
-                    uint4* t = (uint4*)C.dst[c] + 2 * d;
-                    t[0] = s[0];
-                    t[1] = s[1];
-                }
-            }
-    }
-}
-
 // every kept particle of the tile to its slot: the tile's base from the scanned
-// counts, the rank within the tile from warp ballots (kept particles keep their order)
+// counts, the rank within the tile from warp ballots (kept particles keep their
+// order).  The ballots of all CT_ITEMS passes are taken first and their counts
+// scanned once over (pass, warp), so the tile needs two barriers, not three a pass.
 __global__ void __launch_bounds__(CT_BLOCK) k_compact_scatter(ColSet C, long n, const unsigned char* __restrict__ keep,
                                                               const unsigned int* __restrict__ part) {
-    __shared__ unsigned int wcnt[CT_BLOCK / 32];
-    __shared__ unsigned int carry;
+    constexpr int NW = CT_BLOCK / 32, NC = CT_ITEMS * NW;  // counts in (pass, warp) order
+    __shared__ unsigned int cnt[NC];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long base = (long)blockIdx.x * CT_TILE;
-    if (threadIdx.x == 0) carry = part[blockIdx.x];
-    __syncthreads();
+    unsigned int bal[CT_ITEMS];
+#pragma unroll
     for (int k = 0; k < CT_ITEMS; ++k) {
         const long i = base + (long)k * CT_BLOCK + threadIdx.x;
-        const bool kp = i < n && keep[i];
-        const unsigned int bal = __ballot_sync(0xffffffffu, kp);
-        if (lane == 0) wcnt[w] = __popc(bal);
-        __syncthreads();
-        unsigned int before = 0, tot = 0;
-        for (int q = 0; q < CT_BLOCK / 32; ++q) {
-            const unsigned int c = wcnt[q];
-            before += q < w ? c : 0u;
-            tot += c;
+        bal[k] = __ballot_sync(0xffffffffu, i < n && keep[i]);
+        if (lane == 0) cnt[k * NW + w] = __popc(bal[k]);
+    }
+    __syncthreads();
+    // exclusive scan of the NC counts by warp 0 (NC / 32 per lane, then the lanes')
+    if (w == 0) {
+        constexpr int PER = NC / 32;
+        unsigned int v[PER], s = 0;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            v[j] = cnt[lane * PER + j];
+            s += v[j];
         }
-        if (kp) move_cols(C, i, (long)carry + before + __popc(bal & ((1u << lane) - 1u)));
-        __syncthreads();
-        if (threadIdx.x == 0) carry += tot;
-        __syncthreads();
+        unsigned int incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        unsigned int run = part[blockIdx.x] + incl - s;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            cnt[lane * PER + j] = run;
+            run += v[j];
+        }
+    }
+    __syncthreads();
+    unsigned int d[CT_ITEMS];  // (n < 2^32)
+    unsigned int kept = 0;
+#pragma unroll
+    for (int k = 0; k < CT_ITEMS; ++k) {
+        kept |= (bal[k] >> lane & 1u) << k;
+        d[k] = cnt[k * NW + w] + __popc(bal[k] & ((1u << lane) - 1u));
+    }
+    // one particle at a time, column by column: at 32 registers four CTAs of 512 fit
+    // an SM, which keeps more loads in flight than fewer threads holding several each
+    for (int k = 0; k < CT_ITEMS; ++k) {
+        if (!(kept >> k & 1u)) continue;
+        const long i = base + (long)k * CT_BLOCK + threadIdx.x;
+        for (int c = 0; c < C.nc; ++c) {
+            switch (C.wsize[c]) {
+                case 4: ((unsigned int*)C.dst[c])[d[k]] = ((const unsigned int*)C.src[c])[i]; break;
+                case 8: ((unsigned long long*)C.dst[c])[d[k]] = ((const unsigned long long*)C.src[c])[i]; break;
+                case 16: ((uint4*)C.dst[c])[d[k]] = ((const uint4*)C.src[c])[i]; break;
+                default: {
+                    const uint4* s4 = (const uint4*)C.src[c] + 2 * i;
+                    uint4* t4 = (uint4*)C.dst[c] + 2 * (long)d[k];
+                    t4[0] = s4[0];
+                    t4[1] = s4[1];
+                }
+            }
+        }
     }
 }
 
@@ -157,25 +180,33 @@ int pd_remove_marked(pd_vd h, int prop, void* stream) {
     unsigned char* keep = h->tmp2.as<unsigned char>();
     unsigned int* part = reinterpret_cast<unsigned int*>(keep + (((size_t)n + 15) & ~(size_t)15));
     const unsigned g = (unsigned)nt;
+    // the kept particles go straight into new storage of the same capacity, which
+    // then replaces the old (the reference swaps its compacted vectors in,
+    // vector_dist_cuda_funcs.cuh:405-418); after the first call the storage comes
+    // from the library's block cache.  It is taken before the first launch: taking
+    // a block freed since the last synchronisation synchronises the device, which
+    // between the launches would stall them.  The scatter needs no count on the
+    // host, so flip, scan and scatter run back to back and the call synchronises once.
+    void* np = nullptr;
+    int* ng = nullptr;
+    std::vector<char*> nprops;
+    PD_TRY(alloc_storage(h, h->cap, &np, &ng, nprops));
     switch (M.type) {
         case PD_F64: pd::launch(k_flip_mark<double>, g, CT_BLOCK, 0, st, (double*)M.d, n, keep, part); break;
         case PD_F32: pd::launch(k_flip_mark<float>, g, CT_BLOCK, 0, st, (float*)M.d, n, keep, part); break;
         case PD_I32: pd::launch(k_flip_mark<int>, g, CT_BLOCK, 0, st, (int*)M.d, n, keep, part); break;
         case PD_U32: pd::launch(k_flip_mark<unsigned int>, g, CT_BLOCK, 0, st, (unsigned int*)M.d, n, keep, part); break;
         case PD_I64: pd::launch(k_flip_mark<long long>, g, CT_BLOCK, 0, st, (long long*)M.d, n, keep, part); break;
-        default: return PD_EINVAL;
+        default:
+            free_storage(np, ng, nprops);
+            return PD_EINVAL;
     }
-    PD_LAUNCH_CHECK();
-    PD_TRY(scan_partials(part, nt, &h->ctrl->n_keep, st));
-    // the kept particles go straight into new storage of the same capacity, which
-    // then replaces the old (the reference swaps its compacted vectors in,
-    // vector_dist_cuda_funcs.cuh:405-418); after the first call the storage comes
-    // from the library's block cache.  The scatter needs no count on the host, so
-    // flip, scan and scatter run back to back and the call synchronises once.
-    void* np = nullptr;
-    int* ng = nullptr;
-    std::vector<char*> nprops;
-    PD_TRY(alloc_storage(h, h->cap, &np, &ng, nprops));
+    if (cudaGetLastError() != cudaSuccess || scan_partials(part, nt, &h->ctrl->n_keep, st) != PD_OK) {
+        cudaStreamSynchronize(st);
+        free_storage(np, ng, nprops);
+        set_error("remove_marked: the compaction kernels failed");
+        return PD_ECUDA;
+    }
     struct Col {
         const unsigned char* s;
         unsigned char* d;

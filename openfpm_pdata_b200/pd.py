@@ -559,11 +559,19 @@ class VectorDist:
         """remove_marked<p>(): drop the domain particles whose property p is non-zero."""
         check(lib().pd_remove_marked(self.h, int(p), None))
 
-    def get_indexes_by_type(self, p, value, cmp=CMP_EQ, end=None):
-        """get_indexes_by_type<p, functor>(): ascending indexes i < end with prop p `cmp` value."""
+    def get_indexes_by_type(self, p, value, cmp=CMP_EQ, end=None, device=False):
+        """get_indexes_by_type<p, functor>(): ascending indexes i < end with prop p `cmp` value;
+        device=True returns them in a CUDA int32 tensor (device memory, as the reference's
+        vector_gpu), else in a host uint32 array."""
         n = ctypes.c_long(0)
         e = -1 if end is None else int(end)
         cap = self.size_local_with_ghost()
+        if device:
+            import torch
+            t = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
+            check(lib().pd_get_indexes_by_type(self.h, int(p), int(cmp), int(value), e,
+                                               ctypes.c_void_p(t.data_ptr()), cap, ctypes.byref(n), None))
+            return t[: n.value]
         ids = np.zeros(max(cap, 1), np.uint32)
         check(lib().pd_get_indexes_by_type(self.h, int(p), int(cmp), int(value), e, _ptr(ids), cap,
                                            ctypes.byref(n), None))

@@ -127,3 +127,6 @@ def test_get_indexes_by_type(pd, orc):
     assert np.array_equal(vd.get_indexes_by_type(0, 1, end=1234), orc.indexes_by_type(t, 1234, 0, 1))
     assert np.array_equal(vd.get_indexes_by_type(0, 1, end=m), orc.indexes_by_type(t, m, 0, 1))
     assert vd.get_indexes_by_type(0, 7).shape[0] == 0
+    # the indexes in device memory (a CUDA tensor) are the same
+    dev = vd.get_indexes_by_type(0, 1, device=True)
+    assert dev.is_cuda and np.array_equal(dev.cpu().numpy().astype(np.uint32), ids)
