@@ -237,7 +237,8 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
                                                            const unsigned int* __restrict__ csR,
                                                            const unsigned int* __restrict__ csI, unsigned int cap,
                                                            const unsigned int* __restrict__ nbr,
-                                                           const int* __restrict__ nn, long stride, LJP<double> Pr,
+                                                           const int* __restrict__ nn, long stride, int mwords,
+                                                           LJP<double> Pr,
                                                            double* __restrict__ f, long fcap,
                                                            double* __restrict__ part, unsigned int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char tile_raw[];
@@ -295,10 +296,16 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             const unsigned int li = base + i;
             const double2 xyi = sxy[li];
             const double zi = sz[li];
-            const int words = active ? (nn[i] + 1) >> 1 : 0;
             const int Q = (int)q;
-            double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             const unsigned int* row = nbr + i;
+            // the first row words are read together with the row length (within the
+            // buffer's mwords words per particle), not after it
+            unsigned int q0 = sub < mwords ? __ldg(row + (long)sub * stride) : 0u;
+            unsigned int q1 = sub + Q < mwords ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+            unsigned int q2 = sub + 2 * Q < mwords ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+            unsigned int q3 = sub + 3 * Q < mwords ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
+            const int words = active ? (nn[i] + 1) >> 1 : 0;
+            double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             // one pair (rows hold the particle itself, as the reference's full list
             // does): outside the cutoff or self, s6 is zero and with it the force,
             // energy and virial terms -- one select instead of three
@@ -319,10 +326,6 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
                     w = fma(ff, r2, w);
                 }
             };
-            unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
-            unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
-            unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
-            unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
 #pragma unroll 2
             for (int k = sub; k < words; k += Q) {
                 const unsigned int pair = q0;
@@ -558,10 +561,11 @@ static int launch_lj_xyz(pd_vd h, const TileGeom& tg, long ntiles, const unsigne
     }
     int smem = (int)(cap * 24);
     if (smem < 32) smem = 32;
+    const int mwords = (int)std::min<long>((long)(nbr.bytes / (4 * (size_t)stride)), 1L << 30);
     PD_TRY(allow_smem(k_vtile_lj_xyz<E, P, MINB>, smem));
     pd::launch(k_vtile_lj_xyz<E, P, MINB>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
                (const double2*)sxy.as<double2>(), (const double*)sz.as<double>(), h->n_real, tg, csR, csI, cap,
-               nbr.as<unsigned int>(), nn.as<int>(), stride, LP, f, h->cap, part, &h->ctrl->err);
+               nbr.as<unsigned int>(), nn.as<int>(), stride, mwords, LP, f, h->cap, part, &h->ctrl->err);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
