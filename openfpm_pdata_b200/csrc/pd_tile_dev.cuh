@@ -136,28 +136,35 @@ __device__ __forceinline__ void tile_segb(const TileSh& S, unsigned int (*segb)[
     }
 }
 
-// Accept masks of one chunk of n <= 32 staged candidates (c4[0..n)) for the
-// particle at x: the sign of d2 - lo_thr (surely in) and of d2 - hi_thr (possibly
-// in) shifted in, the first candidate ending in the highest bit: bit n-1-k stands
-// for c4[k] (fl(a - b) < 0 exactly when a < b for finite a, b).  The few band
-// candidates are decided exactly in the position type.
+// Accept mask of one chunk of n <= 32 staged candidates (c4[0..n)) for the
+// particle at x: the sign of t = d2 - lo_thr (surely in) shifted in, the first
+// candidate ending in the highest bit: bit n-1-k stands for c4[k] (fl(a - b) < 0
+// exactly when a < b for finite a, b).  Candidates possibly in (lo_thr <= d2 <
+// hi_thr) have 0 <= t <= fl(hi_thr - lo_thr); non-negative floats order like
+// their bit patterns and negative ones have the sign bit, so a running unsigned
+// minimum of the patterns flags them, one instruction a candidate.  The rare
+// flagged chunk is walked again and its band candidates decided exactly in the
+// position type.
 template <class T>
 __device__ __forceinline__ unsigned int chunk_mask(const float4* __restrict__ c4, unsigned int n, const float4 x,
                                                    unsigned int i, const typename V4<T>::type* __restrict__ pos,
                                                    T r2, float lo_thr, float hi_thr) {
-    unsigned int m = 0, h = 0;
+    unsigned int m = 0, umin = 0xffffffffu;
 #pragma unroll 4
     for (unsigned int k = 0; k < n; ++k) {
         const float4 xq = c4[k];
         const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
-        m = __funnelshift_l(__float_as_uint(d2 - lo_thr), m, 1);
-        h = __funnelshift_l(__float_as_uint(d2 - hi_thr), h, 1);
+        const unsigned int t = __float_as_uint(d2 - lo_thr);
+        m = __funnelshift_l(t, m, 1);
+        umin = min(umin, t);
     }
-    unsigned int band = h & ~m;
-    while (band) {
-        const int b = 31 - __clz(band);
-        band ^= 1u << b;
-        if (exact_in<T>(pos, i, __float_as_int(c4[n - 1 - b].w), r2)) m |= 1u << b;
+    if (umin <= __float_as_uint(hi_thr - lo_thr)) {
+        for (unsigned int k = 0; k < n; ++k) {
+            const float4 xq = c4[k];
+            const float d2 = dist2(x.x - xq.x, x.y - xq.y, x.z - xq.z);
+            if (!(d2 < lo_thr) && d2 < hi_thr && exact_in<T>(pos, i, __float_as_int(xq.w), r2))
+                m |= 1u << (n - 1 - k);
+        }
     }
     return m;
 }
