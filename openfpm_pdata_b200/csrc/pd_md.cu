@@ -508,7 +508,20 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
         PD_TRY(gather_bytes(h->img_shift.p, h->tmp2.p, ids, m, 1, st));
         PD_CUDA(cudaMemcpyAsync(h->img_shift.p, h->tmp2.p, (size_t)m, cudaMemcpyDeviceToDevice, st));
     }
-    PD_TRY(tile_plan(cl, n, md->tile_tx, md->tg, md->ntiles));
+    int tx_req = md->tile_tx;
+    if (tx_req == 0 && md->physics == 0) {
+        // LJ: the widest tile with at most about 184 domain particles on average, from
+        // the occupancy of the cells inside the box (the grid's ghost layers hold
+        // images only).  A CTA of 256 threads at two lanes a particle takes 128 in a
+        // first round; a second round of up to 64 runs at four lanes each, so most
+        // lanes are busy in both while tiles stay below 192 (the rows are about
+        // equally long).
+        double inner = 1;
+        for (int d = 0; d < 3; ++d) inner *= std::max(1.0, (h->hi[d] - h->lo[d]) / cl->spacing[d]);
+        const double occ = std::max((double)n / inner, 1e-3);
+        tx_req = std::max(1, std::min(TXMAX, (int)(184.0 / occ)));
+    }
+    PD_TRY(tile_plan(cl, n, tx_req, md->tg, md->ntiles));
     unsigned int tmax = 0, cmax = 0;
     for (;;) {
         PD_TRY(tile_sizes(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), tmax, cmax,
