@@ -303,6 +303,13 @@ template <typename St> class vector_dist_gpu {
         ids.resize((size_t)n);
         return ids;
     }
+    // the same into caller-owned device memory of `cap` entries (as the reference's
+    // vector_gpu keeps them on the device); returns the number of indexes
+    long get_indexes_by_type(int prp, int cmp, long long value, unsigned int* ids_dev, long cap, long end = -1) {
+        long n = 0;
+        check(pd_get_indexes_by_type(h_, prp, cmp, value, end, ids_dev, cap, &n, stream_));
+        return n;
+    }
     void updateVerlet(VerletList& vl) {
         check(pd_verlet_update(h_, vl.handle(), stream_));
         vl.set_size(size_local());
