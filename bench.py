@@ -708,9 +708,10 @@ def main():
         "clocks": ck,
     }
 
-    if rank == 0 and world == 1 and not a.no_e2e:
+    if not a.no_e2e:
         # end to end through the public C ABI: pinned host buffers in, K steps, energies and
-        # final state out; wall clock around create + H2D + run + D2H
+        # final state out; wall clock around create + H2D + run + D2H (every rank its own
+        # replica on its own GPU; the job's time is the slowest rank's)
         # host data in the ABI's layouts (positions [n][3], velocities [3][n]) in pinned memory
         xp = torch.from_numpy(x).pin_memory().numpy()
         vt = np.ascontiguousarray(v.T.astype(np.float32 if mixed else np.float64))
@@ -748,10 +749,12 @@ def main():
         # process's first device allocations of this size wait on the driver for a time
         # that depends on what ran on the GPU before it (measured 6 to 300 ms)
         w_s, w_ms = e2e_pass(max(a.warmup, 2))
+        barrier()
         t_e2e, e2e_ms = e2e_pass(a.steps)
-        out["e2e"] = {"value": n * a.steps / t_e2e, "unit": METRIC,
-                      "h2d_bytes_per_step": (x.nbytes + v.nbytes) / a.steps,
-                      "d2h_bytes_per_step": 32 + (xo.nbytes + vo.nbytes) / a.steps,
+        t_e2e = max_over_ranks(t_e2e * 1000.0, pg, "cuda") / 1000.0
+        out["e2e"] = {"value": world * n * a.steps / t_e2e, "unit": METRIC,
+                      "h2d_bytes_per_step": world * (x.nbytes + v.nbytes) / a.steps,
+                      "d2h_bytes_per_step": world * (32 + (xo.nbytes + vo.nbytes) / a.steps),
                       "includes": "create, H2D of positions+velocities from pinned memory, first list build, "
                                   "K steps, per-step energies and final state D2H into pinned memory; "
                                   "after one untimed warm-up pass of the same calls",
