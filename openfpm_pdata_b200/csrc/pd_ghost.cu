@@ -51,7 +51,8 @@ __global__ void k_ghost_count(const typename V4<T>::type* __restrict__ pos, long
         typename V4<T>::type r = ld4(pos, p);
         unsigned int c = 0;
         int old = -1;
-        for (int i = 0; i < B.nb; ++i) {
+        const int nb = in_core(B, r.x, r.y, r.z) ? 0 : B.nb;
+        for (int i = 0; i < nb; ++i) {
             int s = B.sv[i];
             if (inside_np(B, i, r.x, r.y, r.z) && s != old) {
                 old = s;
@@ -77,7 +78,8 @@ __global__ void k_ghost_write(typename V4<T>::type* __restrict__ pos, int* __res
         typename V4<T>::type r = ld4(pos, p);
         long m = start[p];
         int old = -1;
-        for (int i = 0; i < B.nb; ++i) {
+        const int nb = in_core(B, r.x, r.y, r.z) ? 0 : B.nb;
+        for (int i = 0; i < nb; ++i) {
             int s = B.sv[i];
             if (inside_np(B, i, r.x, r.y, r.z) && s != old) {
                 old = s;
@@ -173,6 +175,7 @@ template <class T> static int domain_boxes(pd_vd h, BoxSet<T>& B, T* shifts) {
         g[d] = (T)h->g[d];
     }
     B.nb = 0;
+    B.core = 0;
     for (int l = 0; l < 27; ++l) {
         int c[3] = {l % 3 - 1, (l / 3) % 3 - 1, l / 9 - 1};
         for (int d = 0; d < 3; ++d)
@@ -202,8 +205,37 @@ template <class T> static int domain_boxes(pd_vd h, BoxSet<T>& B, T* shifts) {
     return B.nb;
 }
 
-template <class T> static int upload_boxes_t(pd_vd h, const BoxSet<T>& B, const T* shifts, int n_shifts,
+// The core of a box set inside the domain: on each axis, between the highest box
+// upper edge at or below the middle and the lowest box lower edge at or above it
+// (boxes across the middle leave that axis open).  Kept only if it is not empty and
+// every box misses it on some axis, so that no point of it lies in a box.
+template <class T> static void box_core(pd_vd h, BoxSet<T>& B) {
+    B.core = 0;
+    if (B.nb <= 0) return;
+    for (int d = 0; d < 3; ++d) {
+        const T lo = (T)h->lo[d], hi = (T)h->hi[d], mid = lo + (hi - lo) / T(2);
+        T cl = lo, ch = hi;
+        for (int i = 0; i < B.nb; ++i) {
+            if (B.hi[i][d] <= mid && B.hi[i][d] > cl) cl = B.hi[i][d];
+            if (B.lo[i][d] >= mid && B.lo[i][d] < ch) ch = B.lo[i][d];
+        }
+        if (!(cl < ch)) return;
+        B.clo[d] = cl;
+        B.chi[d] = ch;
+    }
+    for (int i = 0; i < B.nb; ++i) {
+        bool misses = false;
+        for (int d = 0; d < 3; ++d)
+            if (B.hi[i][d] <= B.clo[d] || B.lo[i][d] >= B.chi[d]) misses = true;
+        if (!misses) return;
+    }
+    B.core = 1;
+}
+
+template <class T> static int upload_boxes_t(pd_vd h, const BoxSet<T>& B_in, const T* shifts, int n_shifts,
                                              cudaStream_t st) {
+    BoxSet<T> B = B_in;
+    box_core(h, B);
     PD_TRY(h->boxes.ensure(sizeof(BoxSet<T>)));
     PD_TRY(h->shifts.ensure(sizeof(T) * 3 * (n_shifts > 27 ? n_shifts : 27)));
     PD_CUDA(cudaMemcpyAsync(h->boxes.p, &B, sizeof(BoxSet<T>), cudaMemcpyHostToDevice, st));
