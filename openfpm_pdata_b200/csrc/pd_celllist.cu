@@ -1,3 +1,4 @@
+#include <utility>
 // pd_celllist.cu -- GPU cell list: geometry, counting-sort build, reorder / restoreOrder,
 // and the reference's test pair functor walking getNNIteratorBox.
 //
@@ -235,8 +236,59 @@ int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, 
     return PD_OK;
 }
 
+// The gather of a reorder straight into the vector's spare storage, which then
+// takes the place of the storage (every column moved once, not gathered into
+// scratch and copied back).  Slots from n_part on hold the spare's old contents and
+// views taken before are stale: for a caller that rewrites the slots past n_part
+// (the images) and moves the epoch on, and not inside a stream capture (the
+// capture would keep the first pair of addresses).
+static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask, bool with_pos, bool with_gid,
+                        cudaStream_t st) {
+    if (n <= 0) return PD_OK;
+    if (!h->spare_pos || h->spare_cap != h->cap || h->spare_props.size() != h->props.size()) {
+        free_storage(h->spare_pos, h->spare_gid, h->spare_props);
+        h->spare_pos = nullptr;
+        h->spare_gid = nullptr;
+        h->spare_props.clear();
+        h->spare_cap = 0;
+        PD_TRY(alloc_storage(h, h->cap, &h->spare_pos, &h->spare_gid, h->spare_props));
+        h->spare_cap = h->cap;
+    }
+    const unsigned g = grid_for(n, 256);
+    if (with_pos) {
+        if (h->dtype == PD_F64)
+            pd::launch(k_gather4<double>, g, 256, 0, st, (const double4*)h->pos, (double4*)h->spare_pos, ids, n);
+        else
+            pd::launch(k_gather4<float>, g, 256, 0, st, (const float4*)h->pos, (float4*)h->spare_pos, ids, n);
+        PD_LAUNCH_CHECK();
+        std::swap(h->pos, h->spare_pos);
+    }
+    if (with_gid) {
+        pd::launch(k_gather<int>, g, 256, 0, st, (const int*)h->gid, h->spare_gid, ids, n);
+        PD_LAUNCH_CHECK();
+        std::swap(h->gid, h->spare_gid);
+    }
+    for (size_t p = 0; p < h->props.size(); ++p) {
+        if (!(prop_mask & (1ul << p))) continue;
+        Prop& P = h->props[p];
+        for (int c = 0; c < P.ncomp; ++c) {
+            const size_t o = (size_t)c * h->cap * P.esize;
+            if (P.esize == 8)
+                pd::launch(k_gather<long long>, g, 256, 0, st, (const long long*)(P.d + o),
+                           (long long*)(h->spare_props[p] + o), ids, n);
+            else
+                pd::launch(k_gather<int>, g, 256, 0, st, (const int*)(P.d + o), (int*)(h->spare_props[p] + o), ids, n);
+            PD_LAUNCH_CHECK();
+        }
+        std::swap(P.d, h->spare_props[p]);
+    }
+    return PD_OK;
+}
+
 int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
-               cudaStream_t st) {
+               cudaStream_t st, bool swap) {
+    if (swap && !g_capturing && !g_alloc_ctx)
+        return permute_swap(h, cl->sorted.as<int>(), n_part, prop_mask, with_pos, with_gid, st);
     return permute(h, cl->sorted.as<int>(), n_part, prop_mask, with_pos, with_gid, false, st);
 }
 

@@ -388,6 +388,12 @@ int ensure_capacity(pd_vd h, long need, cudaStream_t st) {
         dev_free(h->props[p].d);
         h->props[p].d = nprops[p];
     }
+    // a spare of the old capacity no longer fits
+    free_storage(h->spare_pos, h->spare_gid, h->spare_props);
+    h->spare_pos = nullptr;
+    h->spare_gid = nullptr;
+    h->spare_props.clear();
+    h->spare_cap = 0;
     h->pos = np;
     h->gid = ng;
     h->cap = ncap;
@@ -547,6 +553,7 @@ int pd_destroy(pd_vd h) {
     dev_free(h->pos);
     dev_free(h->gid);
     for (auto& P : h->props) dev_free(P.d);
+    free_storage(h->spare_pos, h->spare_gid, h->spare_props);
     h->img_src.release();
     h->img_shift.release();
     h->img_cnt.release();

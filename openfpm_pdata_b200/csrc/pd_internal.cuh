@@ -155,6 +155,12 @@ struct pd_vd_s {
     pd::Ctrl* ctrl = nullptr;    // device
     pd::Ctrl* ctrl_h = nullptr;  // pinned host mirror
     pd::Buf scan_scratch, tmp, tmp2, red;
+    // spare storage of the same capacity: a reorder gathers into it and swaps it in
+    // (cl_reorder with swap); allocated on first use, freed with the storage
+    void* spare_pos = nullptr;
+    int* spare_gid = nullptr;
+    std::vector<char*> spare_props;
+    long spare_cap = 0;
     long epoch = 0;
     // slab decomposition (pd_slab.cu): the rows of the last labelling, in send
     // order (slot of each row, shift code of each halo row), and the halo
@@ -214,7 +220,7 @@ int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cud
 // gather src[ids[k]] -> dst[k] for k < n of 4/8/16/32-byte elements (dst may not alias src)
 int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, cudaStream_t st);
 int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
-               cudaStream_t st);
+               cudaStream_t st, bool swap = false);
 int ghost_boxes_upload(pd_vd h, cudaStream_t st);
 int ghost_generate(pd_vd h, long img_cap, bool sync_count, cudaStream_t st);
 int ghost_replay(pd_vd h, unsigned long prop_mask, bool with_pos, const unsigned int* n_img_dev, long n_img_bound,

@@ -572,7 +572,7 @@ int md_rebuild(pd_md md, cudaStream_t st) {
     PD_TRY(cl_build(h, sort_cl, h->n_real, nullptr, st));
     unsigned long mask = 1ul << md->mp.vel_prop;
     if (md->physics == 1) mask |= (1ul << md->sp.rho_prop) | (1ul << md->sp.type_prop);
-    PD_TRY(cl_reorder(h, sort_cl, h->n_real, mask, true, true, st));
+    PD_TRY(cl_reorder(h, sort_cl, h->n_real, mask, true, true, st, md->swap_reorder));
     if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
     PD_TRY(ghost_generate(h, 0, true, st));
     if (md->mp.use_cell_list) {

@@ -8,6 +8,9 @@
 
 struct pd_md_s {
     pd_vd h = nullptr;
+    // the rebuild's reorder swaps the vector's spare storage in (single-system driver;
+    // off where device pointers are kept in tables, the serving loop)
+    bool swap_reorder = true;
     pd_lj_params_t lj;
     pd_md_params_t mp;
     pd_vl vl = nullptr;   // Verlet list (r_cut + skin)

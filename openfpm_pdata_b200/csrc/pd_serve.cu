@@ -1418,6 +1418,7 @@ static int slot_reset(pd_srv s, SrvSlot& sl, SrvReq* r, const SrvShape& shape) {
         mp.force_prop = sl.fp;
         mp.precision = PD_PREC_MIXED;
         PD_TRY(pd_md_create(sl.h, &s->lj, &mp, &sl.md));
+        sl.md->swap_reorder = false;  // the slot tables keep the vector's device pointers
     } else {
         pd_vd h = sl.h;
         pd_md md = sl.md;
