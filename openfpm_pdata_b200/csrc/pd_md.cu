@@ -920,6 +920,15 @@ int pd_sph_create(pd_vd h, const pd_sph_params_t* sp, const pd_md_params_t* mp, 
 
 int pd_md_destroy(pd_md md) {
     if (!md) return PD_EINVAL;
+    if (md->swap_reorder && md->h) {
+        // the reorder's spare storage lives with the vector; without a driver it has no use
+        pd_vd h = md->h;
+        free_storage(h->spare_pos, h->spare_gid, h->spare_props);
+        h->spare_pos = nullptr;
+        h->spare_gid = nullptr;
+        h->spare_props.clear();
+        h->spare_cap = 0;
+    }
     if (md->vl) pd_verlet_destroy(md->vl);
     if (md->cl) pd_celllist_destroy(md->cl);
     md->xb.release();
