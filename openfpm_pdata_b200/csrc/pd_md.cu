@@ -562,6 +562,17 @@ static bool md_split(pd_md md) {
     return md->physics == 0 && !md->mixed && md->tiles_active && !md->mp.use_cell_list && md->h->dtype == PD_F64;
 }
 
+// The properties the cell-order reorder carries: all but those the step recomputes
+// before it reads them (the force; for SPH also the density rate), so that every
+// other property stays with its particle.
+static unsigned long md_reorder_mask(pd_md md) {
+    const int np = (int)md->h->props.size();
+    unsigned long m = np >= 64 ? ~0ul : ((1ul << np) - 1);
+    m &= ~(1ul << md->mp.force_prop);
+    if (md->physics == 1) m &= ~(1ul << md->sp.drho_prop);
+    return m;
+}
+
 int md_rebuild(pd_md md, cudaStream_t st) {
     pd_vd h = md->h;
     if (md->mixed && md->off_valid) PD_TRY(mixed_to_positions(h, md->vl->cl, md->off, st));
@@ -570,9 +581,7 @@ int md_rebuild(pd_md md, cudaStream_t st) {
     PD_TRY(wrap_positions(h, h->n_real, st));
     pd_cl sort_cl = md->mp.use_cell_list ? md->cl : md->vl->cl;
     PD_TRY(cl_build(h, sort_cl, h->n_real, nullptr, st));
-    unsigned long mask = 1ul << md->mp.vel_prop;
-    if (md->physics == 1) mask |= (1ul << md->sp.rho_prop) | (1ul << md->sp.type_prop);
-    PD_TRY(cl_reorder(h, sort_cl, h->n_real, mask, true, true, st, md->swap_reorder));
+    PD_TRY(cl_reorder(h, sort_cl, h->n_real, md_reorder_mask(md), true, true, st, md->swap_reorder));
     if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
     PD_TRY(ghost_generate(h, 0, true, st));
     if (md->mp.use_cell_list) {
@@ -650,7 +659,7 @@ static int md_step_cl(pd_md md, cudaStream_t st, long img_cap) {
     h->img_valid = false;
     PD_TRY(wrap_positions(h, n, st));
     PD_TRY(cl_build(h, cl, n, nullptr, st));
-    PD_TRY(cl_reorder(h, cl, n, 1ul << md->mp.vel_prop, true, true, st));
+    PD_TRY(cl_reorder(h, cl, n, md_reorder_mask(md), true, true, st));
     PD_TRY(ghost_generate(h, img_cap, false, st));
     PD_TRY(cl_build(h, cl, n + img_cap, &h->ctrl->n_img, st));
     const long bound = n + img_cap;

@@ -172,3 +172,43 @@ def test_ighost_get_equals_ghost_get(pd):
         b.map()
     b.ghost_wait()
     b.map()
+
+
+def test_md_spare_storage_across_storage_changes(pd):
+    """The MD driver's rebuild reorders into the vector's spare storage and swaps it
+    in, carrying every property but the force with its particle (here an int mark
+    set before the run selects the same particles after it).  Across a compaction
+    (new storage of the same capacity) and a property added afterwards (the spare
+    no longer matches), a second driver on the same vector gives the energies of a
+    driver on a fresh vector holding the same state, bit for bit (the same kernels
+    on the same data)."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(12, 1.1, 0.05, seed=51)
+    n = x.shape[0]
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    props = [(pd.PD_F64, 3), (pd.PD_F64, 3), (pd.PD_I32, 1)]
+    vd = pd.VectorDist(n, lo, hi, bc, 2.8, dtype=F64, props=props)
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    vd.hostToDeviceProp(2, (np.arange(n) % 10 == 3).astype(np.int32))
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
+    md.run(12)
+    del md
+    # the mark followed its particles through the run's reorders (gid = original index)
+    gid = vd.gid(with_ghost=False)
+    assert np.array_equal(vd.deviceToHostProp(2, with_ghost=False), (gid % 10 == 3).astype(np.int32))
+    vd.remove_marked(2)
+    extra = vd.add_prop(pd.PD_F64, 2)
+    m = vd.size_local()
+    assert m == n - int((np.arange(n) % 10 == 3).sum())
+    vd.hostToDeviceProp(extra, np.ones((m, 2)))
+    xs = vd.deviceToHostPos(with_ghost=False)
+    vs = vd.deviceToHostProp(0, with_ghost=False)
+    E1 = pd.MD(vd, 0, 1, dt=0.005, skin=0.3).run(15)
+    fresh = pd.VectorDist(m, lo, hi, bc, 2.8, dtype=F64, props=props + [(pd.PD_F64, 2)])
+    fresh.hostToDevicePos(xs)
+    fresh.hostToDeviceProp(0, vs)
+    E2 = pd.MD(fresh, 0, 1, dt=0.005, skin=0.3).run(15)
+    assert np.isfinite(E1).all()
+    assert np.array_equal(E1, E2)
+    assert np.array_equal(vd.deviceToHostProp(extra, with_ghost=False), np.ones((m, 2)))
