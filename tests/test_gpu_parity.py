@@ -339,21 +339,23 @@ def test_md_tiled_rows_equal_oracle_sets(pd, orc, tx):
         assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), np.sort(eidx[eoff[i]:eoff[i + 1]]))
 
 
-@pytest.mark.parametrize("layout", ["uniform", "dense_half"])
+@pytest.mark.parametrize("layout", ["uniform", "dense_half", "non_cubic"])
 def test_md_tiled_rows_random_layouts(pd, orc, layout):
     """The same on layouts that are not lattices: uniform random positions (tile
-    sizes fluctuate around the automatic width's target) and a box whose left half
+    sizes fluctuate around the automatic width's target), a box whose left half
     is three times as dense as its right (tiles far above the mean take the
-    narrower or single-pass builds)."""
-    rng = np.random.default_rng(41 if layout == "uniform" else 42)
+    narrower or single-pass builds), and a 48 x 30 x 21 box (axes of different
+    cell counts)."""
+    rng = np.random.default_rng({"uniform": 41, "dense_half": 42, "non_cubic": 43}[layout])
     L, n = 40.0, 60000
-    if layout == "uniform":
-        x = rng.uniform(0.0, L, size=(n, 3))
-    else:
+    box = np.array([48.0, 30.0, 21.0]) if layout == "non_cubic" else np.full(3, L)
+    if layout == "dense_half":
         k = 3 * n // 4
         x = np.concatenate([rng.uniform([0, 0, 0], [L / 2, L, L], size=(k, 3)),
                             rng.uniform([L / 2, 0, 0], [L, L, L], size=(n - k, 3))])
-    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    else:
+        x = rng.uniform(0.0, 1.0, size=(n, 3)) * box
+    lo, hi, bc = np.zeros(3), box.copy(), np.ones(3, np.int32)
     vd = make_vd(pd, x, lo, hi, bc, 2.8, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
     vd.hostToDeviceProp(0, np.zeros((n, 3)))
     md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
