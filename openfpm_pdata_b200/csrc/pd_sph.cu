@@ -16,6 +16,8 @@
 // with the same 1-D TMA bulk copies: (x, y, z, p) from the position array (the
 // pressure lives in the position record's fourth word) and (vx, vy, vz, rho)
 // from a packed auxiliary array written by the integrator.
+#include <algorithm>
+
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
                                                         const typename V4<T>::type* __restrict__ aux, TileGeom tg,
                                                         const unsigned int* __restrict__ csR, unsigned int cap,
                                                         const unsigned int* __restrict__ nbr,
-                                                        const int* __restrict__ nn, long stride,
+                                                        const int* __restrict__ nn, long stride, int mwords,
                                                         const int* __restrict__ type, SphK<T> K, T* __restrict__ acc,
                                                         T* __restrict__ drho, long cap_p,
                                                         unsigned int* __restrict__ err) {
@@ -235,14 +237,15 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
         const T4 xi = sp[li];
         const T4 ai = sa[li];
         const T pa_r = xi.w;
+        const unsigned int* row = nbr + i;
+        // row words read four iterations ahead (register shift ring); the first four
+        // together with the row length (within the buffer's mwords words per particle)
+        unsigned int q0 = sub < mwords ? __ldg(row + (long)sub * stride) : 0u;
+        unsigned int q1 = sub + Q < mwords ? __ldg(row + (long)(sub + Q) * stride) : 0u;
+        unsigned int q2 = sub + 2 * Q < mwords ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
+        unsigned int q3 = sub + 3 * Q < mwords ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
         const int words = active ? (nn[i] + 1) >> 1 : 0;
         T ax = 0, ay = 0, az = 0, dr = 0;
-        const unsigned int* row = nbr + i;
-        // row words read four iterations ahead (register shift ring)
-        unsigned int q0 = sub < words ? __ldg(row + (long)sub * stride) : 0u;
-        unsigned int q1 = sub + Q < words ? __ldg(row + (long)(sub + Q) * stride) : 0u;
-        unsigned int q2 = sub + 2 * Q < words ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
-        unsigned int q3 = sub + 3 * Q < words ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
         for (int k = sub; k < words; k += Q) {
             const unsigned int pair = q0;
             q0 = q1;
@@ -389,13 +392,14 @@ static int launch_sph(pd_vd h, const TileGeom& tg, long ntiles, const unsigned i
     typedef typename V4<T>::type T4;
     int smem = (int)(2 * cap * sizeof(T4));
     if (smem < 32) smem = 32;
+    const int mwords = (int)std::min<long>((long)(nbr.bytes / (4 * (size_t)stride)), 1L << 30);
     PD_CUDA(cudaFuncSetAttribute(k_vtile_sph<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const Prop& A = h->props[acc_prop];
     const Prop& D = h->props[sp.drho_prop];
     const Prop& Ty = h->props[sp.type_prop];
     pd::launch(k_vtile_sph<T, P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st, (const T4*)h->pos,
                (const T4*)aux.as<T4>(), tg, csR, cap, (const unsigned int*)nbr.as<unsigned int>(),
-               (const int*)nn.as<int>(), stride, (const int*)Ty.d, sphk<T>(sp), (T*)A.d, (T*)D.d, h->cap,
+               (const int*)nn.as<int>(), stride, mwords, (const int*)Ty.d, sphk<T>(sp), (T*)A.d, (T*)D.d, h->cap,
                &h->ctrl->err);
     PD_LAUNCH_CHECK();
     return PD_OK;
