@@ -28,20 +28,29 @@ __device__ __forceinline__ bool in_cut_exact(float r2, float dx, float dy, float
     return in;
 }
 
-// Reciprocal by Newton-Raphson refinement (Newton's method for f(y) = 1/y - x,
-// y' = y (2 - x y), written as e = 1 - x y, y' = y + y e; each step doubles the
-// correct bits; Markstein, "Computation of elementary functions on the IBM
-// RISC System/6000", IBM J. Res. Dev. 34, 1990).  The seed is the hardware
-// approximation rcp.approx.ftz.f64 (relative error below 2^-20), so two steps
-// reach full double precision (within 2 ulp of 1/x; tests/test_gpu_recip.py).
-// Valid for normal positive arguments, which is what squared pair distances are.
+// Reciprocal from the hardware approximation y0 = rcp.approx.ftz.f64(x), whose
+// relative error |e| = |1 - x y0| is below 2^-20: 1/x = y0 / (1 - e) =
+// y0 (1 + e + e^2 + e^3 + ...), and the series to e^2 leaves e^3 < 2^-60, below
+// the double rounding, so one correction y0 + y0 (e + e^2) -- three fused
+// multiply-adds, cubic convergence where a Newton-Raphson step (y' = y + y e) is
+// quadratic and needs two -- gives the reciprocal within 2 ulp
+// (tests/test_gpu_recip.py; Markstein, "Computation of elementary functions on the
+// IBM RISC System/6000", IBM J. Res. Dev. 34, 1990).  Valid for normal positive
+// arguments, which is what squared pair distances are.
 __device__ __forceinline__ double recip(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
+    const double e = fma(-x, y, 1.0);
+    return fma(fma(e, e, e), y, y);
+}
+// a / x by the same series with a folded into the correction: a y0 (1 + e + e^2).
+// NaN for x = 0 (the caller selects the result away).
+__device__ __forceinline__ double div_by(double a, double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    const double ay = a * y;
+    return fma(fma(e, e, e), ay, ay);
 }
 // FP32: hardware approximation (rcp.approx.ftz.f32, ~1 ulp) plus one refinement step
 __device__ __forceinline__ float recip(float x) {
@@ -49,6 +58,16 @@ __device__ __forceinline__ float recip(float x) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     float e = fmaf(-x, y, 1.0f);
     return fmaf(y, e, y);
+}
+
+// FP32 a / x: the approximation is within about 1 ulp, so one correction a y0 (1 + e)
+// leaves e^2 below the float rounding.  NaN for x = 0 (the caller selects it away).
+__device__ __forceinline__ float div_by(float a, float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    const float e = fmaf(-x, y, 1.0f);
+    const float ay = a * y;
+    return fmaf(e, ay, ay);
 }
 
 template <class T>

@@ -115,6 +115,7 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
     }
     const int ncol = S.ncol;
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][ncol - 2];
+    const float c24 = Pr.eps24 / Pr.sig2;
     bool ok = ib != ie && S.total <= cap;
     if (ib != ie && S.total > cap) {
         if (ovf_cnt) {
@@ -213,14 +214,16 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
                     const bool wall = in && r2 < Pr.rclose2 && nd < MIXED_KDEF;
                     if (wall) defer[nd++][threadIdx.x] = (unsigned short)l;
                     const bool in32 = in && !wall;
-                    const float ir2 = recip(in32 ? r2 : 1.f);
-                    const float s2 = Pr.sig2 * ir2;
+                    // s2 zero outside (NaN for the particle itself, selected away) zeroes
+                    // the force, energy and virial terms; 1 / r2 enters as s2 / sig2
+                    const float s2v = div_by(Pr.sig2, r2);
+                    const float s2 = in32 ? s2v : 0.f;
                     const float s6 = s2 * s2 * s2;
-                    const float ff = in32 ? Pr.eps24 * ir2 * s6 * (2.f * s6 - 1.f) : 0.f;
+                    const float ff = s2 * s6 * fmaf(2.f * c24, s6, -c24);  // 24 eps (2 s12 - s6) / r2
                     fx += ff * dx;
                     fy += ff * dy;
                     fz += ff * dz;
-                    e += in32 ? Pr.eps4 * s6 * (s6 - 1.f) : 0.f;
+                    e = fmaf(s6, fmaf(Pr.eps4, s6, -Pr.eps4), e);  // 4 eps (s12 - s6)
                     w += ff * r2;
                 }
                 kx.add(fx);

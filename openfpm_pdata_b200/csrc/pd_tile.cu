@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
     __shared__ TileSh S;
     tile_layout(tg, blockIdx.x, csR, csI, S);
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
+    const double c24 = Pr.eps24 / Pr.sig2;
     double pe = 0, vir = 0;
     // (x, y) by bulk copies; the CTA loads z while they are in flight
     bool staged = false;
@@ -307,17 +308,18 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             const int words = active ? (nn[i] + 1) >> 1 : 0;
             double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             // one pair (rows hold the particle itself, as the reference's full list
-            // does): outside the cutoff or self, s6 is zero and with it the force,
-            // energy and virial terms -- one select instead of three
+            // does): outside the cutoff or self, s2 is zero and with it the force,
+            // energy and virial terms -- one select; 1 / r2 enters the force as
+            // s2 / sig2 (c24 = 24 eps / sig2)
             auto pair_term = [&](unsigned int l) {
                 const double2 xyq = sxy[l];
                 const double dx = xyi.x - xyq.x, dy = xyi.y - xyq.y, dz = zi - sz[l];
                 const double r2 = dist2(dx, dy, dz);
                 const bool in = r2 < Pr.rc2 && l != li;
-                const double ir2 = recip(in ? r2 : 1.0);
-                const double s2 = Pr.sig2 * ir2;
-                const double s6 = in ? s2 * s2 * s2 : 0.0;
-                const double ff = ir2 * s6 * fma(2.0 * Pr.eps24, s6, -Pr.eps24);  // 24 eps (2 s12 - s6) / r2
+                const double s2v = div_by(Pr.sig2, r2);  // NaN for the particle itself, selected away
+                const double s2 = in ? s2v : 0.0;
+                const double s6 = s2 * s2 * s2;
+                const double ff = s2 * s6 * fma(2.0 * c24, s6, -c24);  // 24 eps (2 s12 - s6) / r2
                 fx = fma(ff, dx, fx);
                 fy = fma(ff, dy, fy);
                 fz = fma(ff, dz, fz);
