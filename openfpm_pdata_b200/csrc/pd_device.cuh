@@ -18,6 +18,8 @@ __device__ __forceinline__ double4 ld4(const double4* p, long i) {
     return make_double4(a.x, a.y, b.x, b.y);
 }
 __device__ __forceinline__ float4 ld4(const float4* p, long i) { return __ldg(p + i); }
+// bring the line holding *p into L2 (no register result)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void st4(double4* p, long i, double4 v) {
     double2* q = reinterpret_cast<double2*>(p + i);
     q[0] = make_double2(v.x, v.y);
@@ -163,6 +165,22 @@ template <class T, int BLOCK> __device__ __forceinline__ T block_sum(T v) {
     }
     __syncthreads();
     return r;  // valid in thread 0
+}
+
+// block maximum of non-negative values (valid in thread 0)
+template <class T, int BLOCK> __device__ __forceinline__ T block_max(T v) {
+    __shared__ T sh[BLOCK / 32];
+    v = warp_max(v);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    T r = 0;
+    if (w == 0) {
+        r = (l < BLOCK / 32) ? sh[l] : T(0);
+        r = warp_max(r);
+    }
+    __syncthreads();
+    return r;
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double v) {

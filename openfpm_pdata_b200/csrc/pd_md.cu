@@ -9,6 +9,7 @@
 // Velocity Verlet (Swope et al. 1982): v += dt/2 f/m; x += dt v; [rebuild or
 // refresh images]; f = F(x); v += dt/2 f/m.  Energies are reduced in FP64 with a
 // fixed block order (deterministic).
+#include <utility>
 #include "pd_device.cuh"
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
@@ -336,6 +337,45 @@ __global__ void k_sum_pairs(const double* __restrict__ in, long n, long chunk, d
     }
 }
 
+// the same for (pe, vir, ke) triples: out[3b + q]
+__global__ void k_sum_triples(const double* __restrict__ in, long n, long chunk, double* __restrict__ out) {
+    double a = 0, b = 0, c = 0;
+    long beg = (long)blockIdx.x * chunk, end = min(beg + chunk, n);
+    for (long i = beg + threadIdx.x; i < end; i += 256) {
+        a += in[3 * i];
+        b += in[3 * i + 1];
+        c += in[3 * i + 2];
+    }
+    a = block_sum<double, 256>(a);
+    b = block_sum<double, 256>(b);
+    c = block_sum<double, 256>(c);
+    if (threadIdx.x == 0) {
+        out[3 * blockIdx.x] = a;
+        out[3 * blockIdx.x + 1] = b;
+        out[3 * blockIdx.x + 2] = c;
+    }
+}
+
+// E = (KE, PE, virial, rebuilt) from nb (pe, vir, ke) triples
+__global__ void k_energy3(const double* __restrict__ part, int nb, const unsigned int* __restrict__ rebuilt,
+                          double* __restrict__ E) {
+    double a = 0, b = 0, c = 0;
+    for (int i = threadIdx.x; i < nb; i += 256) {
+        a += part[3 * i + 2];
+        b += part[3 * i];
+        c += part[3 * i + 1];
+    }
+    a = block_sum<double, 256>(a);
+    b = block_sum<double, 256>(b);
+    c = block_sum<double, 256>(c);
+    if (threadIdx.x == 0) {
+        E[0] = a;
+        E[1] = b;
+        E[2] = c;
+        E[3] = rebuilt ? (double)*rebuilt : 0.0;
+    }
+}
+
 // E[s] = (KE, PE, virial, rebuilt) from the fixed-order partials
 __global__ void k_energy(const double* __restrict__ fpart, int nbf, const double* __restrict__ kpart, int nbk,
                          const unsigned int* __restrict__ rebuilt, double* __restrict__ E) {
@@ -550,7 +590,7 @@ static int md_tiles(pd_md md, pd_cl cl, cudaStream_t st) {
     md->tcap = tmax;
     PD_TRY(tile_build(h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                       md->vl->r_cut, md->pos32, md->tnbr, md->tnn, md->tstride, md->tmax_nn, st));
-    PD_TRY(md->tpart.ensure(sizeof(double) * 2 * ((md->ntiles > 0 ? md->ntiles : 1) + 256)));
+    PD_TRY(md->tpart.ensure(sizeof(double) * 3 * ((md->ntiles > 0 ? md->ntiles : 1) + 256)));
     md->tiles_active = true;
     return PD_OK;
 }
@@ -616,7 +656,11 @@ int md_rebuild(pd_md md, cudaStream_t st) {
     return PD_OK;
 }
 
-int md_forces(pd_md md, cudaStream_t st) {
+int md_forces(pd_md md, cudaStream_t st, const DriftArgs* drift) {
+    if (drift && !(md->tiles_active && md->physics == 0 && !md->mixed)) {
+        set_error("md_forces: the fused drift is the plain tiled path's");
+        return PD_EINVAL;
+    }
     if (md->physics == 1)
         return sph_rates(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->tcap, md->tnbr, md->tnn,
                          md->tstride, md->aux, md->sp, md->mp.force_prop, md->tile_p, st);
@@ -627,7 +671,7 @@ int md_forces(pd_md md, cudaStream_t st) {
     if (md->tiles_active)
         return tile_lj(md->h, md->tg, md->ntiles, md->csR.as<unsigned int>(), md->csI.as<unsigned int>(), md->tcap,
                        md->tnbr, md->tnn, md->tstride, md->lj, md->mp.force_prop, md->tpart.as<double>(), true,
-                       md->tile_p, md->sxy, md->sz, st);
+                       md->tile_p, md->sxy, md->sz, st, drift);
     return lj_launch(md->h, md->mp.use_cell_list ? nullptr : md->vl, md->mp.use_cell_list ? md->cl : nullptr, md->lj,
                      md->mp.force_prop, md->fpart.as<double>(), md->nblk, st);
 }
@@ -952,6 +996,8 @@ int pd_md_destroy(pd_md md) {
     md->pos32.release();
     md->sxy.release();
     md->sz.release();
+    md->sxy2.release();
+    md->sz2.release();
     md->off.release();
     md->offb.release();
     md->offK.release();
@@ -981,6 +1027,18 @@ static int md_energy(pd_md md, int s, cudaStream_t st) {
                    (const double*)md->kpart.as<double>(), md->nblk, (const unsigned int*)&h->ctrl->rebuild,
                    md->E.as<double>() + 4 * s);
     }
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+// energies of step s from the per-tile (pe, vir, ke) triples of a pair kernel that drifted
+static int md_energy_drift(pd_md md, int s, cudaStream_t st) {
+    const int nb2 = 256;
+    long chunk = (md->ntiles + nb2 - 1) / nb2;
+    double* stage = md->tpart.as<double>() + 3 * md->ntiles;
+    pd::launch(k_sum_triples, nb2, 256, 0, st, (const double*)md->tpart.as<double>(), md->ntiles, chunk, stage);
+    pd::launch(k_energy3, 1, 256, 0, st, (const double*)stage, nb2, (const unsigned int*)&md->h->ctrl->rebuild,
+               md->E.as<double>() + 4 * s);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
@@ -1022,41 +1080,47 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         unsigned int rebuilt = 0;
         const bool split = md_split(md);  // the drift also refreshes the pair kernel's staging copies
         PD_EV(0);
-        PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-        if (fused && s > 0 && md->mixed) {
-            PD_TRY(mixed_kick_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
-                                         md->mp.dt, md->mp.mass, md->kpart.as<double>(), st));
-            PD_TRY(md_energy(md, s - 1, st));
-        } else if (fused && s > 0) {
-            if (h->dtype == PD_F64)
-                pd::launch(k_kick_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos,
-                           (const double4*)md->xb.as<double4>(), (double*)V.d, (const double*)F.d, h->cap, n, half,
-                           md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), split ? md->sxy.as<double>() : nullptr,
-                           split ? md->sz.as<double>() : nullptr);
+        if (md->drifted) {
+            // the previous step's pair kernel made this step's kick and drift (and the
+            // previous step's closing kick and energies)
+            md->drifted = false;
+        } else {
+            PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
+            if (fused && s > 0 && md->mixed) {
+                PD_TRY(mixed_kick_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+                                             md->mp.dt, md->mp.mass, md->kpart.as<double>(), st));
+                PD_TRY(md_energy(md, s - 1, st));
+            } else if (fused && s > 0) {
+                if (h->dtype == PD_F64)
+                    pd::launch(k_kick_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos,
+                               (const double4*)md->xb.as<double4>(), (double*)V.d, (const double*)F.d, h->cap, n, half,
+                               md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), split ? md->sxy.as<double>() : nullptr,
+                               split ? md->sz.as<double>() : nullptr);
+                else
+                    pd::launch(k_kick_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos,
+                               (const float4*)md->xb.as<float4>(), (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
+                               (float)md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), (float*)nullptr,
+                               (float*)nullptr);
+                PD_LAUNCH_CHECK();
+                PD_TRY(md_energy(md, s - 1, st));
+            } else if (md->physics == 1)
+                PD_TRY(sph_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
+                                      md->mp.dt, st));
+            else if (md->mixed)
+                PD_TRY(mixed_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
+                                        md->mp.dt, st));
+            else if (h->dtype == PD_F64)
+                pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,
+                                                                  (const double*)F.d, h->cap, n, half, md->mp.dt,
+                                                                  &h->ctrl->maxdisp2, split ? md->sxy.as<double>() : nullptr,
+                                                                  split ? md->sz.as<double>() : nullptr);
             else
-                pd::launch(k_kick_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos,
-                           (const float4*)md->xb.as<float4>(), (float*)V.d, (const float*)F.d, h->cap, n, (float)half,
-                           (float)md->mp.dt, md->mp.mass, &h->ctrl->maxdisp2, md->kpart.as<double>(), (float*)nullptr,
-                           (float*)nullptr);
+                pd::launch(k_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos, md->xb.as<float4>(), (float*)V.d,
+                                                                 (const float*)F.d, h->cap, n, (float)half,
+                                                                 (float)md->mp.dt, &h->ctrl->maxdisp2, (float*)nullptr,
+                                                                 (float*)nullptr);
             PD_LAUNCH_CHECK();
-            PD_TRY(md_energy(md, s - 1, st));
-        } else if (md->physics == 1)
-            PD_TRY(sph_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
-                                  md->mp.dt, st));
-        else if (md->mixed)
-            PD_TRY(mixed_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
-                                    md->mp.dt, st));
-        else if (h->dtype == PD_F64)
-            pd::launch(k_kick_drift<double>, md->nblk, FBLOCK, 0, st, (double4*)h->pos, md->xb.as<double4>(), (double*)V.d,
-                                                              (const double*)F.d, h->cap, n, half, md->mp.dt,
-                                                              &h->ctrl->maxdisp2, split ? md->sxy.as<double>() : nullptr,
-                                                              split ? md->sz.as<double>() : nullptr);
-        else
-            pd::launch(k_kick_drift<float>, md->nblk, FBLOCK, 0, st, (float4*)h->pos, md->xb.as<float4>(), (float*)V.d,
-                                                             (const float*)F.d, h->cap, n, (float)half,
-                                                             (float)md->mp.dt, &h->ctrl->maxdisp2, (float*)nullptr,
-                                                             (float*)nullptr);
-        PD_LAUNCH_CHECK();
+        }
         PD_EV(1);
         bool rb = md->mp.skin <= 0 || md->mp.use_cell_list;
         if (!rb) {
@@ -1078,14 +1142,32 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             if (split) PD_TRY(tile_split(h, md->sxy, md->sz, h->n_real, h->n_img, st));
         }
         PD_EV(3);
-        PD_TRY(md_forces(md, st));
+        // plain FP64 tiled steps with a next step in this run: the pair kernel also
+        // makes this step's closing kick and the next step's kick and drift, into the
+        // second pair of staging copies, which then become the current ones
+        const bool drift = fused && !md->mixed && md_split(md) && s + 1 < steps;
+        if (drift) {
+            const size_t cap = (size_t)(h->cap > 0 ? h->cap : 1);
+            PD_TRY(md->sxy2.ensure(cap * sizeof(double2)));
+            PD_TRY(md->sz2.ensure(cap * sizeof(double)));
+            PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
+            DriftArgs D{(double4*)h->pos, md->xb.as<const double4>(), (double*)V.d, h->cap, half, md->mp.dt,
+                        md->mp.mass, md->sxy2.as<double2>(), md->sz2.as<double>(), &h->ctrl->maxdisp2};
+            PD_TRY(md_forces(md, st, &D));
+            std::swap(md->sxy, md->sxy2);
+            std::swap(md->sz, md->sz2);
+            md->drifted = true;
+        } else {
+            PD_TRY(md_forces(md, st));
+        }
         PD_EV(4);
         if (md->timing) rebuilt_at[s] = (unsigned char)rebuilt;
         if (fused) {
-            // the rebuild flag of this step, read by its energies at the next launch
+            // the rebuild flag of this step, read by its energies
             h->ctrl_h->rebuild = rebuilt;
             PD_CUDA(cudaMemcpyAsync(&h->ctrl->rebuild, &h->ctrl_h->rebuild, sizeof(unsigned int),
                                     cudaMemcpyHostToDevice, st));
+            if (drift) PD_TRY(md_energy_drift(md, s, st));
             md->steps++;
             PD_EV(5);
             continue;

@@ -31,6 +31,8 @@ struct pd_md_s {
     int tmax_nn = 0;
     pd::Buf csR, csI, tnbr, tnn, tpart, pos32;
     pd::Buf sxy, sz;  // FP64 tiled path: the pair kernel's (x, y) / z copies of the positions
+    pd::Buf sxy2, sz2;  // the second pair, written by a pair kernel that also drifts
+    bool drifted = false;  // the last pair kernel made the next step's kick and drift
     // precision form: FP32 cell-local offsets (all particles), their value at the
     // last build (real particles) and the constant parts of the image offsets
     int physics = 0;  // 0: Lennard-Jones, 1: WCSPH
@@ -58,8 +60,9 @@ namespace pd {
 int force_blocks(long n);
 // wrap, sort, periodic images, neighbour structure (and the mixed-form offsets)
 int md_rebuild(pd_md md, cudaStream_t st);
-// forces of the current state into the force property
-int md_forces(pd_md md, cudaStream_t st);
+// forces of the current state into the force property (with `drift`, the plain FP64
+// tiled path's pair kernel also makes the next step's kick and drift instead)
+int md_forces(pd_md md, cudaStream_t st, const DriftArgs* drift = nullptr);
 // cell-list mode of a small system: every step of a run in one thread-block cluster (pd_cluster.cu)
 bool md_cluster_eligible(pd_md md);
 int md_run_cluster(pd_md md, int steps, cudaStream_t st, double* E);

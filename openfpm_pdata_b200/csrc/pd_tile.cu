@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_lj(const typename V4<T>::typ
 // copies and z as 8-byte values loaded by the CTA (their ranges need not start on
 // a 16-byte boundary), 24 bytes a record instead of 32; (x, y) records of
 // consecutive slots fall on all eight 16-byte bank groups.
-template <bool ENERGY, int P, int MINB>
+template <bool ENERGY, int P, int MINB, bool DRIFT>
 __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* __restrict__ xy,
                                                            const double* __restrict__ zz, long n_real, TileGeom tg,
                                                            const unsigned int* __restrict__ csR,
@@ -240,7 +240,9 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
                                                            const int* __restrict__ nn, long stride, int mwords,
                                                            LJP<double> Pr,
                                                            double* __restrict__ f, long fcap,
-                                                           double* __restrict__ part, unsigned int* __restrict__ err) {
+                                                           double* __restrict__ part, unsigned int* __restrict__ err,
+                                                           DriftArgs D) {
+    static_assert(ENERGY || !DRIFT, "the drift's kinetic energy partials ride on the energy partials");
     extern __shared__ __align__(128) unsigned char tile_raw[];
     double2* sxy = reinterpret_cast<double2*>(tile_raw);
     double* sz = reinterpret_cast<double*>(tile_raw + (size_t)cap * sizeof(double2));
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
     tile_layout(tg, blockIdx.x, csR, csI, S);
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     const double c24 = Pr.eps24 / Pr.sig2;
-    double pe = 0, vir = 0;
+    double pe = 0, vir = 0, ke = 0, md2 = 0;
     // (x, y) by bulk copies; the CTA loads z while they are in flight
     bool staged = false;
     if (ib != ie) {
@@ -306,6 +308,14 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             unsigned int q2 = sub + 2 * Q < mwords ? __ldg(row + (long)(sub + 2 * Q) * stride) : 0u;
             unsigned int q3 = sub + 3 * Q < mwords ? __ldg(row + (long)(sub + 3 * Q) * stride) : 0u;
             const int words = active ? (nn[i] + 1) >> 1 : 0;
+            if (DRIFT && active && sub == 0) {
+                // the drift's operands into L2 while the row is computed
+                prefetch_l2(D.v + i);
+                prefetch_l2(D.v + D.vcap + i);
+                prefetch_l2(D.v + 2 * D.vcap + i);
+                prefetch_l2(D.pos + i);
+                prefetch_l2(D.xb + i);
+            }
             double fx = 0, fy = 0, fz = 0, e = 0, w = 0;
             // one pair (rows hold the particle itself, as the reference's full list
             // does): outside the cutoff or self, s2 is zero and with it the force,
@@ -348,9 +358,32 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
                 }
             }
             if (active && sub == 0) {
-                f[i] = fx;
-                f[fcap + i] = fy;
-                f[2 * fcap + i] = fz;
+                if (DRIFT) {
+                    const long vc = D.vcap;
+                    double vx = D.v[i] + D.half * fx;
+                    double vy = D.v[vc + i] + D.half * fy;
+                    double vz = D.v[2 * vc + i] + D.half * fz;
+                    ke += 0.5 * D.mass * (vx * vx + vy * vy + vz * vz);
+                    vx = vx + D.half * fx;
+                    vy = vy + D.half * fy;
+                    vz = vz + D.half * fz;
+                    double4 x = ld4(D.pos, i);
+                    x.x += D.dt * vx;
+                    x.y += D.dt * vy;
+                    x.z += D.dt * vz;
+                    D.v[i] = vx;
+                    D.v[vc + i] = vy;
+                    D.v[2 * vc + i] = vz;
+                    st4(D.pos, i, x);
+                    D.sxy_next[i] = make_double2(x.x, x.y);
+                    D.sz_next[i] = x.z;
+                    const double4 b = ld4(D.xb, i);
+                    md2 = fmax(md2, dist2(x.x - b.x, x.y - b.y, x.z - b.z));
+                } else {
+                    f[i] = fx;
+                    f[fcap + i] = fy;
+                    f[2 * fcap + i] = fz;
+                }
                 if (ENERGY) {
                     pe += 0.5 * e;
                     vir += 0.5 * w;
@@ -362,10 +395,21 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
     if (ENERGY) {
         pe = block_sum<double, FBLOCK_T>(pe);
         vir = block_sum<double, FBLOCK_T>(vir);
+        if (DRIFT) ke = block_sum<double, FBLOCK_T>(ke);
         if (threadIdx.x == 0) {
-            part[2 * blockIdx.x] = pe;
-            part[2 * blockIdx.x + 1] = vir;
+            if (DRIFT) {
+                part[3 * blockIdx.x] = pe;
+                part[3 * blockIdx.x + 1] = vir;
+                part[3 * blockIdx.x + 2] = ke;
+            } else {
+                part[2 * blockIdx.x] = pe;
+                part[2 * blockIdx.x + 1] = vir;
+            }
         }
+    }
+    if (DRIFT) {
+        md2 = block_max<double, FBLOCK_T>(md2);
+        if (threadIdx.x == 0) atomic_max_nonneg(D.maxd2, md2);
     }
 }
 
@@ -493,10 +537,11 @@ int tile_build(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR
     }
     max_nn = (max_nn + 1) & ~1;  // whole 32-bit words
     // three z-layer passes with a third of the staging (more resident CTAs) when
-    // the largest layer is well below the whole tile and the tile's domain
-    // particles fit two per thread (the sizes of the tile_sizes call before)
-    const unsigned int pcap = h->ctrl_h->tile_pass_max, cmax = h->ctrl_h->tile_center_max;
-    const bool layers = pcap > 0 && 2 * pcap < cap && cmax <= 2u * TBLOCK;
+    // the largest layer is well below the whole tile (the sizes of the tile_sizes
+    // call before); a tile of more than two domain particles a thread takes the
+    // passes again for the rest
+    const unsigned int pcap = h->ctrl_h->tile_pass_max;
+    const bool layers = pcap > 0 && 2 * pcap < cap;
     for (int attempt = 0; attempt < 3; ++attempt) {
         int smem = (int)((layers ? pcap : cap) * sizeof(float4));
         if (smem < 16) smem = 16;
@@ -553,23 +598,38 @@ int tile_split(pd_vd h, Buf& sxy, Buf& sz, long first, long n, cudaStream_t st) 
     return PD_OK;
 }
 
+template <bool E, int P, int MINB, bool DRIFT>
+static int launch_lj_xyz_k(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
+                           unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<double>& LP,
+                           double* f, double* part, const Buf& sxy, const Buf& sz, const DriftArgs& D,
+                           cudaStream_t st) {
+    int smem = (int)(cap * 24);
+    if (smem < 32) smem = 32;
+    const int mwords = (int)std::min<long>((long)(nbr.bytes / (4 * (size_t)stride)), 1L << 30);
+    PD_TRY(allow_smem(k_vtile_lj_xyz<E, P, MINB, DRIFT>, smem));
+    pd::launch(k_vtile_lj_xyz<E, P, MINB, DRIFT>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
+               (const double2*)sxy.as<double2>(), (const double*)sz.as<double>(), h->n_real, tg, csR, csI, cap,
+               nbr.as<unsigned int>(), nn.as<int>(), stride, mwords, LP, f, h->cap, part, &h->ctrl->err, D);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
 template <bool E, int P, int MINB>
 static int launch_lj_xyz(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                          unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<double>& LP, double* f,
-                         double* part, const Buf& sxy, const Buf& sz, cudaStream_t st) {
+                         double* part, const Buf& sxy, const Buf& sz, const DriftArgs* drift, cudaStream_t st) {
     if (!sxy.p || !sz.p) {
         set_error("tile_lj: the FP64 staging copies were not made");
         return PD_ESTATE;
     }
-    int smem = (int)(cap * 24);
-    if (smem < 32) smem = 32;
-    const int mwords = (int)std::min<long>((long)(nbr.bytes / (4 * (size_t)stride)), 1L << 30);
-    PD_TRY(allow_smem(k_vtile_lj_xyz<E, P, MINB>, smem));
-    pd::launch(k_vtile_lj_xyz<E, P, MINB>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
-               (const double2*)sxy.as<double2>(), (const double*)sz.as<double>(), h->n_real, tg, csR, csI, cap,
-               nbr.as<unsigned int>(), nn.as<int>(), stride, mwords, LP, f, h->cap, part, &h->ctrl->err);
-    PD_LAUNCH_CHECK();
-    return PD_OK;
+    if (!drift) return launch_lj_xyz_k<E, P, MINB, false>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part,
+                                                          sxy, sz, DriftArgs{}, st);
+    if (!E || !drift->sxy_next || !drift->sz_next || drift->sxy_next == sxy.as<double2>()) {
+        set_error("tile_lj: a drift needs the energy partials and a second pair of staging copies");
+        return PD_EINVAL;
+    }
+    return launch_lj_xyz_k<E, P, MINB, E>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, *drift,
+                                          st);
 }
 
 // FP32 storage: the 16-byte records
@@ -577,9 +637,13 @@ template <class T, bool E, int P>
 struct LjLaunch {
     static int run(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                    unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<T>& LP, T* f, double* part,
-                   const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+                   const Buf& sxy, const Buf& sz, int smem, const DriftArgs* drift, cudaStream_t st) {
         (void)sxy;
         (void)sz;
+        if (drift) {
+            set_error("tile_lj: the fused drift is the FP64 path's");
+            return PD_EINVAL;
+        }
         PD_TRY(allow_smem(k_vtile_lj<T, E, P>, smem));
         pd::launch(k_vtile_lj<T, E, P>, (unsigned)ntiles, FBLOCK_T, (size_t)smem, st,
                    (const typename V4<T>::type*)h->pos, h->n_real, tg, csR, csI, cap, nbr.as<unsigned int>(),
@@ -593,16 +657,17 @@ template <bool E, int P>
 struct LjLaunch<double, E, P> {
     static int run(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                    unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const LJP<double>& LP, double* f,
-                   double* part, const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+                   double* part, const Buf& sxy, const Buf& sz, int smem, const DriftArgs* drift, cudaStream_t st) {
         (void)smem;
-        return launch_lj_xyz<E, P, 4>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, st);
+        return launch_lj_xyz<E, P, 4>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, drift, st);
     }
 };
 
 template <class T>
 static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
                      unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, T* f,
-                     double* part, bool energy, int P, const Buf& sxy, const Buf& sz, int smem, cudaStream_t st) {
+                     double* part, bool energy, int P, const Buf& sxy, const Buf& sz, int smem,
+                     const DriftArgs* drift, cudaStream_t st) {
     LJP<T> LP{};
     LP.eps24 = (T)(24.0 * lj.eps);
     LP.eps4 = (T)(4.0 * lj.eps);
@@ -611,7 +676,8 @@ static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned in
     LP.rc2 = rc * rc;
 #define PD_LJ_CASE(E, PP)                                                                                         \
     if (energy == E && P == PP)                                                                                   \
-        return LjLaunch<T, E, PP>::run(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, smem, st);
+        return LjLaunch<T, E, PP>::run(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, LP, f, part, sxy, sz, smem, \
+                                       drift, st);
     PD_LJ_CASE(true, 1)
     PD_LJ_CASE(true, 2)
     PD_LJ_CASE(true, 4)
@@ -625,15 +691,16 @@ static int tile_lj_t(pd_vd h, const TileGeom& tg, long ntiles, const unsigned in
 
 int tile_lj(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,
             unsigned int cap, const Buf& nbr, const Buf& nn, long stride, const pd_lj_params_t& lj, int force_prop,
-            double* part, bool energy, int P, const Buf& sxy, const Buf& sz, cudaStream_t st) {
+            double* part, bool energy, int P, const Buf& sxy, const Buf& sz, cudaStream_t st,
+            const DriftArgs* drift) {
     Prop& F = h->props[force_prop];
     int smem = (int)(cap * h->pos_bytes);
     if (smem < 16) smem = 16;
     if (h->dtype == PD_F64)
         return tile_lj_t<double>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (double*)F.d, part, energy, P,
-                                 sxy, sz, smem, st);
+                                 sxy, sz, smem, drift, st);
     return tile_lj_t<float>(h, tg, ntiles, csR, csI, cap, nbr, nn, stride, lj, (float*)F.d, part, energy, P, sxy,
-                            sz, smem, st);
+                            sz, smem, drift, st);
 }
 
 int tile_translate(pd_vd h, const TileGeom& tg, long ntiles, const unsigned int* csR, const unsigned int* csI,

@@ -267,8 +267,8 @@ __device__ __forceinline__ void tile_rows(const TileSh& S, const unsigned int (*
 // over the passes, so its row holds the entries in the same order as the
 // single-pass walk (tile_rows); entries index the full staging layout, which the
 // pair kernels stage.  The caller owns the mbarrier; `ph` counts its completed
-// phases.  Returns false (uniformly) if the tile does not fit (ERR_TILE_CAP: more
-// than 2 * blockDim domain particles or a layer beyond pcap) or a wait gave up.
+// phases.  Returns false (uniformly) if the tile does not fit (ERR_TILE_CAP: a
+// layer beyond pcap) or a wait gave up.
 template <class T>
 __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned int (*segb)[TXMAX + 3],
                                                  const float4* __restrict__ preal, const float4* __restrict__ pimg,
@@ -281,81 +281,84 @@ __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
     const int ncol = S.ncol, nc = ncol - 1;
     const unsigned int self_base = S.oR[4] - S.cR[4][0];
-    // each thread: one domain particle per 128 (the tile's particles in order)
-    constexpr int MAXI = 2;  // domain particles per thread (tiles of up to 256)
-    float4 xi[MAXI];
-    int jcol[MAXI], cnt[MAXI];
-    unsigned int pend[MAXI];
-    int nmine = 0;
-    for (unsigned int i = ib + threadIdx.x; i < ie && nmine < MAXI; i += blockDim.x, ++nmine) {
-        xi[nmine] = preal[i];
-        int j = 1;
-        while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
-        jcol[nmine] = j;
-        cnt[nmine] = 0;
-        pend[nmine] = 0;
-    }
-    if (ie - ib > (unsigned int)(MAXI * blockDim.x)) {
-        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
-        return false;
-    }
-    for (int pass = 0; pass < 3; ++pass) {
-        const unsigned int base = S.oR[3 * pass];
-        const unsigned int end = pass < 2 ? S.oR[3 * pass + 3] : S.total;
-        const unsigned int tot = end - base;
-        if (tot > pcap) {
-            if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
-            return false;
+    // each thread: up to MAXI domain particles of a sweep, one per blockDim.x of the
+    // tile's particles in order; a tile of more than MAXI * blockDim.x particles (a
+    // dense column) takes further sweeps, each staging the three layers again
+    constexpr int MAXI = 2;
+    const unsigned int sweep = (unsigned int)MAXI * blockDim.x;
+    for (unsigned int sb = ib; sb < ie; sb += sweep) {
+        float4 xi[MAXI];
+        int jcol[MAXI], cnt[MAXI];
+        unsigned int pend[MAXI];
+        int nmine = 0;
+        for (unsigned int i = sb + threadIdx.x; i < ie && nmine < MAXI; i += blockDim.x, ++nmine) {
+            xi[nmine] = preal[i];
+            int j = 1;
+            while (j < ncol - 2 && S.cR[4][j + 1] <= i) ++j;
+            jcol[nmine] = j;
+            cnt[nmine] = 0;
+            pend[nmine] = 0;
         }
-        bool ok = true;
-        if (tot > 0) {
-            if (threadIdx.x == 0) {
-                mbar_arrive_expect_tx(bar, tot * (unsigned int)sizeof(float4));
-                for (int r = 3 * pass; r < 3 * pass + 3; ++r) {
-                    unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-                    if (lr) bulk_g2s(sm + (S.oR[r] - base), preal + S.cR[r][0], lr * (unsigned int)sizeof(float4), bar);
-                    unsigned int li = S.cI[r][nc] - S.cI[r][0];
-                    if (li) bulk_g2s(sm + (S.oI[r] - base), pimg + S.cI[r][0], li * (unsigned int)sizeof(float4), bar);
+        for (int pass = 0; pass < 3; ++pass) {
+            const unsigned int base = S.oR[3 * pass];
+            const unsigned int end = pass < 2 ? S.oR[3 * pass + 3] : S.total;
+            const unsigned int tot = end - base;
+            if (tot > pcap) {
+                if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
+                return false;
+            }
+            bool ok = true;
+            if (tot > 0) {
+                if (threadIdx.x == 0) {
+                    mbar_arrive_expect_tx(bar, tot * (unsigned int)sizeof(float4));
+                    for (int r = 3 * pass; r < 3 * pass + 3; ++r) {
+                        unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+                        if (lr)
+                            bulk_g2s(sm + (S.oR[r] - base), preal + S.cR[r][0], lr * (unsigned int)sizeof(float4), bar);
+                        unsigned int li = S.cI[r][nc] - S.cI[r][0];
+                        if (li)
+                            bulk_g2s(sm + (S.oI[r] - base), pimg + S.cI[r][0], li * (unsigned int)sizeof(float4), bar);
+                    }
                 }
+                ok = mbar_wait_bounded(bar, ph & 1u, 1u << 24);
+                if (!ok) {
+                    atomicOr(err, ERR_TIMEOUT);
+                    mbar_wait_bounded(bar, ph & 1u, 1u << 24);
+                }
+                ++ph;
             }
-            ok = mbar_wait_bounded(bar, ph & 1u, 1u << 24);
-            if (!ok) {
-                atomicOr(err, ERR_TIMEOUT);
-                mbar_wait_bounded(bar, ph & 1u, 1u << 24);
-            }
-            ++ph;
-        }
-        if (!__syncthreads_and(ok ? 1 : 0)) return false;
-        for (int m = 0; m < nmine; ++m) {
-            const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
-            const int j = jcol[m];
-            const float4 x = xi[m];
-            int c = cnt[m];
-            unsigned int pd_ = pend[m];
-            unsigned int* out = nbr + i;
+            if (!__syncthreads_and(ok ? 1 : 0)) return false;
+            for (int m = 0; m < nmine; ++m) {
+                const unsigned int i = sb + threadIdx.x + (unsigned int)m * blockDim.x;
+                const int j = jcol[m];
+                const float4 x = xi[m];
+                int c = cnt[m];
+                unsigned int pd_ = pend[m];
+                unsigned int* out = nbr + i;
 #pragma unroll 1
-            for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg)
-                seg_rows<T>(sm, base, segb[sg][j - 1], segb[sg][j + 2], x, i, pos, r2, lo_thr, hi_thr, out, stride,
-                            max_nn, c, pd_);
-            cnt[m] = c;
-            pend[m] = pd_;
+                for (int sg = 6 * pass; sg < 6 * pass + 6; ++sg)
+                    seg_rows<T>(sm, base, segb[sg][j - 1], segb[sg][j + 2], x, i, pos, r2, lo_thr, hi_thr, out,
+                                stride, max_nn, c, pd_);
+                cnt[m] = c;
+                pend[m] = pd_;
+            }
+            // every thread is done with this layer before the next one is copied over it
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
         }
-        // every thread is done with this layer before the next one is copied over it
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-    }
-    for (int m = 0; m < nmine; ++m) {
-        const unsigned int i = ib + threadIdx.x + (unsigned int)m * blockDim.x;
-        int c = cnt[m];
-        unsigned int* out = nbr + i;
-        // odd rows end with the particle itself, which the pair kernel skips
-        if ((c & 1) && c < max_nn) out[(long)(c >> 1) * stride] = pend[m] | ((self_base + i) << 16);
-        if (c > max_nn) {
-            atomicOr(err, ERR_NN_OVERFLOW);
-            atomicMax(nn_max, (unsigned int)c);
-            c = max_nn;
+        for (int m = 0; m < nmine; ++m) {
+            const unsigned int i = sb + threadIdx.x + (unsigned int)m * blockDim.x;
+            int c = cnt[m];
+            unsigned int* out = nbr + i;
+            // odd rows end with the particle itself, which the pair kernel skips
+            if ((c & 1) && c < max_nn) out[(long)(c >> 1) * stride] = pend[m] | ((self_base + i) << 16);
+            if (c > max_nn) {
+                atomicOr(err, ERR_NN_OVERFLOW);
+                atomicMax(nn_max, (unsigned int)c);
+                c = max_nn;
+            }
+            nn[i] = c;
         }
-        nn[i] = c;
     }
     return true;
 }

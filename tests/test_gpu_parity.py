@@ -339,14 +339,15 @@ def test_md_tiled_rows_equal_oracle_sets(pd, orc, tx):
         assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), np.sort(eidx[eoff[i]:eoff[i + 1]]))
 
 
-@pytest.mark.parametrize("layout", ["uniform", "dense_half", "non_cubic"])
+@pytest.mark.parametrize("layout", ["uniform", "dense_half", "non_cubic", "wide_tiles"])
 def test_md_tiled_rows_random_layouts(pd, orc, layout):
     """The same on layouts that are not lattices: uniform random positions (tile
     sizes fluctuate around the automatic width's target), a box whose left half
-    is three times as dense as its right (tiles far above the mean take the
-    narrower or single-pass builds), and a 48 x 30 x 21 box (axes of different
-    cell counts)."""
-    rng = np.random.default_rng({"uniform": 41, "dense_half": 42, "non_cubic": 43}[layout])
+    is three times as dense as its right (tiles far above the mean take further
+    sweeps of the layered build), a 48 x 30 x 21 box (axes of different cell
+    counts), and tiles of 14 cells (about 290 domain particles each: more than
+    one sweep of two particles a thread takes)."""
+    rng = np.random.default_rng({"uniform": 41, "dense_half": 42, "non_cubic": 43, "wide_tiles": 44}[layout])
     L, n = 40.0, 60000
     box = np.array([48.0, 30.0, 21.0]) if layout == "non_cubic" else np.full(3, L)
     if layout == "dense_half":
@@ -359,7 +360,7 @@ def test_md_tiled_rows_random_layouts(pd, orc, layout):
     vd = make_vd(pd, x, lo, hi, bc, 2.8, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
     vd.hostToDeviceProp(0, np.zeros((n, 3)))
     md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
-    md.set_tiles(True, 0)
+    md.set_tiles(True, 14 if layout == "wide_tiles" else 0)
     md.run(0)
     off, idx, tiled = md.verlet()
     assert tiled
