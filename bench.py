@@ -664,23 +664,29 @@ def main():
     f_ms, f_cnt = timers["force"]
     f_avg_s = f_ms / max(f_cnt, 1) / 1000.0
     # tiled rows: 2-byte entries, the position record is staged once per tile (counted once);
-    # mixed form: 16-byte FP32 offset records and FP32 forces
+    # mixed form: 16-byte FP32 offset records and FP32 forces.  The FP64 tiled kernel of
+    # every step but a run's last also makes the next step's kick and drift in place of
+    # storing the force: it reads the 32-byte position record, the velocity (24) and the
+    # 32-byte build position and writes the record, the velocity and the 24-byte staging
+    # copy (168 bytes, those of the separate kick-drift kernel it replaces); the launches
+    # of the timed run average steps - 1 of those and one force store
     if mixed:
         alg_bytes = n * (16 + 4 + 2 * mean_nn + 12)
     elif a.tiles:
-        alg_bytes = n * (24 + 4 + 2 * mean_nn + 24)
+        drift_share = (a.steps - 1) / max(a.steps, 1)
+        alg_bytes = n * (24 + 4 + 2 * mean_nn + drift_share * 168 + (1 - drift_share) * 24)
     else:
         alg_bytes = n * (32 + 4 + 4 * mean_nn + 24)
     peak, peak_kind = peaks()
     achieved = alg_bytes / f_avg_s / 1e9
     # secondary roofline of the FP64 pair kernel (its arithmetic, not HBM, is the
     # nearer ceiling): flops counted as executed -- distance 8 per row entry; inside
-    # r_cut another 29 (reciprocal seed + two Newton steps 9, s2 1, s6 2, force
-    # factor 5, three force FMAs 6, energy 4, virial 2); pairs inside r_cut
-    # estimated from the density (4/3 pi r_cut^3 rho)
+    # r_cut another 25 (sigma^2 / r^2 from the reciprocal seed by one series correction
+    # 7, s6 2, force factor 4, three force FMAs 6, energy 4, virial 2); pairs inside
+    # r_cut estimated from the density (4/3 pi r_cut^3 rho)
     rho = n / (L * L * L)
     in_cut = 4.18879 * R_CUT ** 3 * rho
-    flops = n * (8 * mean_nn + 29 * in_cut)
+    flops = n * (8 * mean_nn + 25 * in_cut)
     fma_peak = pd.measure_fma_rate(pd.PD_F32 if mixed else pd.PD_F64)
     kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_xyz" if a.tiles else "k_lj_verlet_f64")
     traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
