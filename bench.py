@@ -304,7 +304,8 @@ def form_cell_list_every_step(pd, torch, steps=100, warmup=5):
     return {"workload": "LJ MD FP64, N=4096 (16^3 lattice, spacing 1, jitter 0.05), box 16, r_cut 2.5, "
                         "cell list rebuilt every step, dt 0.005",
             "value": x.shape[0] * steps / (ms / 1e3), "unit": METRIC, "steps": steps, "ms_per_step": ms / steps,
-            "gpu_launches_per_step": (pd.launch_count() - l0) / steps}
+            "gpu_launches_per_step": (pd.launch_count() - l0) / steps,
+            "cluster_ctas": md.launch_shape()["cluster_ctas"]}
 
 
 def _ev_ms(torch, fn, reps):
@@ -696,7 +697,8 @@ def main():
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+kahan/f64-energy" if mixed else "f64", "data": "synthetic",
         "config": bench_config(n, world, a.nside, mixed),
-        "verlet_list": {"rebuilds_in_timed_region": builds, "mean_row": round(mean_nn, 2), "max_row": max_nn},
+        "verlet_list": {"rebuilds_in_timed_region": builds, "mean_row": round(mean_nn, 2), "max_row": max_nn,
+                        "tile_cells": md.launch_shape()["tile_tx"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
                      "kernel": "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_xyz (FP64)" if a.tiles else

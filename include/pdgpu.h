@@ -380,6 +380,11 @@ int pd_md_verlet_get(pd_md md, int* counts, int* idx, long idx_cap, int* tiled);
 /* Verlet rows of the last build: domain particles, mean and longest row */
 int pd_md_list_stats(pd_md md, long* n_dom, double* mean_nn, int* max_nn);
 int pd_md_timers(pd_md md, double* ms, long* counts);
+/* launch shape of the driver's kernels: CTAs of the one-cluster run of a small
+ * cell-list system (16, or 8 where the GPU cannot place 16; 0 before such a run),
+ * and the tile width in cells and lanes per particle of the tiled rows of the last
+ * build (0 and 0 without them) */
+int pd_md_launch_shape(pd_md md, int* cluster_ctas, int* tile_tx, int* threads_per_particle);
 
 /* ---- serving loop -------------------------------------------------------- */
 /* Many independent periodic LJ systems (precision form, FP32 forces / FP64

@@ -415,6 +415,7 @@ template <class T> static int md_run_cluster_t(pd_md md, int steps, cudaStream_t
     attr[0].val.clusterDim.z = 1;
     PD_CUDA(cudaLaunchKernelEx(&cfg, k_md_cluster<T>, A));
     __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED);
+    md->cluster_ctas = nct;
     unsigned int tot = 0;
     PD_CUDA(cudaMemcpyAsync(&tot, A.tot, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     if (E && steps > 0) PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));

@@ -1257,6 +1257,14 @@ int pd_md_set_timing(pd_md md, int on) {
     return PD_OK;
 }
 
+int pd_md_launch_shape(pd_md md, int* cluster_ctas, int* tile_tx, int* threads_per_particle) {
+    if (!md || !cluster_ctas || !tile_tx || !threads_per_particle) return PD_EINVAL;
+    *cluster_ctas = md->cluster_ctas;
+    *tile_tx = md->tiles_active ? md->tg.TX : 0;
+    *threads_per_particle = md->tiles_active ? md->tile_p : 0;
+    return PD_OK;
+}
+
 int pd_md_timers(pd_md md, double* ms, long* counts) {
     if (!md || !ms || !counts) return PD_EINVAL;
     for (int i = 0; i < 4; ++i) {

@@ -49,6 +49,7 @@ struct pd_md_s {
     std::vector<uintptr_t> gcl_key;  // the buffers and sizes the graph captured
     unsigned long long gcl_kernels = 0;
     pd::Buf eidx;
+    int cluster_ctas = 0;  // CTAs of the last one-cluster run (0: none so far)
     // optional per-phase device timing (CUDA events on the run's stream)
     bool timing = false;
     std::vector<cudaEvent_t> evp;  // six per step of a timed run, recorded without synchronising

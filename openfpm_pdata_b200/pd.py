@@ -155,6 +155,7 @@ def lib():
                               P(ctypes.c_long), vp], ip),
             "pd_set_cache_limit": ([lp, P(ctypes.c_long)], ip),
             "pd_md_list_stats": ([vp, P(ctypes.c_long), P(ctypes.c_double), P(ctypes.c_int)], ip),
+            "pd_md_launch_shape": ([vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)], ip),
             "pd_celllist_build_static": ([ip, vp, lp, dp, dp, P(ctypes.c_int), ip, vp, vp, vp, vp], ip),
             "pd_slab_map_label": ([vp, P(SlabT), P(ctypes.c_long), vp], ip),
             "pd_slab_halo_label": ([vp, P(SlabT), ip, P(ctypes.c_long), vp], ip),
@@ -687,6 +688,12 @@ class MD:
         n, m, x = ctypes.c_long(0), ctypes.c_double(0), ctypes.c_int(0)
         check(lib().pd_md_list_stats(self.h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(x)))
         return n.value, m.value, x.value
+
+    def launch_shape(self):
+        """{cluster_ctas, tile_tx, threads_per_particle} of the driver's kernels (see pdgpu.h)."""
+        c, t, p = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().pd_md_launch_shape(self.h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(p)))
+        return {"cluster_ctas": c.value, "tile_tx": t.value, "threads_per_particle": p.value}
 
     def stats(self):
         b, s, e = ctypes.c_long(0), ctypes.c_long(0), ctypes.c_int(0)

@@ -212,3 +212,30 @@ def test_md_spare_storage_across_storage_changes(pd):
     assert np.isfinite(E1).all()
     assert np.array_equal(E1, E2)
     assert np.array_equal(vd.deviceToHostProp(extra, with_ghost=False), np.ones((m, 2)))
+
+
+def test_md_launch_shape(pd):
+    """The driver reports the shapes its kernels ran with: the one-cluster step of
+    a small cell-list system (16 CTAs, or 8 where 16 cannot be placed) and the
+    tile width of the tiled rows."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(16, 1.0, 0.05, seed=1)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    vd = pd.VectorDist(x.shape[0], lo, hi, bc, 2.5, dtype=F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.0, r_cut=2.5, use_cell_list=True)
+    assert md.launch_shape()["cluster_ctas"] == 0
+    md.run(2)
+    assert md.launch_shape()["cluster_ctas"] in (8, 16)
+
+    x, v, L = workloads.lj_lattice(24, 1.1, 0.05, seed=2)
+    vd = pd.VectorDist(x.shape[0], np.zeros(3), np.full(3, L), bc, 2.8, dtype=F64,
+                       props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+    vd.hostToDevicePos(x)
+    vd.hostToDeviceProp(0, v)
+    md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
+    md.set_tiles(True, 7)
+    md.run(1)
+    s = md.launch_shape()
+    assert s["tile_tx"] == 7 and s["threads_per_particle"] == 2 and s["cluster_ctas"] == 0
