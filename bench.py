@@ -49,13 +49,13 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic(kernel_file):
+def read_traffic(kernel_file, key="traffic_bytes_per_launch"):
     """dram bytes per force launch (scaled to the full workload) from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", kernel_file)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -691,6 +691,11 @@ def main():
     fma_peak = pd.measure_fma_rate(pd.PD_F32 if mixed else pd.PD_F64)
     kname = "k_vtile_lj_mixed" if mixed else ("k_vtile_lj_xyz" if a.tiles else "k_lj_verlet_f64")
     traffic = read_traffic(f"{kname}_lj4M.md") if a.nside == N_SIDE else None
+    if traffic is not None and a.tiles and not mixed:
+        # the drifting launches' traffic and the last launch's, averaged like alg_bytes
+        plain = read_traffic(f"{kname}_lj4M.md", "traffic_bytes_per_launch_no_drift")
+        if plain is not None:
+            traffic = drift_share * traffic + (1 - drift_share) * plain
 
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
