@@ -258,24 +258,36 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             if (threadIdx.x == 0) atomicOr(err, ERR_TILE_CAP);
         } else {
             const int nc = S.ncol - 1;
-            if (threadIdx.x == 0) {
-                mbar_init(&S.bar, 1);
-                mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(double2));
-                for (int r = 0; r < 9; ++r) {
-                    const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
-                    if (lr) bulk_g2s(sxy + S.oR[r], xy + S.cR[r][0], lr * (unsigned int)sizeof(double2), &S.bar);
-                    if (li)
-                        bulk_g2s(sxy + S.oI[r], xy + n_real + S.cI[r][0], li * (unsigned int)sizeof(double2), &S.bar);
+            const unsigned int lane = threadIdx.x & 31u;
+            if (threadIdx.x < 32) {
+                if (lane == 0) {
+                    mbar_init(&S.bar, 1);
+                    mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(double2));
+                }
+                __syncwarp();
+                // one lane a range: lane 2r row r's real range, 2r + 1 its images
+                if (lane < 18u) {
+                    const int r = (int)(lane >> 1);
+                    const bool img = lane & 1u;
+                    const unsigned int c0 = img ? S.cI[r][0] : S.cR[r][0];
+                    const unsigned int len = (img ? S.cI[r][nc] : S.cR[r][nc]) - c0;
+                    if (len)
+                        bulk_g2s(sxy + (img ? S.oI[r] : S.oR[r]), xy + (img ? n_real : 0L) + c0,
+                                 len * (unsigned int)sizeof(double2), &S.bar);
                 }
             }
-            for (int r = 0; r < 9; ++r) {
-                const unsigned int lr = S.cR[r][nc] - S.cR[r][0], li = S.cI[r][nc] - S.cI[r][0];
-                for (unsigned int k = threadIdx.x; k < lr; k += blockDim.x)
-                    sz[S.oR[r] + k] = __ldg(zz + S.cR[r][0] + k);
-                for (unsigned int k = threadIdx.x; k < li; k += blockDim.x)
-                    sz[S.oI[r] + k] = __ldg(zz + n_real + S.cI[r][0] + k);
+            // z of the same ranges, a warp a range, while the copies are in flight
+            for (int sg = (int)(threadIdx.x >> 5); sg < 18; sg += FBLOCK_T / 32) {
+                const int r = sg >> 1;
+                const bool img = sg & 1;
+                const unsigned int c0 = img ? S.cI[r][0] : S.cR[r][0];
+                const unsigned int len = (img ? S.cI[r][nc] : S.cR[r][nc]) - c0;
+                const double* src = zz + (img ? n_real : 0L) + c0;
+                double* dst = sz + (img ? S.oI[r] : S.oR[r]);
+#pragma unroll 4
+                for (unsigned int k = lane; k < len; k += 32u) dst[k] = __ldg(src + k);
             }
-            // every thread waits on the barrier only after thread 0 initialised it
+            // every thread waits on the barrier only after the first lane initialised it
             __syncthreads();
             bool ok = mbar_wait_bounded(&S.bar, 0, 1u << 24);
             if (!ok) {

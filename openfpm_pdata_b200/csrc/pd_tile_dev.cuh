@@ -42,16 +42,24 @@ __device__ __forceinline__ void tile_layout(const TileGeom& tg, long t, const un
         else S.cR[r][j] = csR[c];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int off = 0;
-        for (int r = 0; r < 9; ++r) {
-            S.oR[r] = off;
-            off += S.cR[r][ncol - 1] - S.cR[r][0];
-            S.oI[r] = off;
-            off += S.cI[r][ncol - 1] - S.cI[r][0];
+    // staging offsets of the 18 ranges (row r's real range, then its images, r = 0..8):
+    // an exclusive scan of their lengths across the first warp
+    if (threadIdx.x < 32) {
+        const int s = (int)threadIdx.x, r = s >> 1;
+        unsigned int len = 0;
+        if (s < 18) len = (s & 1) ? S.cI[r][ncol - 1] - S.cI[r][0] : S.cR[r][ncol - 1] - S.cR[r][0];
+        unsigned int inc = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (s >= o) inc += v;
         }
-        S.total = off;
-        S.ncol = ncol;
+        if (s < 18) {
+            if (s & 1) S.oI[r] = inc - len;
+            else S.oR[r] = inc - len;
+        }
+        if (s == 17) S.total = inc;
+        if (s == 0) S.ncol = ncol;
     }
     __syncthreads();
 }
