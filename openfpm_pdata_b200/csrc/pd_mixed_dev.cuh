@@ -5,6 +5,7 @@
 #include "pd_internal.cuh"
 #include "pd_lj.cuh"
 #include "pd_tile.cuh"
+#include "pd_tile_dev.cuh"
 
 namespace pd {
 
@@ -130,16 +131,8 @@ __device__ __forceinline__ bool mixed_tile(long tile, const float4* __restrict__
             S.segb[sg][j] = (sg & 1) ? S.oI[r] + (S.cI[r][j] - S.cI[r][0]) : S.oR[r] + (S.cR[r][j] - S.cR[r][0]);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            mbar_arrive_expect_tx(bar, S.total * (unsigned int)sizeof(float4));
-            const int nc = ncol - 1;
-            for (int r = 0; r < 9; ++r) {
-                unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-                if (lr) bulk_g2s(sm + S.oR[r], off + S.cR[r][0], lr * (unsigned int)sizeof(float4), bar);
-                unsigned int li = S.cI[r][nc] - S.cI[r][0];
-                if (li) bulk_g2s(sm + S.oI[r], off + n_real + S.cI[r][0], li * (unsigned int)sizeof(float4), bar);
-            }
-        }
+        if (threadIdx.x < 32)
+            stage_ranges_warp(S, 0, 9, sm, 0u, off, off + n_real, S.total * (unsigned int)sizeof(float4), bar);
         bool waited = mbar_wait_bounded(bar, uses & 1u, 1u << 24);
         if (!waited) {
             atomicOr(err, ERR_TIMEOUT);

@@ -201,14 +201,17 @@ __global__ void __launch_bounds__(FBLOCK_T) k_vtile_sph(const typename V4<T>::ty
     }
     if (threadIdx.x == 0) mbar_init(&S.bar, 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&S.bar, 2u * S.total * (unsigned int)sizeof(T4));
-        const int nc = ncol - 1;
-        for (int r = 0; r < 9; ++r) {
-            unsigned int lr = S.cR[r][nc] - S.cR[r][0];
+    if (threadIdx.x < 32) {
+        // one lane a copy: lane 2r row r's position records, 2r + 1 its velocity records
+        const unsigned int lane = threadIdx.x;
+        if (lane == 0) mbar_arrive_expect_tx(&S.bar, 2u * S.total * (unsigned int)sizeof(T4));
+        __syncwarp();
+        if (lane < 18u) {
+            const int r = (int)(lane >> 1), nc = ncol - 1;
+            const unsigned int lr = S.cR[r][nc] - S.cR[r][0];
             if (lr) {
-                bulk_g2s(sp + S.oR[r], pos + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
-                bulk_g2s(sa + S.oR[r], aux + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
+                if (lane & 1u) bulk_g2s(sa + S.oR[r], aux + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
+                else bulk_g2s(sp + S.oR[r], pos + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
             }
         }
     }

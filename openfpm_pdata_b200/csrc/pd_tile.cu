@@ -260,21 +260,9 @@ __global__ void __launch_bounds__(FBLOCK_T, MINB) k_vtile_lj_xyz(const double2* 
             const int nc = S.ncol - 1;
             const unsigned int lane = threadIdx.x & 31u;
             if (threadIdx.x < 32) {
-                if (lane == 0) {
-                    mbar_init(&S.bar, 1);
-                    mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(double2));
-                }
+                if (lane == 0) mbar_init(&S.bar, 1);
                 __syncwarp();
-                // one lane a range: lane 2r row r's real range, 2r + 1 its images
-                if (lane < 18u) {
-                    const int r = (int)(lane >> 1);
-                    const bool img = lane & 1u;
-                    const unsigned int c0 = img ? S.cI[r][0] : S.cR[r][0];
-                    const unsigned int len = (img ? S.cI[r][nc] : S.cR[r][nc]) - c0;
-                    if (len)
-                        bulk_g2s(sxy + (img ? S.oI[r] : S.oR[r]), xy + (img ? n_real : 0L) + c0,
-                                 len * (unsigned int)sizeof(double2), &S.bar);
-                }
+                stage_ranges_warp(S, 0, 9, sxy, 0u, xy, xy + n_real, S.total * (unsigned int)sizeof(double2), &S.bar);
             }
             // z of the same ranges, a warp a range, while the copies are in flight
             for (int sg = (int)(threadIdx.x >> 5); sg < 18; sg += FBLOCK_T / 32) {

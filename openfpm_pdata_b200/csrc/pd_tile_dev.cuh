@@ -64,6 +64,28 @@ __device__ __forceinline__ void tile_layout(const TileGeom& tg, long t, const un
     __syncthreads();
 }
 
+// The bulk copies of a tile's staged ranges of rows [r0, r0 + nrow), issued by the
+// first warp, one lane a range (lane 2k: row r0 + k's real range, 2k + 1: its
+// images), into dst at the ranges' staging offsets less `base`; lane 0 first sets the
+// barrier's expected bytes.  Called by the whole first warp.
+template <class TS, class T4>
+__device__ __forceinline__ void stage_ranges_warp(const TS& S, int r0, int nrow, T4* dst, unsigned int base,
+                                                  const T4* __restrict__ preal, const T4* __restrict__ pimg,
+                                                  unsigned int bytes, unsigned long long* bar) {
+    const unsigned int lane = threadIdx.x & 31u;
+    if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+    __syncwarp();
+    if (lane < 2u * (unsigned int)nrow) {
+        const int r = r0 + (int)(lane >> 1), nc = S.ncol - 1;
+        const bool img = lane & 1u;
+        const unsigned int c0 = img ? S.cI[r][0] : S.cR[r][0];
+        const unsigned int len = (img ? S.cI[r][nc] : S.cR[r][nc]) - c0;
+        if (len)
+            bulk_g2s(dst + ((img ? S.oI[r] : S.oR[r]) - base), (img ? pimg : preal) + c0,
+                     len * (unsigned int)sizeof(T4), bar);
+    }
+}
+
 // Stage the tile's 18 ranges; false (uniformly) if the tile does not fit or the
 // bounded wait gave up (error bit set).
 template <class T>
@@ -78,16 +100,7 @@ __device__ __forceinline__ bool tile_stage(const typename V4<T>::type* __restric
     if (S.total == 0) return true;
     if (threadIdx.x == 0) mbar_init(&S.bar, 1);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(&S.bar, S.total * (unsigned int)sizeof(T4));
-        const int nc = S.ncol - 1;
-        for (int r = 0; r < 9; ++r) {
-            unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-            if (lr) bulk_g2s(sm + S.oR[r], preal + S.cR[r][0], lr * (unsigned int)sizeof(T4), &S.bar);
-            unsigned int li = S.cI[r][nc] - S.cI[r][0];
-            if (li) bulk_g2s(sm + S.oI[r], pimg + S.cI[r][0], li * (unsigned int)sizeof(T4), &S.bar);
-        }
-    }
+    if (threadIdx.x < 32) stage_ranges_warp(S, 0, 9, sm, 0u, preal, pimg, S.total * (unsigned int)sizeof(T4), &S.bar);
     bool ok = mbar_wait_bounded(&S.bar, 0, 1u << 24);
     if (!ok) {
         atomicOr(err, ERR_TIMEOUT);
@@ -110,16 +123,7 @@ __device__ __forceinline__ int tile_stage_bar(const typename V4<T>::type* __rest
         return -1;
     }
     if (S.total == 0) return 0;
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, S.total * (unsigned int)sizeof(T4));
-        const int nc = S.ncol - 1;
-        for (int r = 0; r < 9; ++r) {
-            unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-            if (lr) bulk_g2s(sm + S.oR[r], preal + S.cR[r][0], lr * (unsigned int)sizeof(T4), bar);
-            unsigned int li = S.cI[r][nc] - S.cI[r][0];
-            if (li) bulk_g2s(sm + S.oI[r], pimg + S.cI[r][0], li * (unsigned int)sizeof(T4), bar);
-        }
-    }
+    if (threadIdx.x < 32) stage_ranges_warp(S, 0, 9, sm, 0u, preal, pimg, S.total * (unsigned int)sizeof(T4), bar);
     bool ok = mbar_wait_bounded(bar, parity, 1u << 24);
     if (!ok) {
         atomicOr(err, ERR_TIMEOUT);
@@ -317,17 +321,8 @@ __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned
             }
             bool ok = true;
             if (tot > 0) {
-                if (threadIdx.x == 0) {
-                    mbar_arrive_expect_tx(bar, tot * (unsigned int)sizeof(float4));
-                    for (int r = 3 * pass; r < 3 * pass + 3; ++r) {
-                        unsigned int lr = S.cR[r][nc] - S.cR[r][0];
-                        if (lr)
-                            bulk_g2s(sm + (S.oR[r] - base), preal + S.cR[r][0], lr * (unsigned int)sizeof(float4), bar);
-                        unsigned int li = S.cI[r][nc] - S.cI[r][0];
-                        if (li)
-                            bulk_g2s(sm + (S.oI[r] - base), pimg + S.cI[r][0], li * (unsigned int)sizeof(float4), bar);
-                    }
-                }
+                if (threadIdx.x < 32)
+                    stage_ranges_warp(S, 3 * pass, 3, sm, base, preal, pimg, tot * (unsigned int)sizeof(float4), bar);
                 ok = mbar_wait_bounded(bar, ph & 1u, 1u << 24);
                 if (!ok) {
                     atomicOr(err, ERR_TIMEOUT);
