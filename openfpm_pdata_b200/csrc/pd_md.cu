@@ -1043,6 +1043,23 @@ static int md_energy_drift(pd_md md, int s, cudaStream_t st) {
     return PD_OK;
 }
 
+// Fold the per-phase times of the last timed run into the totals (its events are
+// complete: the run synchronised before it returned).
+static void md_fold_timing(pd_md md) {
+    const size_t steps = md->ev_rebuilt.size();
+    for (size_t s = 0; s < steps; ++s) {
+        float t[5];
+        for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], md->evp[6 * s + k], md->evp[6 * s + k + 1]);
+        md->ms[0] += t[0] + t[4];  // (fused) kick-drift and the previous step's energies; closing kick
+        md->cnt[0] += 1;
+        md->ms[md->ev_rebuilt[s] ? 1 : 2] += t[2];
+        md->cnt[md->ev_rebuilt[s] ? 1 : 2] += 1;
+        md->ms[3] += t[3];
+        md->cnt[3] += 1;
+    }
+    md->ev_rebuilt.clear();
+}
+
 int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     if (!md || steps < 0) return PD_EINVAL;
     if (md_cluster_eligible(md)) return md_run_cluster(md, steps, S(stream), E);
@@ -1073,6 +1090,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             PD_CUDA(cudaEventCreate(&e));
             md->evp.push_back(e);
         }
+    md_fold_timing(md);  // the previous run's events are recorded again below
     std::vector<unsigned char> rebuilt_at(md->timing ? steps : 0, 0);
 #define PD_EV(k) \
     if (md->timing) PD_CUDA(cudaEventRecord(md->evp[6 * (size_t)s + (k)], st))
@@ -1227,19 +1245,9 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     if (E && steps > 0) {
         PD_CUDA(cudaMemcpyAsync(E, md->E.p, sizeof(double) * 4 * steps, cudaMemcpyDeviceToHost, st));
     }
-    PD_CUDA(cudaStreamSynchronize(st));
-    if (md->timing)
-        for (int s = 0; s < steps; ++s) {
-            float t[5];
-            for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], md->evp[6 * (size_t)s + k], md->evp[6 * (size_t)s + k + 1]);
-            md->ms[0] += t[0] + t[4];  // (fused) kick-drift and the previous step's energies; closing kick
-            md->cnt[0] += 1;
-            md->ms[rebuilt_at[s] ? 1 : 2] += t[2];
-            md->cnt[rebuilt_at[s] ? 1 : 2] += 1;
-            md->ms[3] += t[3];
-            md->cnt[3] += 1;
-        }
+    // the energies and the error word in one synchronisation
     PD_TRY(read_ctrl(h, st));
+    if (md->timing) md->ev_rebuilt = std::move(rebuilt_at);  // read by pd_md_timers or the next run
     if (h->ctrl_h->err & (ERR_IMG_OVERFLOW | ERR_NN_OVERFLOW)) {
         set_error("pd_md_run: device capacity overflow (err=0x%x)", h->ctrl_h->err);
         return PD_EOVERFLOW;
@@ -1250,6 +1258,7 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
 int pd_md_set_timing(pd_md md, int on) {
     if (!md) return PD_EINVAL;
     md->timing = on != 0;
+    md->ev_rebuilt.clear();
     for (int i = 0; i < 4; ++i) {
         md->ms[i] = 0;
         md->cnt[i] = 0;
@@ -1267,6 +1276,7 @@ int pd_md_launch_shape(pd_md md, int* cluster_ctas, int* tile_tx, int* threads_p
 
 int pd_md_timers(pd_md md, double* ms, long* counts) {
     if (!md || !ms || !counts) return PD_EINVAL;
+    md_fold_timing(md);
     for (int i = 0; i < 4; ++i) {
         ms[i] = md->ms[i];
         counts[i] = md->cnt[i];

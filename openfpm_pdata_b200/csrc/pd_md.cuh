@@ -55,6 +55,9 @@ struct pd_md_s {
     std::vector<cudaEvent_t> evp;  // six per step of a timed run, recorded without synchronising
     double ms[4] = {0, 0, 0, 0};   // integrate, rebuild, images, force
     long cnt[4] = {0, 0, 0, 0};
+    // the last timed run's events, read when the times are asked for or before the
+    // next run records them again (not inside the run)
+    std::vector<unsigned char> ev_rebuilt;  // per step of that run: rebuilt or not
 };
 
 namespace pd {

@@ -291,7 +291,7 @@ __device__ __forceinline__ bool tile_rows_layers(const TileSh& S, const unsigned
                                                  unsigned int* __restrict__ nn_max, unsigned long long* bar,
                                                  unsigned int& ph) {
     const unsigned int ib = S.cR[4][1], ie = S.cR[4][S.ncol - 2];
-    const int ncol = S.ncol, nc = ncol - 1;
+    const int ncol = S.ncol;
     const unsigned int self_base = S.oR[4] - S.cR[4][0];
     // each thread: up to MAXI domain particles of a sweep, one per blockDim.x of the
     // tile's particles in order; a tile of more than MAXI * blockDim.x particles (a

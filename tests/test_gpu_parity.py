@@ -456,3 +456,28 @@ def test_md_cell_list_graph_recaptured_after_growth(pd):
         out.append(xs)
     assert np.array_equal(out[0], out[2])
     assert np.array_equal(out[1], out[3])
+
+
+def test_md_one_run_equals_runs_of_one_step(pd):
+    """A run of 24 steps -- whose pair kernels also make the next step's kick and drift
+    -- leaves the same positions and velocities, bit for bit, the same rebuild steps and
+    the same energies as 24 runs of one step each (separate kick and drift kernels)."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(20, 1.1, 0.05, seed=33)
+    lo, hi, bc = np.zeros(3), np.full(3, L), np.ones(3, np.int32)
+    out = []
+    for split in (False, True):
+        vd = make_vd(pd, x, lo, hi, bc, 2.8, F64, props=[(pd.PD_F64, 3), (pd.PD_F64, 3)])
+        vd.hostToDeviceProp(0, v)
+        md = pd.MD(vd, 0, 1, dt=0.005, skin=0.3)
+        E = np.concatenate([md.run(1) for _ in range(24)]) if split else md.run(24)
+        pos = vd.deviceToHostPos(with_ghost=False)
+        vel = vd.deviceToHostProp(0, with_ghost=False)
+        out.append((E, pos, vel, md.stats()[0]))
+    (E0, p0, v0, b0), (E1, p1, v1, b1) = out
+    assert b0 == b1 and b0 >= 3  # rebuilds inside the run
+    np.testing.assert_array_equal(E0[:, 3], E1[:, 3])
+    np.testing.assert_array_equal(p0, p1)
+    np.testing.assert_array_equal(v0, v1)
+    np.testing.assert_allclose(E0[:, 1:3], E1[:, 1:3], rtol=1e-13, atol=1e-9)
+    np.testing.assert_allclose(E0[:, 0], E1[:, 0], rtol=1e-12)
