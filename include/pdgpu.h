@@ -365,8 +365,11 @@ int pd_sph_create(pd_vd h, const pd_sph_params_t* sp, const pd_md_params_t* mp, 
 int pd_md_run(pd_md md, int steps, void* stream, double* E);
 /* statistics: builds so far, steps so far, device-side error word */
 int pd_md_stats(pd_md md, long* builds, long* steps, int* err);
-/* per-phase device time (CUDA events on the run's stream, one synchronisation per
- * step while enabled): ms/counts[4] = integrate, rebuild, image refresh, force */
+/* per-phase device time (CUDA events on the run's stream, recorded without a
+ * synchronisation and read when pd_md_timers is called or the next run starts):
+ * ms/counts[4] = integrate, rebuild, image refresh, force (on the plain FP64 tiled
+ * path the pair kernel also makes the next step's kick and drift, so "force" holds
+ * them and "integrate" the energies); enabling resets them */
 int pd_md_set_timing(pd_md md, int on);
 /* neighbour structure of the driver: tiled shared-memory rows (on, default) or
  * global-index rows; tx = cells per tile along x (0 = from the mean occupancy),
