@@ -1015,7 +1015,12 @@ int pd_md_destroy(pd_md md) {
 // of that step's force launch, the rebuild flag in the control block)
 static int md_energy(pd_md md, int s, cudaStream_t st) {
     pd_vd h = md->h;
-    if (md->tiles_active) {
+    if (md->physics == 1) {
+        // WCSPH: kinetic energy of the fluid, sum of densities
+        pd::launch(k_energy, 1, 256, 0, st, (const double*)md->rpart.as<double>(), md->nblk,
+                   (const double*)md->kpart.as<double>(), md->nblk, (const unsigned int*)&h->ctrl->rebuild,
+                   md->E.as<double>() + 4 * s);
+    } else if (md->tiles_active) {
         const int nb2 = 256;
         long chunk = (md->ntiles + nb2 - 1) / nb2;
         double* stage = md->tpart.as<double>() + 2 * md->ntiles;
@@ -1079,10 +1084,10 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
     double half = 0.5 * md->mp.dt / md->mp.mass;
     double lim = 0.5 * md->mp.skin;
     double lim2 = lim * lim;
-    // plain LJ: a step's closing half kick is fused with the next step's kick-drift
-    // (k_kick_kick_drift); the step's energies follow it, the last step's closing
-    // kick runs after the loop
-    const bool fused = md->physics == 0;
+    // a step's closing half kick is fused with the next step's kick-drift
+    // (k_kick_kick_drift, k_sph_kick_kick_drift); the step's energies follow it, the
+    // last step's closing kick runs after the loop
+    const bool fused = md->physics == 0 || md->physics == 1;
     // timing: six events per step, read after the run (no synchronisation in the loop)
     if (md->timing)
         while (md->evp.size() < (size_t)6 * steps) {
@@ -1104,7 +1109,11 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
             md->drifted = false;
         } else {
             PD_CUDA(cudaMemsetAsync(&h->ctrl->maxdisp2, 0, sizeof(unsigned long long), st));
-            if (fused && s > 0 && md->mixed) {
+            if (fused && s > 0 && md->physics == 1) {
+                PD_TRY(sph_kick_kick_drift(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->xb, md->aux, md->nblk,
+                                           md->mp.dt, md->kpart.as<double>(), md->rpart.as<double>(), st));
+                PD_TRY(md_energy(md, s - 1, st));
+            } else if (fused && s > 0 && md->mixed) {
                 PD_TRY(mixed_kick_kick_drift(h, md->vl->cl, md->off, md->offb, md->mp.vel_prop, md->mp.force_prop, md->nblk, half,
                                              md->mp.dt, md->mp.mass, md->kpart.as<double>(), st));
                 PD_TRY(md_energy(md, s - 1, st));
@@ -1226,7 +1235,11 @@ int pd_md_run(pd_md md, int steps, void* stream, double* E) {
         PD_EV(5);
     }
 #undef PD_EV
-    if (fused && steps > 0 && md->mixed) {
+    if (fused && steps > 0 && md->physics == 1) {
+        PD_TRY(sph_kick(h, md->sp, md->mp.vel_prop, md->mp.force_prop, md->nblk, md->mp.dt, md->kpart.as<double>(),
+                        md->rpart.as<double>(), st));
+        PD_TRY(md_energy(md, steps - 1, st));
+    } else if (fused && steps > 0 && md->mixed) {
         PD_TRY(mixed_kick(h, md->mp.vel_prop, md->mp.force_prop, md->nblk, half, md->mp.mass, md->kpart.as<double>(),
                           st));
         PD_TRY(md_energy(md, steps - 1, st));

@@ -142,6 +142,66 @@ __global__ void __launch_bounds__(256) k_sph_kick(T* __restrict__ v, const T* __
     }
 }
 
+// The end of one step and the start of the next in one pass: k_sph_kick of the step
+// (kinetic energy and density partials) and k_sph_kick_drift of the next, the same
+// operations in the same order, each array read and written once.
+template <class T>
+__global__ void __launch_bounds__(256) k_sph_kick_kick_drift(typename V4<T>::type* __restrict__ pos,
+                                                             const typename V4<T>::type* __restrict__ xb,
+                                                             typename V4<T>::type* __restrict__ aux,
+                                                             T* __restrict__ v, const T* __restrict__ a,
+                                                             T* __restrict__ rho, const T* __restrict__ drho,
+                                                             const int* __restrict__ type, long cap, long n, T half,
+                                                             T dt, SphK<T> P, double m,
+                                                             unsigned long long* __restrict__ maxd2,
+                                                             double* __restrict__ kpart, double* __restrict__ rpart) {
+    double mx = 0, ke = 0, rs = 0;
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
+        typename V4<T>::type x = ld4(pos, i);
+        T vx = v[i], vy = v[cap + i], vz = v[2 * cap + i];
+        if (type[i] == 0) {
+            const T ax = a[i], ay = a[cap + i], az = a[2 * cap + i];
+            vx = vx + half * ax;  // the step's closing half kick
+            vy = vy + half * ay;
+            vz = vz + half * az;
+            ke += 0.5 * m * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            vx = vx + half * ax;  // the next step's opening half kick and drift
+            vy = vy + half * ay;
+            vz = vz + half * az;
+            x.x += dt * vx;
+            x.y += dt * vy;
+            x.z += dt * vz;
+            v[i] = vx;
+            v[cap + i] = vy;
+            v[2 * cap + i] = vz;
+            typename V4<T>::type b = ld4(xb, i);
+            mx = fmax(mx, (double)dist2(x.x - b.x, x.y - b.y, x.z - b.z));
+        }
+        const T dr = drho[i];
+        T r = rho[i] + half * dr;
+        rs += (double)r;
+        r = r + half * dr;
+        rho[i] = r;
+        x.w = p_over_rho2(P, r);
+        st4(pos, i, x);
+        typename V4<T>::type au;
+        au.x = vx;
+        au.y = vy;
+        au.z = vz;
+        au.w = r;
+        st4(aux, i, au);
+    }
+    mx = warp_max(mx);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxd2, mx);
+    ke = block_sum<double, 256>(ke);
+    rs = block_sum<double, 256>(rs);
+    if (threadIdx.x == 0) {
+        kpart[blockIdx.x] = ke;
+        rpart[2 * blockIdx.x] = rs;
+        rpart[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
 struct TileShS {
     unsigned int cR[9][TXMAX + 3];
     unsigned int oR[9];
@@ -384,6 +444,28 @@ int sph_kick(pd_vd h, const pd_sph_params_t& sp, int vel_prop, int acc_prop, int
     else
         pd::launch(k_sph_kick<float>, nblk, 256, 0, st, (float*)V.d, (const float*)A.d, (float*)R.d,
                    (const float*)D.d, (const int*)Ty.d, h->cap, n, (float)(0.5 * dt), sp.mass, kpart, rpart);
+    PD_LAUNCH_CHECK();
+    return PD_OK;
+}
+
+int sph_kick_kick_drift(pd_vd h, const pd_sph_params_t& sp, int vel_prop, int acc_prop, const Buf& xb, Buf& aux,
+                        int nblk, double dt, double* kpart, double* rpart, cudaStream_t st) {
+    long n = h->n_real;
+    const Prop& V = h->props[vel_prop];
+    const Prop& A = h->props[acc_prop];
+    const Prop& R = h->props[sp.rho_prop];
+    const Prop& D = h->props[sp.drho_prop];
+    const Prop& Ty = h->props[sp.type_prop];
+    if (h->dtype == PD_F64)
+        pd::launch(k_sph_kick_kick_drift<double>, nblk, 256, 0, st, (double4*)h->pos,
+                   (const double4*)xb.as<double4>(), aux.as<double4>(), (double*)V.d, (const double*)A.d,
+                   (double*)R.d, (const double*)D.d, (const int*)Ty.d, h->cap, n, 0.5 * dt, dt, sphk<double>(sp),
+                   sp.mass, &h->ctrl->maxdisp2, kpart, rpart);
+    else
+        pd::launch(k_sph_kick_kick_drift<float>, nblk, 256, 0, st, (float4*)h->pos, (const float4*)xb.as<float4>(),
+                   aux.as<float4>(), (float*)V.d, (const float*)A.d, (float*)R.d, (const float*)D.d,
+                   (const int*)Ty.d, h->cap, n, (float)(0.5 * dt), (float)dt, sphk<float>(sp), sp.mass,
+                   &h->ctrl->maxdisp2, kpart, rpart);
     PD_LAUNCH_CHECK();
     return PD_OK;
 }
