@@ -165,6 +165,37 @@ __global__ void k_gather(const E* __restrict__ src, E* __restrict__ dst, const i
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
         dst[k] = src[ids[k]];
 }
+// the same for up to GCOLS columns at once (positions, global ids, property components):
+// each permutation entry read once; a column's element is 4, 8, 16 or 32 bytes
+static constexpr int GCOLS = 16;
+struct GatherCols {
+    const char* src[GCOLS];
+    char* dst[GCOLS];
+    int esize[GCOLS];
+    int ncol;
+};
+__global__ void k_gather_cols(const int* __restrict__ ids, long n, GatherCols G) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const long id = ids[k];
+        for (int c = 0; c < G.ncol; ++c) {
+            const int es = G.esize[c];
+            if (es == 32) {
+                const double2* s2 = reinterpret_cast<const double2*>(G.src[c]) + 2 * id;
+                double2* d2 = reinterpret_cast<double2*>(G.dst[c]) + 2 * k;
+                const double2 a = __ldg(s2), b = __ldg(s2 + 1);
+                d2[0] = a;
+                d2[1] = b;
+            } else if (es == 16) {
+                reinterpret_cast<double2*>(G.dst[c])[k] = __ldg(reinterpret_cast<const double2*>(G.src[c]) + id);
+            } else if (es == 8) {
+                reinterpret_cast<long long*>(G.dst[c])[k] = __ldg(reinterpret_cast<const long long*>(G.src[c]) + id);
+            } else {
+                reinterpret_cast<int*>(G.dst[c])[k] = __ldg(reinterpret_cast<const int*>(G.src[c]) + id);
+            }
+        }
+    }
+}
+
 // restore: dst[sorted[k]] = src[k]
 template <class T>
 __global__ void k_scatter4(const typename V4<T>::type* __restrict__ src, typename V4<T>::type* __restrict__ dst,
@@ -255,33 +286,38 @@ static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask
         h->spare_cap = h->cap;
     }
     const unsigned g = grid_for(n, 256);
-    if (with_pos) {
-        if (h->dtype == PD_F64)
-            pd::launch(k_gather4<double>, g, 256, 0, st, (const double4*)h->pos, (double4*)h->spare_pos, ids, n);
-        else
-            pd::launch(k_gather4<float>, g, 256, 0, st, (const float4*)h->pos, (float4*)h->spare_pos, ids, n);
+    // every column moved by one gather kernel per GCOLS columns
+    GatherCols G{};
+    auto flush = [&]() -> int {
+        if (G.ncol == 0) return PD_OK;
+        pd::launch(k_gather_cols, g, 256, 0, st, ids, n, G);
         PD_LAUNCH_CHECK();
-        std::swap(h->pos, h->spare_pos);
-    }
-    if (with_gid) {
-        pd::launch(k_gather<int>, g, 256, 0, st, (const int*)h->gid, h->spare_gid, ids, n);
-        PD_LAUNCH_CHECK();
-        std::swap(h->gid, h->spare_gid);
-    }
+        G.ncol = 0;
+        return PD_OK;
+    };
+    auto add = [&](const void* src, void* dst, int esize) -> int {
+        if (G.ncol == GCOLS) PD_TRY(flush());
+        G.src[G.ncol] = (const char*)src;
+        G.dst[G.ncol] = (char*)dst;
+        G.esize[G.ncol] = esize;
+        G.ncol++;
+        return PD_OK;
+    };
+    if (with_pos) PD_TRY(add(h->pos, h->spare_pos, (int)h->pos_bytes));
+    if (with_gid) PD_TRY(add(h->gid, h->spare_gid, 4));
     for (size_t p = 0; p < h->props.size(); ++p) {
         if (!(prop_mask & (1ul << p))) continue;
         Prop& P = h->props[p];
         for (int c = 0; c < P.ncomp; ++c) {
             const size_t o = (size_t)c * h->cap * P.esize;
-            if (P.esize == 8)
-                pd::launch(k_gather<long long>, g, 256, 0, st, (const long long*)(P.d + o),
-                           (long long*)(h->spare_props[p] + o), ids, n);
-            else
-                pd::launch(k_gather<int>, g, 256, 0, st, (const int*)(P.d + o), (int*)(h->spare_props[p] + o), ids, n);
-            PD_LAUNCH_CHECK();
+            PD_TRY(add(P.d + o, h->spare_props[p] + o, P.esize));
         }
-        std::swap(P.d, h->spare_props[p]);
     }
+    PD_TRY(flush());
+    if (with_pos) std::swap(h->pos, h->spare_pos);
+    if (with_gid) std::swap(h->gid, h->spare_gid);
+    for (size_t p = 0; p < h->props.size(); ++p)
+        if (prop_mask & (1ul << p)) std::swap(h->props[p].d, h->spare_props[p]);
     return PD_OK;
 }
 
