@@ -173,10 +173,20 @@ struct GatherCols {
     char* dst[GCOLS];
     int esize[GCOLS];
     int ncol;
+    // with FP64 records in column 0: the same records also to xb and as (x, y) / z copies
+    double4* xb;
+    double2* sxy;
+    double* sz;
 };
 __global__ void k_gather_cols(const int* __restrict__ ids, long n, GatherCols G) {
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
         const long id = ids[k];
+        if (G.xb) {
+            const double4 x = ld4(reinterpret_cast<const double4*>(G.src[0]), id);
+            st4(G.xb, k, x);
+            G.sxy[k] = make_double2(x.x, x.y);
+            G.sz[k] = x.z;
+        }
         for (int c = 0; c < G.ncol; ++c) {
             const int es = G.esize[c];
             if (es == 32) {
@@ -274,7 +284,7 @@ int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, 
 // (the images) and moves the epoch on, and not inside a stream capture (the
 // capture would keep the first pair of addresses).
 static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask, bool with_pos, bool with_gid,
-                        cudaStream_t st) {
+                        cudaStream_t st, const ReorderExtra* extra, bool* done) {
     if (n <= 0) return PD_OK;
     if (!h->spare_pos || h->spare_cap != h->cap || h->spare_props.size() != h->props.size()) {
         free_storage(h->spare_pos, h->spare_gid, h->spare_props);
@@ -293,6 +303,9 @@ static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask
         pd::launch(k_gather_cols, g, 256, 0, st, ids, n, G);
         PD_LAUNCH_CHECK();
         G.ncol = 0;
+        G.xb = nullptr;  // only with the records in column 0
+        G.sxy = nullptr;
+        G.sz = nullptr;
         return PD_OK;
     };
     auto add = [&](const void* src, void* dst, int esize) -> int {
@@ -304,6 +317,13 @@ static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask
         return PD_OK;
     };
     if (with_pos) PD_TRY(add(h->pos, h->spare_pos, (int)h->pos_bytes));
+    if (extra && with_pos && h->dtype == PD_F64) {
+        // column 0 holds the records: the first launch also writes the extra outputs
+        G.xb = extra->xb;
+        G.sxy = extra->sxy;
+        G.sz = extra->sz;
+        if (done) *done = true;
+    }
     if (with_gid) PD_TRY(add(h->gid, h->spare_gid, 4));
     for (size_t p = 0; p < h->props.size(); ++p) {
         if (!(prop_mask & (1ul << p))) continue;
@@ -322,9 +342,10 @@ static int permute_swap(pd_vd h, const int* ids, long n, unsigned long prop_mask
 }
 
 int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
-               cudaStream_t st, bool swap) {
+               cudaStream_t st, bool swap, const ReorderExtra* extra, bool* done) {
+    if (done) *done = false;
     if (swap && !g_capturing && !g_alloc_ctx)
-        return permute_swap(h, cl->sorted.as<int>(), n_part, prop_mask, with_pos, with_gid, st);
+        return permute_swap(h, cl->sorted.as<int>(), n_part, prop_mask, with_pos, with_gid, st, extra, done);
     return permute(h, cl->sorted.as<int>(), n_part, prop_mask, with_pos, with_gid, false, st);
 }
 

@@ -219,8 +219,16 @@ int cl_geometry(pd_cl cl, pd_vd h, double r_cut, double enlarge, int nn_box);
 int cl_build(pd_vd h, pd_cl cl, long n_part, const unsigned int* n_part_dev, cudaStream_t st, long first = 0);
 // gather src[ids[k]] -> dst[k] for k < n of 4/8/16/32-byte elements (dst may not alias src)
 int gather_bytes(const void* src, void* dst, const int* ids, long n, int esize, cudaStream_t st);
+// Further outputs of the reorder of FP64 positions into spare storage: the reordered
+// records also to `xb` and as (x, y) / z copies to `sxy` / `sz` (room for n_part);
+// *done tells whether they were written (not by the in-place reorder)
+struct ReorderExtra {
+    double4* xb;
+    double2* sxy;
+    double* sz;
+};
 int cl_reorder(pd_vd h, pd_cl cl, long n_part, unsigned long prop_mask, bool with_pos, bool with_gid,
-               cudaStream_t st, bool swap = false);
+               cudaStream_t st, bool swap = false, const ReorderExtra* extra = nullptr, bool* done = nullptr);
 int ghost_boxes_upload(pd_vd h, cudaStream_t st);
 int ghost_generate(pd_vd h, long img_cap, bool sync_count, cudaStream_t st);
 int ghost_replay(pd_vd h, unsigned long prop_mask, bool with_pos, const unsigned int* n_img_dev, long n_img_bound,

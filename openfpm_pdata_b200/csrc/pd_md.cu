@@ -621,7 +621,21 @@ int md_rebuild(pd_md md, cudaStream_t st) {
     PD_TRY(wrap_positions(h, h->n_real, st));
     pd_cl sort_cl = md->mp.use_cell_list ? md->cl : md->vl->cl;
     PD_TRY(cl_build(h, sort_cl, h->n_real, nullptr, st));
-    PD_TRY(cl_reorder(h, sort_cl, h->n_real, md_reorder_mask(md), true, true, st, md->swap_reorder));
+    // the plain FP64 path: the reorder also writes the build positions and the pair
+    // kernel's staging copies of the real particles
+    const bool split_cand = md->physics == 0 && !md->mixed && !md->mp.use_cell_list && h->dtype == PD_F64;
+    bool extra_done = false;
+    PD_TRY(md->xb.ensure((size_t)(h->n_real > 0 ? h->n_real : 1) * h->pos_bytes));  // room for the build positions
+    if (split_cand) {
+        const size_t cap = (size_t)(h->cap > 0 ? h->cap : 1);
+        PD_TRY(md->sxy.ensure(cap * sizeof(double2)));
+        PD_TRY(md->sz.ensure(cap * sizeof(double)));
+        const ReorderExtra ex{md->xb.as<double4>(), md->sxy.as<double2>(), md->sz.as<double>()};
+        PD_TRY(cl_reorder(h, sort_cl, h->n_real, md_reorder_mask(md), true, true, st, md->swap_reorder, &ex,
+                          &extra_done));
+    } else {
+        PD_TRY(cl_reorder(h, sort_cl, h->n_real, md_reorder_mask(md), true, true, st, md->swap_reorder));
+    }
     if (h->nbox == 0) PD_TRY(ghost_boxes_upload(h, st));
     PD_TRY(ghost_generate(h, 0, true, st));
     if (md->mp.use_cell_list) {
@@ -647,8 +661,18 @@ int md_rebuild(pd_md md, cudaStream_t st) {
             PD_CUDA(cudaMemcpyAsync(md->offb.p, md->off.p, sizeof(float4) * h->n_real, cudaMemcpyDeviceToDevice, st));
         } else {
             if (!md->tiles_active) PD_TRY(verlet_build(h, md->vl, h->n_real, nullptr, st, true));
-            PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice, st));
-            if (md_split(md)) PD_TRY(tile_split(h, md->sxy, md->sz, 0, h->n_total, st));
+            if (!extra_done)
+                PD_CUDA(cudaMemcpyAsync(md->xb.p, h->pos, (size_t)h->n_real * h->pos_bytes, cudaMemcpyDeviceToDevice,
+                                        st));
+            if (md_split(md)) {
+                // the reorder wrote the real particles' copies, unless the images grew the
+                // vector's capacity since (tile_split then takes larger, new buffers)
+                const size_t cap = (size_t)(h->cap > 0 ? h->cap : 1);
+                const bool kept = extra_done && md->sxy.bytes >= cap * sizeof(double2) &&
+                                  md->sz.bytes >= cap * sizeof(double);
+                const long first = kept ? h->n_real : 0;
+                PD_TRY(tile_split(h, md->sxy, md->sz, first, h->n_total - first, st));
+            }
         }
     }
     h->epoch++;
