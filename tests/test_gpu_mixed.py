@@ -130,3 +130,24 @@ def test_mixed_energies_track_fp64(pd):
     print("max rel total-energy diff", np.max(np.abs(tot32 - tot64) / np.abs(tot64)))
     assert np.max(np.abs(tot32 - tot64) / np.abs(tot64)) < 2e-5
     assert np.max(np.abs(E32[:, 1] - E64[:, 1]) / np.abs(E64[:, 1])) < 2e-5
+
+
+def test_mixed_one_run_equals_runs_of_one_step(pd):
+    """Precision form: a run of 24 steps (a step's closing kick fused with the next
+    step's kick and drift of the FP32 offsets) leaves the same positions and
+    velocities, bit for bit, and the same rebuild steps as 24 runs of one step each
+    (separate kick and kick-drift kernels)."""
+    from openfpm_pdata_b200 import workloads
+    x, v, L = workloads.lj_lattice(20, 1.1, 0.05, seed=35)
+    out = []
+    for split in (False, True):
+        vd, md = _system(pd, x, v, L, pd.PREC_MIXED)
+        E = np.concatenate([md.run(1) for _ in range(24)]) if split else md.run(24)
+        out.append((E, vd.deviceToHostPos(with_ghost=False), vd.deviceToHostProp(0, with_ghost=False),
+                    md.stats()[0]))
+    (E0, p0, v0, b0), (E1, p1, v1, b1) = out
+    assert b0 == b1 and b0 >= 3
+    np.testing.assert_array_equal(E0[:, 3], E1[:, 3])
+    np.testing.assert_array_equal(p0, p1)
+    np.testing.assert_array_equal(v0, v1)
+    np.testing.assert_allclose(E0[:, :3], E1[:, :3], rtol=1e-12, atol=1e-9)
