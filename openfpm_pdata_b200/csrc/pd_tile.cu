@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(TBLOCK) k_vtile_build(const typename V4<T>::ty
 // List build in three passes of one z-layer each (tile_rows_layers in
 // pd_tile_dev.cuh): a third of the full staging, more resident CTAs.
 template <class T>
-__global__ void __launch_bounds__(TBLOCK, 10) k_vtile_build3(const typename V4<T>::type* __restrict__ pos,
+__global__ void __launch_bounds__(TBLOCK, 9) k_vtile_build3(const typename V4<T>::type* __restrict__ pos,
                                                          const float4* __restrict__ pos32, long n_real,
                                                          TileGeom tg, const unsigned int* __restrict__ csR,
                                                          const unsigned int* __restrict__ csI, unsigned int pcap,
